@@ -1,0 +1,312 @@
+"""Benchmark of the flip2_b200 fluid step (one JSON line on rank 0).
+
+Workload (default): the 256^3 dam-break at scale -- block x,y in [0,0.5],
+z in [0,1] of the unit box, 8 jittered particles per fluid voxel (seed 0),
+33,554,432 particles, FP32 state, FLIP 0.95, dt = 1/480, Jacobi-PCG to 1e-6
+relative residual with FP64 reductions.  A step is one pass of the whole path:
+bin (keys, radix sort, gather, segment heads), P2G, gravity + divergence,
+pressure solve, projection, G2P + RK2 advection.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: the step does not shard (one box per GPU), so N ranks run N
+independent replicas of the workload; the time is the maximum over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 256
+BLOCK = (0.5, 0.5, 1.0)
+DT = 1.0 / 480.0
+METRIC = "particle-steps/s"
+WORKLOAD = ("dam-break 256^3 voxels (cell 1/256), block 0.5x0.5x1, 8 jittered particles per fluid voxel (seed 0), "
+            "FP32 state, FLIP 0.95, RK2, dt=1/480, Jacobi-PCG to 1e-6 relative residual (FP64 dots)")
+# algorithmic bytes of one PCG iteration per active voxel, fused minimum:
+# matvec+pAp 9 B, x/r/z update with r.z 28 B, direction update 12 B
+PCG_BYTES_PER_VOXEL = 49.0
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="flip2_b200", choices=["flip2_b200", "reference"])
+    ap.add_argument("--cells", type=int, default=N_CELLS, help="voxels per axis (default 256)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def scene(cells):
+    from flip2_b200 import scenes
+    return scenes.dam_break(cells, block=BLOCK, seed=0)
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_sample(cells, max_particles):
+    """Bounded sample of the same workload: the particles of the dam-break
+    scene inside the corner sub-box [0, s]^2 x [0, 2s] (same density, same dt),
+    run with the reference's algorithm restated on the host."""
+    pos, vel = scene(cells)
+    s = 0.5
+    while True:
+        m = (pos[:, 0] < s) & (pos[:, 1] < s) & (pos[:, 2] < 2 * s)
+        if m.sum() <= max_particles or s < 1e-3:
+            break
+        s *= 0.5 ** (1.0 / 3.0)
+    return pos[m].astype(np.float64), vel[m].astype(np.float64), s
+
+
+def ref_substeps(pos, vel, cells, steps):
+    from oracle import oracle as O
+    g = O.grid(0.0, 0.0, 0.0, cells // 4, cells // 4, cells // 4, 4.0 / cells)
+    arrs = [pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2]]
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
+        times.append(time.perf_counter() - t)
+    return times
+
+
+def cpu_baseline(cells, budget_s=20.0):
+    pos, vel, s = cpu_sample(cells, 400_000)
+    t = ref_substeps(pos, vel, cells, 1)[0]
+    n = pos.shape[0]
+    return {"value": n / t, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
+            "sample": "reference algorithm (oracle/flip_oracle.c orc_ref_substep: bin, tent P2G, Courant dt + "
+                      "red-black SOR pressure loop, projection, G2P, Euler advect; FP64, OpenMP) for one sub-step "
+                      "of the %d particles of the workload inside [0,%.3f]^2x[0,%.3f]" % (n, s, 2 * s),
+            "seconds": t}
+
+
+# ------------------------------------------------------------ clocks
+class Clocks:
+    def __init__(self, gpu_index):
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 ".bench_clocks_%d.csv" % gpu_index)
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + CLOCK_QUERY,
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            c = [x.strip() for x in line.split(",")]
+            if len(c) >= 9 and c[1].replace(".", "").isdigit():
+                rows.append(c)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(float(r[2]) for r in rows),
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cells = args.cells
+    steps, warm = max(1, args.steps), max(0, args.warmup)
+    # each sample step ~1 s of host work per 60k particles: keep the run within ~2 minutes
+    budget_particles = int(max(20_000, min(400_000, 110.0 / (steps + warm) * 60_000)))
+    pos, vel, s = cpu_sample(cells, budget_particles)
+    n = pos.shape[0]
+    from oracle import oracle as O
+    g = O.grid(0.0, 0.0, 0.0, cells // 4, cells // 4, cells // 4, 4.0 / cells)
+    arrs = [pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2]]
+    for _ in range(warm):
+        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
+    sec = time.perf_counter() - t0
+    value = n * steps / sec
+    sample = ("reference algorithm restated on the host (oracle/flip_oracle.c orc_ref_substep, FP64, OpenMP, %d "
+              "threads): %d particles of the workload inside [0,%.3f]^2x[0,%.3f], one sub-step per step"
+              % (os.cpu_count(), n, s, 2 * s))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles_sampled": n},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": os.cpu_count(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ own arm
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import flip2_b200 as F
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    pos, vel = scene(args.cells)
+    n = pos.shape[0]
+    stream = torch.cuda.Stream(device=dev)
+    params = F.default_params(F.MODE_NATIVE, device=local)
+    P = F.Particles(n, mode=F.MODE_NATIVE, params=params, stream=stream.cuda_stream)
+    R = args.cells // 4
+    P.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / args.cells)
+    # pinned host state for the end-to-end leg
+    host = [torch.from_numpy(np.ascontiguousarray(pos[:, k])).pin_memory() for k in range(3)]
+    host += [torch.from_numpy(np.ascontiguousarray(vel[:, k])).pin_memory() for k in range(3)]
+    ptrs = [t.data_ptr() for t in host]
+    P.upload_ptrs(ptrs)
+    del pos, vel
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(3, args.warmup)):
+        P.step(DT)
+    P.sync()
+    l0 = P.info().launches
+
+    # ---- device-resident timed region
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    phys = int(vis[local]) if local < len(vis) and vis[local].strip().isdigit() else local
+    clocks = Clocks(phys)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        P.step(DT)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = P.info().launches - l0
+    info = P.info()
+    ms_max = max_over_ranks(ms)
+    value = n * world * args.steps / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        P.upload_ptrs(ptrs)
+        P.step(DT)
+        P.download_ptrs(ptrs)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": n * world * args.steps / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": 24 * n,
+           "d2h_bytes_per_step": 24 * n, "ms_per_step": ms_e2e / args.steps}
+
+    # ---- per-stage breakdown (separate, synchronised steps)
+    P.set_timing(True)
+    P.stage_ms(reset=True)
+    nprof = 3
+    pcg_iters = 0
+    iters = []
+    for _ in range(nprof):
+        P.step(DT)
+        iters.append(P.info().pressure_iters)
+        pcg_iters += iters[-1]
+    stages = {k: v / nprof for k, v in P.stage_ms(reset=True).items()}
+    P.set_timing(False)
+    fluid_tiles = P.info().nodes
+    voxels = fluid_tiles * 512
+    t_iter_ms = stages["pcg_iterations"] / max(1.0, pcg_iters / nprof)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = PCG_BYTES_PER_VOXEL * voxels / (t_iter_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tr.get("pcg_iteration_bytes_per_voxel")
+        if traffic is not None:
+            traffic = traffic * voxels
+    except (OSError, ValueError):
+        pass
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "pcg iteration (matvec+pAp, x/r update with r.r and r.z, direction)",
+                "algorithmic_bytes": "49 B per active voxel per iteration x %d voxels" % voxels,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cells)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "particles": n, "grid": "%d^3" % args.cells, "dt": DT,
+                           "parallelism": "replicas x%d" % world,
+                           "l2": "inputs larger than L2: %.0f MB particle state per replica" % (24 * n / 1e6)},
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+                "pcg_iters_per_step": iters, "pressure_solve_ms": stages["pcg_setup"] + stages["pcg_iterations"],
+                "stages_ms": stages, "fluid_tiles": fluid_tiles,
+                "pcg_rel_residual": info.residual, "error_flags": info.error_flags}
+        print(json.dumps(line), flush=True)
+    P.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

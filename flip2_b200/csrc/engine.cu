@@ -1,0 +1,955 @@
+// engine.cu -- the flip_engine handle: the B200 counterpart of the
+// reference's Particles class (engine/particles.hu:11-95, particles.cu).
+//
+// Ownership: the handle owns every device buffer.  Buffers whose size is
+// known at flip_create/flip_set_domain come from one arena allocation; the
+// reference-mode voxel buffers, whose size depends on the particles, grow
+// geometrically and are never shrunk (the reference reallocates with
+// cudaMallocAsync every step).  Nothing is allocated inside flip_step in
+// native mode.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "native.cuh"
+#include "ref_kernels.cuh"
+
+using namespace flip;
+
+struct flip_engine {
+    flip_params P{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint64_t n = 0;
+    bool have_domain = false, binned = false, have_voxels = false;
+    flip_grid grid{};
+    std::string err;
+
+    // arena
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+
+    // shared binning buffers
+    uint32_t *keys = nullptr, *perm = nullptr, *flags = nullptr, *starts = nullptr, *node_keys = nullptr;
+    uint32_t* d_counts = nullptr;  // [0] nodes/tiles, [1] grid tiles, [2..] spare
+    void* sort_scratch = nullptr;
+    size_t sort_scratch_bytes = 0;
+    void* scan_scratch = nullptr;
+    size_t scan_scratch_bytes = 0;
+    int key_bits = 32;
+    uint32_t* h_small = nullptr;  // pinned readback words
+    uint32_t nodes = 0;
+
+    // ---- reference mode (FP64)
+    double* pd[6] = {};  // px py pz vx vy vz
+    double* pt[6] = {};  // gather targets
+    uint32_t *ytable = nullptr, *counts = nullptr, *masks = nullptr, *node_voxels = nullptr;
+    uint64_t node_cap = 0;
+    double* getmax_buf = nullptr;
+    uint64_t vox_cap = 0;
+    uint32_t voxels = 0;
+    uint32_t* voxel_ids = nullptr;
+    int8_t* solids = nullptr;
+    double *ux = nullptr, *uy = nullptr, *uz = nullptr, *divU = nullptr, *p = nullptr, *res = nullptr;
+    double dt = 0.0, frameDt = 1.0 / 24.0, elapsed = 0.0, elapsedThisFrame = 0.0, residual = 0.0;
+    uint32_t gs_iters = 0;
+
+    // ---- native mode (FP32)
+    NatDims D{};
+    uint64_t nslots = 0, ntiles_total = 0;
+    float* fp[6] = {};
+    float* fq[6] = {};
+    float *m[3] = {}, *w[3] = {}, *o[3] = {};
+    uint8_t *type = nullptr, *solid_tiled = nullptr, *tile_flags = nullptr;
+    bool has_solid = false;
+    uint32_t* grid_tiles = nullptr;
+    PcgBuffers pcg{};
+    PcgState* h_state = nullptr;
+    cudaGraphExec_t pcg_graph = nullptr;
+    int pcg_graph_iters = 0;
+    int sms = 148;
+    int last_iters = 0, last_converged = 0;
+    double last_rel = 0.0;
+    uint32_t launches = 0;
+    // stage timing
+    bool timing = false;
+    cudaEvent_t ev[FLIP_NUM_STAGES + 1] = {};
+    double stage_ms[FLIP_NUM_STAGES] = {};
+    int mark(int k) {
+        if (!timing) return FLIP_OK;
+        return cuda(cudaEventRecord(ev[k], stream), "cudaEventRecord");
+    }
+
+    int fail(int code, const std::string& what) {
+        err = what;
+        set_error_text(what.c_str());
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return FLIP_OK;
+        int c = set_cuda_error(e, what);
+        err = error_text();
+        return c;
+    }
+};
+
+#define E_TRY(expr)                                            \
+    do {                                                       \
+        int _r = (expr);                                       \
+        if (_r != FLIP_OK) {                                   \
+            if (e->err.empty()) e->err = ::flip::error_text(); \
+            return _r;                                         \
+        }                                                      \
+    } while (0)
+#define E_CUDA(expr) E_TRY(e->cuda((expr), #expr))
+
+static size_t al(size_t v) { return (v + 255) / 256 * 256; }
+
+extern "C" void flip_default_params(int mode, flip_params* out) {
+    if (!out) return;
+    memset(out, 0, sizeof(*out));
+    out->mode = mode;
+    out->flip_ratio = 0.95f;
+    out->gravity_y = -9.8f;
+    out->pcg_tol = 1e-6;
+    out->pcg_max_iter = 5000;
+    out->pcg_check_every = 16;
+    out->true_residual_every = 50;
+    out->permute_velocities = 0;
+    out->device = 0;
+    out->max_substep_dt = 1.0 / 240.0;
+}
+
+extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, flip_engine** out) {
+    if (!out || n == 0 || n >= (1ull << 30)) {
+        set_error_text("flip_create: n must be in 1..2^30-1 and out non-null");
+        return FLIP_ERR_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error_text("flip_create: no CUDA device");
+        return FLIP_ERR_DEVICE;
+    }
+    flip_engine* e = new flip_engine();
+    if (params) e->P = *params;
+    else flip_default_params(FLIP_MODE_NATIVE, &e->P);
+    if (e->P.pcg_check_every <= 0) e->P.pcg_check_every = 16;
+    if (e->P.max_substep_dt <= 0.0) e->P.max_substep_dt = 1.0 / 240.0;
+    e->n = n;
+    int rc = e->cuda(cudaSetDevice(e->P.device), "cudaSetDevice");
+    if (rc) { delete e; return rc; }
+    cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->P.device);
+    if (stream) {
+        e->stream = (cudaStream_t)stream;
+    } else {
+        rc = e->cuda(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (rc) { delete e; return rc; }
+        e->own_stream = true;
+    }
+    rc = e->cuda(cudaMallocHost((void**)&e->h_small, 4096), "cudaMallocHost");
+    if (rc) { flip_destroy(e); return rc; }
+    rc = e->cuda(cudaMallocHost((void**)&e->h_state, sizeof(PcgState)), "cudaMallocHost");
+    if (rc) { flip_destroy(e); return rc; }
+    *out = e;
+    return FLIP_OK;
+}
+
+static void free_arena(flip_engine* e) {
+    if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
+    if (e->arena) cudaFree(e->arena);
+    e->arena = nullptr;
+    e->arena_bytes = 0;
+}
+static void free_ref_voxels(flip_engine* e) {
+    void* ps[] = {e->voxel_ids, e->solids, e->ux, e->uy, e->uz, e->divU, e->p, e->res};
+    for (void* q : ps) if (q) cudaFree(q);
+    e->voxel_ids = nullptr; e->solids = nullptr;
+    e->ux = e->uy = e->uz = e->divU = e->p = e->res = nullptr;
+    e->vox_cap = 0;
+}
+
+static int bits_for(uint64_t maxkey) {
+    int b = 1;
+    while (b < 32 && (maxkey >> b) != 0) ++b;
+    return b;
+}
+
+extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, uint32_t x, uint32_t y, uint32_t z,
+                               double cellSize) {
+    if (!e) return FLIP_ERR_ARG;
+    if (x == 0 || y == 0 || z == 0 || !(cellSize > 0.0)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: empty domain");
+    E_CUDA(cudaSetDevice(e->P.device));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    free_arena(e);
+    free_ref_voxels(e);
+    e->grid.negX = (float)nx; e->grid.negY = (float)ny; e->grid.negZ = (float)nz;  // Grid narrows to float (grid.hpp:118-129)
+    e->grid.sizeX = x; e->grid.sizeY = y; e->grid.sizeZ = z;
+    e->grid.cellSize = (float)cellSize;
+    e->have_domain = true;
+    e->binned = e->have_voxels = false;
+    const uint64_t n = e->n;
+    std::vector<std::pair<void**, size_t>> plan;
+    auto add = [&](void** ptr, size_t bytes) { plan.push_back({ptr, bytes}); };
+    add((void**)&e->keys, 4 * n);
+    add((void**)&e->perm, 4 * n);
+    add((void**)&e->starts, 4 * n);
+    add((void**)&e->d_counts, 64);
+    e->sort_scratch_bytes = flip_sort_pairs_scratch_bytes(n);
+    e->scan_scratch_bytes = scan_scratch_bytes(n);
+    add(&e->sort_scratch, e->sort_scratch_bytes);
+    add(&e->scan_scratch, e->scan_scratch_bytes);
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        // x <= sizeX etc. after the clamp, so keys are bounded by this value
+        uint64_t maxkey = (uint64_t)x + (uint64_t)y * x + (uint64_t)z * x * y;
+        e->key_bits = maxkey >= 0xFFFFFFFFull ? 32 : bits_for(maxkey);
+        e->node_cap = std::min<uint64_t>(n, maxkey + 1);
+        add((void**)&e->flags, 4 * n);
+        for (int a = 0; a < 6; ++a) { add((void**)&e->pd[a], 8 * n); add((void**)&e->pt[a], 8 * n); }
+        add((void**)&e->ytable, 4 * (size_t)y * z);
+        add((void**)&e->counts, 4 * e->node_cap);
+        add((void**)&e->node_voxels, 4 * e->node_cap);
+        add((void**)&e->masks, 64 * e->node_cap);
+        add((void**)&e->getmax_buf, 16 * (n / 512 + 2));
+    } else {
+        uint64_t NX = 4ull * x, NY = 4ull * y, NZ = 4ull * z;
+        if (NX % 8 || NY % 8 || NZ % 8)
+            return e->fail(FLIP_ERR_ARG, "flip_set_domain: native mode needs 4*size to be a multiple of 8 on every axis");
+        NatDims& D = e->D;
+        D.nx = (int)NX; D.ny = (int)NY; D.nz = (int)NZ;
+        D.tx = D.nx / 8; D.ty = D.ny / 8; D.tz = D.nz / 8;
+        D.ox = e->grid.negX; D.oy = e->grid.negY; D.oz = e->grid.negZ;
+        D.h = e->grid.cellSize / 4.0f;
+        e->ntiles_total = (uint64_t)D.tx * D.ty * D.tz;
+        e->nslots = e->ntiles_total * 512;
+        if (e->nslots >= (1ull << 32)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: grid above 2^32 voxels");
+        e->key_bits = bits_for(e->ntiles_total - 1);
+        add((void**)&e->node_keys, 4 * std::min<uint64_t>(n, e->ntiles_total));
+        for (int a = 0; a < 6; ++a) { add((void**)&e->fp[a], 4 * n); add((void**)&e->fq[a], 4 * n); }
+        for (int c = 0; c < 3; ++c) {
+            add((void**)&e->m[c], 4 * e->nslots);
+            add((void**)&e->w[c], 4 * e->nslots);
+            add((void**)&e->o[c], 4 * e->nslots);
+        }
+        add((void**)&e->type, e->nslots);
+        add((void**)&e->tile_flags, e->ntiles_total);
+        add((void**)&e->grid_tiles, 4 * e->ntiles_total);
+        float** pv[6] = {&e->pcg.b, &e->pcg.x, &e->pcg.r, &e->pcg.p, &e->pcg.q, &e->pcg.dinv};
+        for (float** q : pv) add((void**)q, 4 * e->nslots);
+        add((void**)&e->pcg.st, sizeof(PcgState));
+        add((void**)&e->pcg.partials, sizeof(double) * 4 * kPcgBlocks);
+    }
+    size_t total = 0;
+    for (auto& pr : plan) total += al(pr.second ? pr.second : 1);
+    E_CUDA(cudaMalloc((void**)&e->arena, total));
+    e->arena_bytes = total;
+    size_t off = 0;
+    for (auto& pr : plan) { *pr.first = e->arena + off; off += al(pr.second ? pr.second : 1); }
+    if (e->P.mode == FLIP_MODE_NATIVE) {
+        // zero everything once so that stale tiles read as zero
+        E_CUDA(cudaMemsetAsync(e->arena, 0, total, e->stream));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    return FLIP_OK;
+}
+
+// ------------------------------------------------------------- uploads
+extern "C" int flip_upload_particles_f64(flip_engine* e, const double* px, const double* py, const double* pz,
+                                         const double* vx, const double* vy, const double* vz, uint64_t n) {
+    if (!e || !px || !py || !pz) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "upload before setDomain");
+    if (n != e->n) return e->fail(FLIP_ERR_ARG, "upload size differs from the engine size");  // cudaVec.cu:90-93 exits here
+    const double* src[6] = {px, py, pz, vx, vy, vz};
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        for (int a = 0; a < 6; ++a) {
+            if (src[a]) E_CUDA(cudaMemcpyAsync(e->pd[a], src[a], 8 * n, cudaMemcpyDefault, e->stream));
+            else E_CUDA(cudaMemsetAsync(e->pd[a], 0, 8 * n, e->stream));
+        }
+    } else {
+        std::vector<float> tmp(n);
+        for (int a = 0; a < 6; ++a) {
+            if (src[a]) {
+                for (uint64_t i = 0; i < n; ++i) tmp[i] = (float)src[a][i];
+                E_CUDA(cudaMemcpyAsync(e->fp[a], tmp.data(), 4 * n, cudaMemcpyDefault, e->stream));
+                E_CUDA(cudaStreamSynchronize(e->stream));
+            } else {
+                E_CUDA(cudaMemsetAsync(e->fp[a], 0, 4 * n, e->stream));
+            }
+        }
+    }
+    e->binned = e->have_voxels = false;
+    return FLIP_OK;
+}
+
+extern "C" int flip_upload_particles_f32(flip_engine* e, const float* px, const float* py, const float* pz,
+                                         const float* vx, const float* vy, const float* vz, uint64_t n) {
+    if (!e || !px || !py || !pz) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "upload before setDomain");
+    if (n != e->n) return e->fail(FLIP_ERR_ARG, "upload size differs from the engine size");
+    const float* src[6] = {px, py, pz, vx, vy, vz};
+    if (e->P.mode == FLIP_MODE_NATIVE) {
+        for (int a = 0; a < 6; ++a) {
+            if (src[a]) E_CUDA(cudaMemcpyAsync(e->fp[a], src[a], 4 * n, cudaMemcpyDefault, e->stream));
+            else E_CUDA(cudaMemsetAsync(e->fp[a], 0, 4 * n, e->stream));
+        }
+    } else {
+        std::vector<double> tmp(n);
+        for (int a = 0; a < 6; ++a) {
+            if (src[a]) {
+                for (uint64_t i = 0; i < n; ++i) tmp[i] = (double)src[a][i];
+                E_CUDA(cudaMemcpyAsync(e->pd[a], tmp.data(), 8 * n, cudaMemcpyDefault, e->stream));
+                E_CUDA(cudaStreamSynchronize(e->stream));
+            } else {
+                E_CUDA(cudaMemsetAsync(e->pd[a], 0, 8 * n, e->stream));
+            }
+        }
+    }
+    e->binned = e->have_voxels = false;
+    return FLIP_OK;
+}
+
+extern "C" int flip_download_particles_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy,
+                                           float* vz, uint64_t n) {
+    if (!e) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "download before setDomain");
+    if (n != e->n) return e->fail(FLIP_ERR_ARG, "download size differs from the engine size");
+    float* dst[6] = {px, py, pz, vx, vy, vz};
+    if (e->P.mode == FLIP_MODE_NATIVE) {
+        for (int a = 0; a < 6; ++a)
+            if (dst[a]) E_CUDA(cudaMemcpyAsync(dst[a], e->fp[a], 4 * n, cudaMemcpyDefault, e->stream));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+    } else {
+        std::vector<double> tmp(n);
+        for (int a = 0; a < 6; ++a) {
+            if (!dst[a]) continue;
+            E_CUDA(cudaMemcpyAsync(tmp.data(), e->pd[a], 8 * n, cudaMemcpyDefault, e->stream));
+            E_CUDA(cudaStreamSynchronize(e->stream));
+            for (uint64_t i = 0; i < n; ++i) dst[a][i] = (float)tmp[i];
+        }
+    }
+    return FLIP_OK;
+}
+
+extern "C" int flip_download_particles_f64(flip_engine* e, double* px, double* py, double* pz, double* vx, double* vy,
+                                           double* vz, uint64_t n) {
+    if (!e) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "download before setDomain");
+    if (n != e->n) return e->fail(FLIP_ERR_ARG, "download size differs from the engine size");
+    double* dst[6] = {px, py, pz, vx, vy, vz};
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        for (int a = 0; a < 6; ++a)
+            if (dst[a]) E_CUDA(cudaMemcpyAsync(dst[a], e->pd[a], 8 * n, cudaMemcpyDefault, e->stream));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+    } else {
+        std::vector<float> tmp(n);
+        for (int a = 0; a < 6; ++a) {
+            if (!dst[a]) continue;
+            E_CUDA(cudaMemcpyAsync(tmp.data(), e->fp[a], 4 * n, cudaMemcpyDefault, e->stream));
+            E_CUDA(cudaStreamSynchronize(e->stream));
+            for (uint64_t i = 0; i < n; ++i) dst[a][i] = (double)tmp[i];
+        }
+    }
+    return FLIP_OK;
+}
+
+extern "C" int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uint64_t n_voxels) {
+    if (!e) return FLIP_ERR_ARG;
+    if (e->P.mode != FLIP_MODE_NATIVE || !e->have_domain) return e->fail(FLIP_ERR_STATE, "solid mask needs a native-mode domain");
+    const NatDims& D = e->D;
+    if (n_voxels != (uint64_t)D.nx * D.ny * D.nz) return e->fail(FLIP_ERR_ARG, "solid mask size != voxel count");
+    if (!e->solid_tiled) E_CUDA(cudaMalloc((void**)&e->solid_tiled, e->nslots));
+    uint8_t* lin = nullptr;
+    E_CUDA(cudaMalloc((void**)&lin, n_voxels));
+    int rc = e->cuda(cudaMemcpyAsync(lin, mask_host, n_voxels, cudaMemcpyDefault, e->stream), "cudaMemcpyAsync");
+    if (!rc) rc = nat_launch_mask_to_tiles(lin, D, e->solid_tiled, e->stream);
+    if (!rc) rc = e->cuda(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    cudaFree(lin);
+    if (rc) return rc;
+    e->has_solid = true;
+    return FLIP_OK;
+}
+
+// ================================================== reference-mode stages
+static int ref_check(flip_engine* e) {
+    if (!e) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain");
+    return FLIP_OK;
+}
+
+static int ref_align(flip_engine* e) {
+    return ref_launch_keys(e->pd[0], e->pd[1], e->pd[2], e->n, e->grid, e->keys, nullptr, e->stream);
+}
+
+static int ref_sort(flip_engine* e) {
+    E_TRY(flip_sort_pairs(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
+                          e->stream));
+    // sortParticles gathers positions only (particles.cu:69-71); velocities
+    // keep their order unless permute_velocities is set
+    int na = e->P.permute_velocities ? 6 : 3;
+    for (int a = 0; a < na; ++a) {
+        E_TRY(ref_gather_f64(e->perm, e->n, e->pd[a], e->pt[a], e->stream));
+        std::swap(e->pd[a], e->pt[a]);
+    }
+    e->binned = true;
+    return FLIP_OK;
+}
+
+static int ensure_voxels(flip_engine* e, uint64_t need) {
+    if (need <= e->vox_cap) return FLIP_OK;
+    uint64_t cap = std::max<uint64_t>(need + need / 4, 4096);
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    free_ref_voxels(e);
+    E_CUDA(cudaMalloc((void**)&e->voxel_ids, 4 * cap));
+    E_CUDA(cudaMalloc((void**)&e->solids, cap));
+    double** d[6] = {&e->ux, &e->uy, &e->uz, &e->divU, &e->p, &e->res};
+    for (double** q : d) E_CUDA(cudaMalloc((void**)q, 8 * cap));
+    e->vox_cap = cap;
+    return FLIP_OK;
+}
+
+static int ref_generate_voxels(flip_engine* e) {
+    if (!e->binned) return e->fail(FLIP_ERR_STATE, "generateVoxels before sortParticles");
+    E_TRY(flip_segment_heads(e->keys, e->n, e->flags, e->starts, nullptr, e->d_counts, e->scan_scratch,
+                             e->scan_scratch_bytes, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_small, e->d_counts, 4, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->nodes = e->h_small[0];
+    if (e->nodes == 0 || e->nodes > e->node_cap) return e->fail(FLIP_ERR_STATE, "node count out of range");
+    E_TRY(ref_launch_ydim(e->starts, e->keys, e->nodes, e->grid, e->ytable, e->stream));
+    E_TRY(ref_launch_voxel_counts(e->starts, e->keys, e->nodes, e->n, e->pd[0], e->pd[1], e->pd[2], e->grid, e->counts,
+                                  e->masks, e->stream));
+    E_TRY(flip_inclusive_scan_u32(e->counts, e->node_voxels, e->nodes, e->scan_scratch, e->scan_scratch_bytes, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_small, e->node_voxels + e->nodes - 1, 4, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->voxels = e->h_small[0];
+    E_TRY(ensure_voxels(e, e->voxels));
+    E_TRY(ref_launch_voxel_ids(e->keys, e->nodes, e->masks, e->node_voxels, e->grid, e->voxel_ids, e->solids, e->stream));
+    E_CUDA(cudaMemsetAsync(e->p, 0, 8 * (size_t)e->voxels, e->stream));
+    e->have_voxels = true;
+    return FLIP_OK;
+}
+
+static int ref_p2g_stage(flip_engine* e) {
+    if (!e->have_voxels) return e->fail(FLIP_ERR_STATE, "particleVelToVoxels before generateVoxels");
+    return ref_launch_p2g(e->starts, e->keys, e->nodes, e->n, e->pd[0], e->pd[1], e->pd[2], e->pd[3], e->pd[4], e->pd[5],
+                          e->node_voxels, e->voxel_ids, e->solids, e->grid, e->ux, e->uy, e->uz, e->stream);
+}
+
+// CudaVec<double>::getMax (cudaVec.cu:205-233) with the reference's reduction
+static int ref_getmax(flip_engine* e, const double* a, uint64_t n, bool absolute, double* out) {
+    double* b0 = e->getmax_buf;
+    double* b1 = e->getmax_buf + (e->n / 512 + 2);
+    E_TRY(ref_launch_getmax_level(n, a, b0, absolute ? 1 : 0, e->stream));
+    for (uint64_t i = n / 512 + 1; i > 1; i = i / 512 + 1) {
+        E_TRY(ref_launch_getmax_level(i, b0, b1, absolute ? 1 : 0, e->stream));
+        std::swap(b0, b1);
+    }
+    double v = 0.0;
+    E_CUDA(cudaMemcpyAsync(e->h_small, b0, 8, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    memcpy(&v, e->h_small, 8);
+    *out = v;
+    return FLIP_OK;
+}
+
+static int ref_courant_dt(flip_engine* e, double* dt) {
+    double a, b, c;
+    E_TRY(ref_getmax(e, e->pd[3], e->n, true, &a));
+    E_TRY(ref_getmax(e, e->pd[4], e->n, true, &b));
+    E_TRY(ref_getmax(e, e->pd[5], e->n, true, &c));
+    double maxVel = std::max(std::fabs(a), std::max(std::fabs(b), std::fabs(c)));
+    double voxelSize = (double)e->grid.cellSize / (8.0 - 2.0 * std::floor(2.0));
+    *dt = 0.7 * (voxelSize / maxVel);
+    return FLIP_OK;
+}
+
+static double ref_scale(const flip_engine* e, double dt) {
+    double vs = (double)(e->grid.cellSize / 4.0f);
+    return dt / (0.014 * vs * vs);
+}
+
+// cudaGSiteration (voxelSolveFunctions.cu:391-412): the convergence reads
+// happen after iteration 0 and then every 1024 iterations, so the sweeps in
+// between run in shared memory in one launch
+static int ref_gs_solve(flip_engine* e, double dt, double threshold, uint32_t max_iter, double* out_res, uint32_t* out_it) {
+    double maxR = 10.0, prevR = 100.0;
+    uint32_t it = 0;
+    const double scale = ref_scale(e, dt), w = 1.9;
+    while (maxR > threshold && it < max_iter) {
+        uint32_t chunk;
+        if (it % 1024 == 0) chunk = 1;
+        else chunk = 1024 - it % 1024;
+        chunk = std::min(chunk, max_iter - it);
+        E_TRY(ref_launch_gs(e->nodes, e->node_voxels, e->voxel_ids, e->solids, e->divU, e->p, e->res, scale, w, chunk,
+                            e->stream));
+        // the iterations inside a chunk never read the residual, and no exit
+        // test can fire before the chunk ends except it == max_iter (the chunk
+        // is clipped to it)
+        uint32_t first = it;
+        it += chunk;
+        if (first % 1024 == 0) {
+            prevR = maxR;
+            E_TRY(ref_getmax(e, e->res, e->voxels, true, &maxR));
+        }
+        if (it == max_iter || (std::fabs(prevR - maxR) < threshold / 1000 && maxR > threshold)) break;
+    }
+    *out_res = maxR;
+    *out_it = it;
+    return FLIP_OK;
+}
+
+static int ref_pressure(flip_engine* e) {
+    if (!e->have_voxels) return e->fail(FLIP_ERR_STATE, "pressureSolve before generateVoxels");
+    const double threshold = 0.01;
+    const uint32_t maxIterations = 16384;
+    double prevTerm = 100.0, term = 0.0;
+    double dt;
+    E_TRY(ref_courant_dt(e, &dt));
+    if (e->frameDt - e->elapsedThisFrame < dt) dt = e->frameDt - e->elapsedThisFrame;
+    E_TRY(ref_launch_gravity(e->voxels, e->solids, e->uy, dt, 0, e->stream));
+    E_TRY(ref_launch_divergence(e->nodes, e->node_voxels, e->voxel_ids, e->ux, e->uy, e->uz, e->grid, e->ytable, e->starts,
+                                e->keys, e->divU, e->stream));
+    uint32_t it = 0, total = 0;
+    for (;;) {
+        E_TRY(ref_gs_solve(e, dt, threshold, maxIterations, &term, &it));
+        total += it;
+        if (!(prevTerm - term > 0)) break;
+        if (term < threshold) break;
+        E_TRY(ref_launch_gravity(e->voxels, e->solids, e->uy, dt, 1, e->stream));
+        dt /= 2.0;
+        E_CUDA(cudaMemsetAsync(e->p, 0, 8 * (size_t)e->voxels, e->stream));
+        E_TRY(ref_launch_gravity(e->voxels, e->solids, e->uy, dt, 0, e->stream));
+        prevTerm = term;
+        E_TRY(ref_launch_divergence(e->nodes, e->node_voxels, e->voxel_ids, e->ux, e->uy, e->uz, e->grid, e->ytable,
+                                    e->starts, e->keys, e->divU, e->stream));
+    }
+    e->dt = dt;
+    e->elapsed += dt;
+    e->elapsedThisFrame += dt;
+    e->residual = term;
+    e->gs_iters = total;
+    return FLIP_OK;
+}
+
+static int ref_update_vel(flip_engine* e) {
+    return ref_launch_velocity_update(e->nodes, e->node_voxels, e->voxel_ids, e->solids, e->p, e->ux, e->uy, e->uz,
+                                      ref_scale(e, e->dt), e->stream);
+}
+static int ref_g2p_stage(flip_engine* e) {
+    return ref_launch_g2p(e->starts, e->keys, e->nodes, e->n, e->pd[0], e->pd[1], e->pd[2], e->node_voxels, e->voxel_ids,
+                          e->ux, e->uy, e->uz, e->grid, e->pd[3], e->pd[4], e->pd[5], e->stream);
+}
+static int ref_advect_stage(flip_engine* e) {
+    return ref_launch_advect(e->n, e->dt, e->pd[0], e->pd[1], e->pd[2], e->pd[3], e->pd[4], e->pd[5], e->stream);
+}
+static int ref_move_solids_stage(flip_engine* e) {
+    E_TRY(ref_launch_move_solids(e->nodes, e->n, e->starts, e->keys, e->pd[0], e->pd[1], e->pd[2], e->node_voxels,
+                                 e->voxel_ids, e->solids, e->grid, e->stream));
+    return ref_g2p_stage(e);
+}
+
+// ===================================================== native-mode step
+static int nat_grid(flip_engine* e, int per_sm) { return e->sms * per_sm; }
+
+static int nat_bin(flip_engine* e) {
+    E_TRY(e->mark(0));
+    E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
+    E_TRY(e->mark(1));
+    E_TRY(flip_sort_pairs(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
+                          e->stream));
+    E_TRY(e->mark(2));
+    E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
+    for (int a = 0; a < 6; ++a) std::swap(e->fp[a], e->fq[a]);
+    E_TRY(e->mark(3));
+    E_TRY(flip_segment_heads(e->keys, e->n, nullptr, e->starts, e->node_keys, e->d_counts, e->scan_scratch,
+                             e->scan_scratch_bytes, e->stream));
+    E_TRY(e->mark(4));
+    e->launches += 1 + 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 1;
+    e->binned = true;
+    return FLIP_OK;
+}
+
+static int nat_p2g_stage(flip_engine* e, double dt) {
+    const size_t fb = 4 * e->nslots;
+    for (int c = 0; c < 3; ++c) {
+        E_CUDA(cudaMemsetAsync(e->m[c], 0, fb, e->stream));
+        E_CUDA(cudaMemsetAsync(e->w[c], 0, fb, e->stream));
+    }
+    E_CUDA(cudaMemsetAsync(e->type, 0, e->nslots, e->stream));
+    E_CUDA(cudaMemsetAsync(e->tile_flags, 0, e->ntiles_total, e->stream));
+    E_TRY(e->mark(5));
+    E_TRY(nat_launch_p2g(e->node_keys, e->starts, e->d_counts, e->n, (const float* const*)e->fp,
+                         (const float* const*)(e->fp + 3), e->D, e->m, e->w, e->type, nat_grid(e, 8), e->stream));
+    if (e->has_solid) E_TRY(nat_launch_apply_solids(e->solid_tiled, e->type, e->nslots, e->stream));
+    E_TRY(e->mark(6));
+    E_TRY(nat_launch_dilate_compact(e->node_keys, e->d_counts, e->D, e->tile_flags, e->grid_tiles, e->d_counts + 1,
+                                    nat_grid(e, 2), e->stream));
+    E_TRY(e->mark(7));
+    E_TRY(nat_launch_normalize(e->grid_tiles, e->d_counts + 1, e->D, (float)(e->P.gravity_y * dt), e->m,
+                               (const float* const*)e->w, e->o, e->type, nat_grid(e, 4), e->stream));
+    E_TRY(e->mark(8));
+    e->launches += 1 + (e->has_solid ? 1 : 0) + 2 + 1;
+    e->have_voxels = true;
+    return FLIP_OK;
+}
+
+static int nat_pcg_graph(flip_engine* e, int iters) {
+    if (e->pcg_graph && e->pcg_graph_iters == iters) return FLIP_OK;
+    if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = FLIP_OK;
+    for (int k = 0; k < iters && rc == FLIP_OK; ++k)
+        rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->type, e->pcg, e->stream);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    E_CUDA(ce);
+    ce = cudaGraphInstantiate(&e->pcg_graph, g, 0);
+    cudaGraphDestroy(g);
+    E_CUDA(ce);
+    e->pcg_graph_iters = iters;
+    return FLIP_OK;
+}
+
+static int nat_pressure(flip_engine* e) {
+    PcgState init{};
+    init.tol2 = e->P.pcg_tol * e->P.pcg_tol;
+    init.max_iter = e->P.pcg_max_iter;
+    init.true_every = e->P.true_residual_every;
+    *e->h_state = init;
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, (const float* const*)e->m, e->type, e->pcg, e->stream));
+    e->launches += 1;
+    E_TRY(e->mark(9));
+    const int chunk = e->P.pcg_check_every;
+    E_TRY(nat_pcg_graph(e, chunk));
+    int launched = 0;
+    for (;;) {
+        E_CUDA(cudaGraphLaunch(e->pcg_graph, e->stream));
+        e->launches += 4u * (uint32_t)chunk;
+        launched += chunk;
+        E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        if (e->h_state->done) break;
+        if (launched > e->P.pcg_max_iter + 2 * chunk) break;  // host-side bound as well
+    }
+    E_TRY(e->mark(10));
+    const PcgState& s = *e->h_state;
+    e->last_iters = s.iter;
+    e->last_converged = (s.done == 1) ? 1 : 0;
+    double rr = s.true_checks ? s.rr_true : s.rr;
+    e->last_rel = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
+    return FLIP_OK;
+}
+
+static int nat_step(flip_engine* e, double dt) {
+    E_TRY(nat_bin(e));
+    E_TRY(nat_p2g_stage(e, dt));
+    E_TRY(nat_pressure(e));
+    E_TRY(nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->type, e->m, nat_grid(e, 4), e->stream));
+    E_TRY(e->mark(11));
+    E_TRY(nat_launch_g2p(e->n, e->D, (float)dt, e->P.flip_ratio, (const float* const*)e->m, (const float* const*)e->o,
+                         e->fp, e->fp + 3, e->stream));
+    E_TRY(e->mark(12));
+    e->launches += 2;
+    if (e->timing) {
+        E_CUDA(cudaEventSynchronize(e->ev[12]));
+        for (int k = 0; k < FLIP_NUM_STAGES; ++k) {
+            float ms = 0.0f;
+            E_CUDA(cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]));
+            e->stage_ms[k] += ms;
+        }
+    }
+    e->dt = dt;
+    e->elapsed += dt;
+    e->binned = false;
+    return FLIP_OK;
+}
+
+// ============================================================ public API
+#define CHECK_E()                                                             \
+    do {                                                                      \
+        if (!e) return FLIP_ERR_ARG;                                          \
+        if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain"); \
+        e->err.clear();                                                       \
+        E_CUDA(cudaSetDevice(e->P.device));                                   \
+    } while (0)
+
+extern "C" int flip_align_particles_to_grid(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_align(e);
+    return nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream);
+}
+extern "C" int flip_sort_particles(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_sort(e);
+    return nat_bin(e);
+}
+extern "C" int flip_generate_voxels(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_generate_voxels(e);
+    if (!e->binned) E_TRY(nat_bin(e));
+    return FLIP_OK;
+}
+extern "C" int flip_particle_vel_to_voxels(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_p2g_stage(e);
+    if (!e->binned) E_TRY(nat_bin(e));
+    return nat_p2g_stage(e, e->P.max_substep_dt);
+}
+extern "C" int flip_pressure_solve(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_pressure(e);
+    if (!e->have_voxels) return e->fail(FLIP_ERR_STATE, "pressureSolve before particleVelToVoxels");
+    return nat_pressure(e);
+}
+extern "C" int flip_update_voxel_velocities(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_update_vel(e);
+    return nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->type, e->m, nat_grid(e, 4), e->stream);
+}
+extern "C" int flip_voxel_vels_to_particles(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_g2p_stage(e);
+    // native G2P moves the particles as well (advection is fused)
+    return nat_launch_g2p(e->n, e->D, (float)e->P.max_substep_dt, e->P.flip_ratio, (const float* const*)e->m,
+                          (const float* const*)e->o, e->fp, e->fp + 3, e->stream);
+}
+extern "C" int flip_advect_particles(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_advect_stage(e);
+    return FLIP_OK;  // fused into flip_voxel_vels_to_particles
+}
+extern "C" int flip_move_solid_particles(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) return ref_move_solids_stage(e);
+    return FLIP_OK;  // native positions are clamped inside the box by G2P
+}
+extern "C" int flip_initialize(flip_engine* e) {
+    CHECK_E();
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        E_TRY(ref_align(e));
+        E_TRY(ref_sort(e));
+        E_TRY(ref_generate_voxels(e));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        return FLIP_OK;
+    }
+    return nat_bin(e);
+}
+extern "C" double flip_get_courant_dt(flip_engine* e) {
+    if (!e || !e->have_domain || e->P.mode != FLIP_MODE_REFERENCE) return 0.0;
+    double dt = 0.0;
+    if (ref_courant_dt(e, &dt)) return 0.0;
+    return dt;
+}
+
+extern "C" int flip_solve_frame(flip_engine* e, double fps) {
+    CHECK_E();
+    if (!(fps > 0.0)) return e->fail(FLIP_ERR_ARG, "fps must be positive");
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        // Particles::solveFrame (particles.cu:784-803)
+        if (!e->have_voxels) return e->fail(FLIP_ERR_STATE, "solveFrame before initialize");
+        e->frameDt = 1.0 / fps;
+        e->dt = e->frameDt / 10.0;
+        e->elapsedThisFrame = 0.0;
+        int guard = 0;
+        while (e->elapsedThisFrame < e->frameDt) {
+            E_TRY(ref_p2g_stage(e));
+            E_TRY(ref_pressure(e));
+            E_TRY(ref_update_vel(e));
+            E_TRY(ref_g2p_stage(e));
+            E_TRY(ref_advect_stage(e));
+            E_TRY(ref_move_solids_stage(e));
+            E_TRY(ref_align(e));
+            E_TRY(ref_sort(e));
+            E_TRY(ref_generate_voxels(e));
+            if (++guard > 1000000) return e->fail(FLIP_ERR_STATE, "solveFrame: dt collapsed");
+        }
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        return FLIP_OK;
+    }
+    const double frameDt = 1.0 / fps;
+    const int nsub = std::max(1, (int)std::ceil(frameDt / e->P.max_substep_dt - 1e-9));
+    for (int k = 0; k < nsub; ++k) E_TRY(nat_step(e, frameDt / nsub));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    return FLIP_OK;
+}
+
+extern "C" int flip_step(flip_engine* e, double dt) {
+    CHECK_E();
+    if (!(dt > 0.0)) return e->fail(FLIP_ERR_ARG, "dt must be positive");
+    if (e->P.mode == FLIP_MODE_NATIVE) return nat_step(e, dt);
+    // reference math with a fixed dt: bin, P2G, gravity + divergence, SOR,
+    // projection, G2P, advection (no Courant clamp, no dt halving)
+    E_TRY(ref_align(e));
+    E_TRY(ref_sort(e));
+    E_TRY(ref_generate_voxels(e));
+    E_TRY(ref_p2g_stage(e));
+    E_TRY(ref_launch_gravity(e->voxels, e->solids, e->uy, dt, 0, e->stream));
+    E_TRY(ref_launch_divergence(e->nodes, e->node_voxels, e->voxel_ids, e->ux, e->uy, e->uz, e->grid, e->ytable, e->starts,
+                                e->keys, e->divU, e->stream));
+    double term;
+    uint32_t it;
+    E_TRY(ref_gs_solve(e, dt, 0.01, 16384, &term, &it));
+    e->dt = dt;
+    e->residual = term;
+    e->gs_iters = it;
+    E_TRY(ref_update_vel(e));
+    E_TRY(ref_g2p_stage(e));
+    E_TRY(ref_advect_stage(e));
+    e->elapsed += dt;
+    return FLIP_OK;
+}
+
+extern "C" int flip_sync(flip_engine* e) {
+    if (!e) return FLIP_ERR_ARG;
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    return FLIP_OK;
+}
+
+extern "C" int flip_write_positions_csv(flip_engine* e, const char* path) {
+    if (!e || !path) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain");
+    std::vector<double> x(e->n), y(e->n), z(e->n);
+    E_TRY(flip_download_particles_f64(e, x.data(), y.data(), z.data(), nullptr, nullptr, nullptr, e->n));
+    FILE* f = fopen(path, "w");
+    if (!f) return e->fail(FLIP_ERR_ARG, std::string("cannot open ") + path);
+    // std::ostream's default format is %g with 6 significant digits
+    for (uint64_t i = 0; i < e->n; ++i) fprintf(f, "%g, %g, %g\n", x[i], y[i], z[i]);
+    fclose(f);
+    return FLIP_OK;
+}
+
+extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, uint32_t* elem_size) {
+    if (!e || !dev_ptr || !count || !elem_size) return FLIP_ERR_ARG;
+    const bool ref = e->P.mode == FLIP_MODE_REFERENCE;
+    if (!ref && e->have_domain) {  // refresh the device-side tile count
+        E_CUDA(cudaMemcpyAsync(e->h_small, e->d_counts, 8, cudaMemcpyDeviceToHost, e->stream));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        e->nodes = e->h_small[0];
+    }
+    void* p = nullptr;
+    uint64_t c = 0;
+    uint32_t es = 4;
+    switch (which) {
+    case FLIP_BUF_PX: case FLIP_BUF_PY: case FLIP_BUF_PZ: case FLIP_BUF_VX: case FLIP_BUF_VY: case FLIP_BUF_VZ:
+        p = ref ? (void*)e->pd[which] : (void*)e->fp[which];
+        c = e->n; es = ref ? 8 : 4; break;
+    case FLIP_BUF_KEYS: p = e->keys; c = e->n; break;
+    case FLIP_BUF_PERM: p = e->perm; c = e->n; break;
+    case FLIP_BUF_FLAGS: p = e->flags; c = ref ? e->n : 0; break;
+    case FLIP_BUF_STARTS: p = e->starts; c = e->nodes; break;
+    case FLIP_BUF_YTABLE: p = e->ytable; c = ref ? (uint64_t)e->grid.sizeY * e->grid.sizeZ : 0; break;
+    case FLIP_BUF_NODE_VOXELS: p = e->node_voxels; c = ref ? e->nodes : 0; break;
+    case FLIP_BUF_VOXEL_IDS: p = e->voxel_ids; c = ref ? e->voxels : 0; break;
+    case FLIP_BUF_SOLIDS: p = e->solids; c = ref ? e->voxels : 0; es = 1; break;
+    case FLIP_BUF_UX: p = ref ? (void*)e->ux : (void*)e->m[0]; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_UY: p = ref ? (void*)e->uy : (void*)e->m[1]; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_UZ: p = ref ? (void*)e->uz : (void*)e->m[2]; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_DIVU: p = ref ? (void*)e->divU : (void*)e->pcg.b; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_P: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_RES: p = ref ? (void*)e->res : (void*)e->pcg.r; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_GRID_U: p = e->m[0]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_GRID_V: p = e->m[1]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_GRID_W: p = e->m[2]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_CELL_TYPE: p = e->type; c = ref ? 0 : e->nslots; es = 1; break;
+    case FLIP_BUF_PRESSURE: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_TILE_LIST: p = e->node_keys; c = ref ? 0 : e->nodes; break;
+    case FLIP_BUF_GRID_U_P2G: p = e->o[0]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_GRID_V_P2G: p = e->o[1]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_GRID_W_P2G: p = e->o[2]; c = ref ? 0 : e->nslots; break;
+    default: return e->fail(FLIP_ERR_ARG, "unknown buffer id");
+    }
+    *dev_ptr = p;
+    *count = c;
+    *elem_size = es;
+    return FLIP_OK;
+}
+
+extern "C" int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint64_t bytes) {
+    if (!e || !host_dst) return FLIP_ERR_ARG;
+    void* p = nullptr;
+    uint64_t c = 0;
+    uint32_t es = 0;
+    E_TRY(flip_get_buffer(e, which, &p, &c, &es));
+    if (bytes > c * es || !p) return e->fail(FLIP_ERR_ARG, "flip_read_buffer: more bytes than the buffer holds");
+    E_CUDA(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    return FLIP_OK;
+}
+
+extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
+    if (!e || !out) return FLIP_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    if (e->have_domain) {
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        if (e->P.mode == FLIP_MODE_NATIVE) {
+            E_CUDA(cudaMemcpy(e->h_small, e->d_counts, 8, cudaMemcpyDeviceToHost));
+            e->nodes = e->h_small[0];
+            out->nodes = e->h_small[0];
+            out->voxels = e->h_small[1];
+            out->pressure_iters = e->last_iters;
+            out->converged = e->last_converged;
+            out->residual = e->last_rel;
+            uint32_t ew[2] = {0, 0};
+            E_CUDA(cudaMemcpy(ew, e->sort_scratch, 4, cudaMemcpyDeviceToHost));
+            E_CUDA(cudaMemcpy(ew + 1, e->scan_scratch, 4, cudaMemcpyDeviceToHost));
+            out->error_flags = ew[0] | ew[1];
+        } else {
+            out->nodes = e->nodes;
+            out->voxels = e->voxels;
+            out->pressure_iters = (int32_t)e->gs_iters;
+            out->converged = e->residual < 0.01 ? 1 : 0;
+            out->residual = e->residual;
+            uint32_t ew[2] = {0, 0};
+            E_CUDA(cudaMemcpy(ew, e->sort_scratch, 4, cudaMemcpyDeviceToHost));
+            E_CUDA(cudaMemcpy(ew + 1, e->scan_scratch, 4, cudaMemcpyDeviceToHost));
+            out->error_flags = ew[0] | ew[1];
+        }
+    }
+    out->dt = e->dt;
+    out->elapsed_time = e->elapsed;
+    out->n = e->n;
+    out->launches = e->launches;
+    return FLIP_OK;
+}
+
+extern "C" int flip_set_timing(flip_engine* e, int enable) {
+    if (!e) return FLIP_ERR_ARG;
+    if (enable && !e->ev[0])
+        for (auto& v : e->ev) E_CUDA(cudaEventCreate(&v));
+    e->timing = enable != 0;
+    return FLIP_OK;
+}
+
+extern "C" int flip_get_stage_ms(flip_engine* e, double* ms, int n, int reset) {
+    if (!e || !ms || n < 0) return FLIP_ERR_ARG;
+    for (int k = 0; k < n && k < FLIP_NUM_STAGES; ++k) ms[k] = e->stage_ms[k];
+    if (reset)
+        for (double& v : e->stage_ms) v = 0.0;
+    return FLIP_OK;
+}
+
+extern "C" const char* flip_last_error(flip_engine* e) {
+    if (!e) return error_text();
+    return e->err.c_str();
+}
+
+extern "C" int flip_destroy(flip_engine* e) {
+    if (!e) return FLIP_OK;
+    cudaSetDevice(e->P.device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_arena(e);
+    free_ref_voxels(e);
+    if (e->solid_tiled) cudaFree(e->solid_tiled);
+    if (e->h_small) cudaFreeHost(e->h_small);
+    if (e->h_state) cudaFreeHost(e->h_state);
+    for (auto& v : e->ev) if (v) cudaEventDestroy(v);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return FLIP_OK;
+}

@@ -1,0 +1,604 @@
+// native.cu -- the north-star fluid step on sm_100a (FP32 state).
+//
+// Grid layout.  Voxel grids are dense, allocated once for the whole box
+// (256^3 voxels are 64 MiB per float field; a B200 holds 180 GB) and stored
+// tile-blocked: slot = tile*512 + (i&7) + 8*(j&7) + 64*(k&7), tile =
+// (i>>3) + TX*((j>>3) + TY*(k>>3)).  A tile's 512 values are one contiguous
+// 2 KiB block, neighbours are address arithmetic (no index tables), and only
+// the tiles that hold particles (or touch their stencils) are visited.  Face
+// (i,j,k) of a velocity component is the negative face of cell (i,j,k); the
+// positive box walls are implicit zeros.
+//
+// Particles are SoA float arrays sorted by tile every step (sort.cu), so a
+// CTA working on one tile reads one contiguous particle range.
+#include "common.cuh"
+#include "native.cuh"
+
+namespace flip {
+
+__device__ __forceinline__ uint32_t nslot(int i, int j, int k, const NatDims& D) {
+    uint32_t t = (uint32_t)((i >> 3) + D.tx * ((j >> 3) + D.ty * (k >> 3)));
+    return (t << 9) | (uint32_t)((i & 7) | ((j & 7) << 3) | ((k & 7) << 6));
+}
+__device__ __forceinline__ int nat_cell(float p, float o, float h, int n) {
+    float t = floorf(__fdiv_rn(__fsub_rn(p, o), h));
+    int c = (t >= (float)n) ? n - 1 : (int)t;
+    if (!(t > 0.0f)) c = 0;
+    return c;
+}
+__device__ __forceinline__ uint8_t nat_type(const uint8_t* type, int i, int j, int k, const NatDims& D) {
+    if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return kSolid;
+    return type[nslot(i, j, k, D)];
+}
+__device__ __forceinline__ void nat_axis(float s, int M, int& i0, float& f) {
+    s = fminf(fmaxf(s, 0.0f), (float)M);
+    int b = (int)floorf(s);
+    b = min(b, M - 1);
+    b = max(b, 0);
+    i0 = b;
+    f = s - (float)b;
+}
+// trilinear stencil of component c at grid coordinates (gx, gy, gz)
+__device__ __forceinline__ void nat_stencil(int c, float gx, float gy, float gz, const NatDims& D, int& i0, int& j0, int& k0,
+                                            float& fx, float& fy, float& fz) {
+    nat_axis(c == 0 ? gx : gx - 0.5f, c == 0 ? D.nx : D.nx - 1, i0, fx);
+    nat_axis(c == 1 ? gy : gy - 0.5f, c == 1 ? D.ny : D.ny - 1, j0, fy);
+    nat_axis(c == 2 ? gz : gz - 0.5f, c == 2 ? D.nz : D.nz - 1, k0, fz);
+}
+__device__ __forceinline__ bool nat_wall(int c, int i, int j, int k, const NatDims& D) {
+    if (c == 0) return i == 0 || i == D.nx;
+    if (c == 1) return j == 0 || j == D.ny;
+    return k == 0 || k == D.nz;
+}
+__device__ __forceinline__ float nat_sample(const float* __restrict__ f, int c, float gx, float gy, float gz,
+                                            const NatDims& D) {
+    int i0, j0, k0;
+    float fx, fy, fz;
+    nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
+    float s = 0.0f;
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+            for (int di = 0; di < 2; ++di) {
+                int i = i0 + di, j = j0 + dj, k = k0 + dk;
+                if (nat_wall(c, i, j, k, D)) continue;
+                float w = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) * (dk ? fz : 1.0f - fz);
+                s = fmaf(w, __ldg(f + nslot(i, j, k, D)), s);
+            }
+    return s;
+}
+
+// ------------------------------------------------------------- binning
+__global__ void nat_keys_kernel(const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
+                                uint64_t n, NatDims D, uint32_t* __restrict__ keys) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int i = nat_cell(px[p], D.ox, D.h, D.nx), j = nat_cell(py[p], D.oy, D.h, D.ny), k = nat_cell(pz[p], D.oz, D.h, D.nz);
+    keys[p] = (uint32_t)((i >> 3) + D.tx * ((j >> 3) + D.ty * (k >> 3)));
+}
+
+// gather of the six state arrays through the sort permutation
+__global__ void nat_gather_kernel(const uint32_t* __restrict__ perm, uint64_t n, const float* __restrict__ a0,
+                                  const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ a3,
+                                  const float* __restrict__ a4, const float* __restrict__ a5, float* __restrict__ b0,
+                                  float* __restrict__ b1, float* __restrict__ b2, float* __restrict__ b3,
+                                  float* __restrict__ b4, float* __restrict__ b5) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = perm[i];
+    if (s >= n) s = (uint32_t)i;  // a valid permutation always has s < n
+    b0[i] = __ldg(a0 + s); b1[i] = __ldg(a1 + s); b2[i] = __ldg(a2 + s);
+    b3[i] = __ldg(a3 + s); b4[i] = __ldg(a4 + s); b5[i] = __ldg(a5 + s);
+}
+
+// ------------------------------------------------------------------ P2G
+// One CTA per occupied tile (persistent loop).  The tile's particles scatter
+// trilinear weights into a shared-memory box of 10^3 nodes per component
+// (the tile plus the one-node halo its stencils reach); the box is then
+// added to the global grids.  Also marks the cells that hold particles.
+constexpr int kP2GThreads = 256;
+constexpr int kBox = 10;
+constexpr int kBoxN = kBox * kBox * kBox;
+
+__global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
+    const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
+    uint64_t n, const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
+    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, NatDims D,
+    float* __restrict__ mu, float* __restrict__ mv, float* __restrict__ mw, float* __restrict__ wu,
+    float* __restrict__ wv, float* __restrict__ ww, uint8_t* __restrict__ type) {
+    __shared__ float sm[3][2][kBoxN];
+    const uint32_t ntiles = *d_ntiles;
+    float* gm[3] = {mu, mv, mw};
+    float* gw[3] = {wu, wv, ww};
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        for (int l = threadIdx.x; l < 3 * 2 * kBoxN; l += kP2GThreads) (&sm[0][0][0])[l] = 0.0f;
+        __syncthreads();
+        const uint32_t key = tile_keys[t];
+        const int tx = key % D.tx, ty = (key / D.tx) % D.ty, tz = key / (D.tx * D.ty);
+        const int bi = 8 * tx - 1, bj = 8 * ty - 1, bk = 8 * tz - 1;  // box origin
+        const uint32_t start = starts[t];
+        const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
+        for (uint64_t p = start + threadIdx.x; p < end; p += kP2GThreads) {
+            const float x = px[p], y = py[p], z = pz[p];
+            const float gx = __fdiv_rn(__fsub_rn(x, D.ox), D.h), gy = __fdiv_rn(__fsub_rn(y, D.oy), D.h),
+                        gz = __fdiv_rn(__fsub_rn(z, D.oz), D.h);
+            type[nslot(nat_cell(x, D.ox, D.h, D.nx), nat_cell(y, D.oy, D.h, D.ny), nat_cell(z, D.oz, D.h, D.nz), D)] = kFluid;
+            const float v[3] = {vx[p], vy[p], vz[p]};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                int i0, j0, k0;
+                float fx, fy, fz;
+                nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
+#pragma unroll
+                for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+                    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+                        for (int di = 0; di < 2; ++di) {
+                            int i = i0 + di, j = j0 + dj, k = k0 + dk;
+                            if (nat_wall(c, i, j, k, D)) continue;
+                            int li = i - bi, lj = j - bj, lk = k - bk;
+                            if ((unsigned)li >= (unsigned)kBox || (unsigned)lj >= (unsigned)kBox || (unsigned)lk >= (unsigned)kBox)
+                                continue;  // cannot happen for particles of this tile; guards the box
+                            float w = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) * (dk ? fz : 1.0f - fz);
+                            int l = li + kBox * (lj + kBox * lk);
+                            atomicAdd(&sm[c][0][l], w * v[c]);
+                            atomicAdd(&sm[c][1][l], w);
+                        }
+            }
+        }
+        __syncthreads();
+        for (int l = threadIdx.x; l < kBoxN; l += kP2GThreads) {
+            const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
+            const int i = bi + li, j = bj + lj, k = bk + lk;
+            if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) continue;
+            const uint32_t s = nslot(i, j, k, D);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float w = sm[c][1][l];
+                if (w != 0.0f) {
+                    atomicAdd(gw[c] + s, w);
+                    atomicAdd(gm[c] + s, sm[c][0][l]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// tiles touched by the stencils of occupied tiles: 3x3x3 dilation
+__global__ void nat_dilate_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                  uint8_t* __restrict__ flags) {
+    const uint32_t ntiles = *d_ntiles;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+        uint32_t key = tile_keys[t];
+        int tx = key % D.tx, ty = (key / D.tx) % D.ty, tz = key / (D.tx * D.ty);
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int a = tx + dx, b = ty + dy, c = tz + dz;
+                    if (a < 0 || b < 0 || c < 0 || a >= D.tx || b >= D.ty || c >= D.tz) continue;
+                    flags[a + D.tx * (b + D.ty * c)] = 1;
+                }
+    }
+}
+
+// single-CTA compaction of tile flags into a list (ascending tile order)
+constexpr int kCompactThreads = 1024;
+__global__ void __launch_bounds__(kCompactThreads) nat_compact_kernel(const uint8_t* __restrict__ flags, uint32_t ntotal,
+                                                                       uint32_t* __restrict__ list, uint32_t* __restrict__ d_count) {
+    __shared__ uint32_t sh[kCompactThreads / 32 + 1];
+    const uint32_t per = (ntotal + kCompactThreads - 1) / kCompactThreads;
+    const uint32_t b0 = threadIdx.x * per, b1 = min(ntotal, b0 + per);
+    uint32_t c = 0;
+    for (uint32_t i = b0; i < b1; ++i) c += flags[i] ? 1u : 0u;
+    uint32_t total;
+    uint32_t o = block_exclusive_scan<kCompactThreads>(c, sh, &total);
+    for (uint32_t i = b0; i < b1; ++i)
+        if (flags[i]) list[o++] = i;
+    if (threadIdx.x == 0) *d_count = total;
+}
+
+// solid mask (tile-blocked) onto the cell types
+__global__ void nat_apply_solids_kernel(const uint8_t* __restrict__ solid, uint8_t* __restrict__ type, uint64_t nslots) {
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nslots && solid[s]) type[s] = kSolid;
+}
+
+// linear (x fastest) mask -> tile-blocked
+__global__ void nat_mask_to_tiles_kernel(const uint8_t* __restrict__ lin, NatDims D, uint8_t* __restrict__ tiled) {
+    uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    if (id >= nc) return;
+    int i = (int)(id % D.nx), j = (int)((id / D.nx) % D.ny), k = (int)(id / ((uint64_t)D.nx * D.ny));
+    tiled[nslot(i, j, k, D)] = lin[id];
+}
+
+// -------------------------------------------- normalise + classify faces
+// 512 threads per tile, one per slot.  Momentum/weight -> velocity; the
+// pre-gravity value is the FLIP "old" grid; faces touching a solid cell are
+// zero; faces touching a fluid cell receive gravity.
+__global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_count,
+                                                             NatDims D, float gdt, float* __restrict__ mu, float* __restrict__ mv,
+                                                             float* __restrict__ mw, const float* __restrict__ wu,
+                                                             const float* __restrict__ wv, const float* __restrict__ ww,
+                                                             float* __restrict__ ou, float* __restrict__ ov,
+                                                             float* __restrict__ ow, const uint8_t* __restrict__ type) {
+    const uint32_t cnt = *d_count;
+    float* m[3] = {mu, mv, mw};
+    const float* w[3] = {wu, wv, ww};
+    float* o[3] = {ou, ov, ow};
+    const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
+    for (uint32_t t = blockIdx.x; t < cnt; t += gridDim.x) {
+        const uint32_t key = tiles[t];
+        const int i = 8 * (key % D.tx) + li, j = 8 * ((key / D.tx) % D.ty) + lj, k = 8 * (key / (D.tx * D.ty)) + lk;
+        const uint32_t s = (key << 9) | threadIdx.x;
+        const uint8_t tb = type[s];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float wt = w[c][s];
+            float val = wt > 0.0f ? __fdiv_rn(m[c][s], wt) : 0.0f;
+            o[c][s] = val;
+            uint8_t ta = nat_type(type, i - (c == 0), j - (c == 1), k - (c == 2), D);
+            if (ta == kSolid || tb == kSolid) val = 0.0f;
+            else if (c == 1 && (ta == kFluid || tb == kFluid)) val += gdt;
+            m[c][s] = val;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- PCG
+// q = A p on fluid cells: A has diagonal = number of non-solid neighbours and
+// -1 for each fluid neighbour (air neighbours are Dirichlet zero).
+__device__ __forceinline__ float nat_apply_A(const float* __restrict__ x, const uint8_t* __restrict__ type, int i, int j,
+                                             int k, uint32_t s, const NatDims& D) {
+    const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+    float d = 0.0f, sum = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        int a = i + oi[q], b = j + oj[q], c = k + ok[q];
+        uint8_t t = nat_type(type, a, b, c, D);
+        if (t == kSolid) continue;
+        d += 1.0f;
+        if (t == kFluid) sum += __ldg(x + nslot(a, b, c, D));
+    }
+    return fmaf(d, x[s], -sum);
+}
+__device__ __forceinline__ double nat_apply_A_f64(const float* __restrict__ x, const uint8_t* __restrict__ type, int i, int j,
+                                                  int k, uint32_t s, const NatDims& D) {
+    const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+    double d = 0.0, sum = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        int a = i + oi[q], b = j + oj[q], c = k + ok[q];
+        uint8_t t = nat_type(type, a, b, c, D);
+        if (t == kSolid) continue;
+        d += 1.0;
+        if (t == kFluid) sum += (double)x[nslot(a, b, c, D)];
+    }
+    return d * (double)x[s] - sum;
+}
+
+// last CTA to finish sums the per-CTA partials (fixed order: deterministic)
+template <int NV>
+__device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
+                                                  double (&out)[NV]) {
+    __shared__ bool s_last;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double r = block_sum_f64<512>(v[q], sh);
+        if (threadIdx.x == 0) partials[q * kPcgBlocks + blockIdx.x] = r;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 512) a += ((volatile double*)partials)[q * kPcgBlocks + b];
+        out[q] = block_sum_f64<512>(a, sh);
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;  // out[] valid in thread 0
+}
+
+#define NAT_TILE_LOOP_BEGIN                                                                   \
+    const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;      \
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {                               \
+        const uint32_t key = tiles[t];                                                        \
+        const int i = 8 * (key % D.tx) + li, j = 8 * ((key / D.tx) % D.ty) + lj,             \
+                  k = 8 * (key / (D.tx * D.ty)) + lk;                                         \
+        const uint32_t s = (key << 9) | threadIdx.x;                                          \
+        (void)i; (void)j; (void)k;
+#define NAT_TILE_LOOP_END }
+
+// divergence -> b = -div; PCG start x = 0, r = b, p = z = D^-1 r
+__global__ void __launch_bounds__(512) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
+                                                        NatDims D, const float* __restrict__ u, const float* __restrict__ v,
+                                                        const float* __restrict__ w, const uint8_t* __restrict__ type,
+                                                        float* __restrict__ bv, float* __restrict__ x, float* __restrict__ r,
+                                                        float* __restrict__ p, float* __restrict__ dinv, PcgState* st,
+                                                        double* partials) {
+    __shared__ double sh[32];
+    const uint32_t ntiles = *d_ntiles;
+    double bb = 0.0, rz = 0.0;
+    NAT_TILE_LOOP_BEGIN
+    float b = 0.0f, di = 0.0f;
+    if (type[s] == kFluid) {
+        float up = (i + 1 < D.nx) ? u[nslot(i + 1, j, k, D)] : 0.0f;
+        float vp = (j + 1 < D.ny) ? v[nslot(i, j + 1, k, D)] : 0.0f;
+        float wp = (k + 1 < D.nz) ? w[nslot(i, j, k + 1, D)] : 0.0f;
+        float div = ((up - u[s]) + (vp - v[s])) + (wp - w[s]);
+        b = -div;
+        int dcount = 0;
+        dcount += nat_type(type, i - 1, j, k, D) != kSolid;
+        dcount += nat_type(type, i + 1, j, k, D) != kSolid;
+        dcount += nat_type(type, i, j - 1, k, D) != kSolid;
+        dcount += nat_type(type, i, j + 1, k, D) != kSolid;
+        dcount += nat_type(type, i, j, k - 1, D) != kSolid;
+        dcount += nat_type(type, i, j, k + 1, D) != kSolid;
+        di = dcount ? 1.0f / (float)dcount : 0.0f;
+    }
+    float z = b * di;
+    bv[s] = b; x[s] = 0.0f; r[s] = b; p[s] = z; dinv[s] = di;
+    bb += (double)b * (double)b;
+    rz += (double)b * (double)z;
+    NAT_TILE_LOOP_END
+    double vals[2] = {bb, rz}, out[2];
+    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->bb = out[0];
+        st->rz = out[1];
+        st->rz_prev = out[1];
+        st->rr = out[0];
+        st->iter = 0;
+        st->pending = 0;
+        st->done = (out[0] == 0.0) ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(512) pcg_matvec_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
+                                                          NatDims D, const float* __restrict__ p, const uint8_t* __restrict__ type,
+                                                          float* __restrict__ q, PcgState* st, double* partials) {
+    if (st->done) return;
+    __shared__ double sh[32];
+    const uint32_t ntiles = *d_ntiles;
+    double pq = 0.0;
+    NAT_TILE_LOOP_BEGIN
+    float qq = (type[s] == kFluid) ? nat_apply_A(p, type, i, j, k, s, D) : 0.0f;
+    q[s] = qq;
+    pq += (double)p[s] * (double)qq;
+    NAT_TILE_LOOP_END
+    double vals[1] = {pq}, out[1];
+    if (last_block_reduce<1>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->pq = out[0];
+        if (out[0] > 0.0) st->alpha = st->rz / out[0];
+        else { st->alpha = 0.0; st->done = 3; }  // breakdown
+    }
+}
+
+__global__ void __launch_bounds__(512) pcg_update_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
+                                                          NatDims D, float* __restrict__ x, float* __restrict__ r,
+                                                          const float* __restrict__ p, const float* __restrict__ q,
+                                                          const float* __restrict__ dinv, PcgState* st, double* partials) {
+    if (st->done) return;
+    __shared__ double sh[32];
+    const uint32_t ntiles = *d_ntiles;
+    const float a = (float)st->alpha;
+    double rr = 0.0, rz = 0.0;
+    NAT_TILE_LOOP_BEGIN
+    float xs = fmaf(a, p[s], x[s]);
+    float rs = fmaf(-a, q[s], r[s]);
+    x[s] = xs;
+    r[s] = rs;
+    float z = rs * dinv[s];
+    rr += (double)rs * (double)rs;
+    rz += (double)rs * (double)z;
+    NAT_TILE_LOOP_END
+    double vals[2] = {rr, rz}, out[2];
+    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->iter += 1;
+        st->rr = out[0];
+        st->rz_prev = st->rz;
+        st->rz = out[1];
+        st->beta = st->rz / st->rz_prev;
+        if (out[0] <= st->tol2 * st->bb) st->pending = 1;  // confirm with the true residual
+        else if (st->iter >= st->max_iter) st->done = 2;
+    }
+}
+
+// true residual r = b - A x in FP64 every `true_every` iterations and
+// whenever the recursive residual claims convergence
+__global__ void __launch_bounds__(512) pcg_true_residual_kernel(const uint32_t* __restrict__ tiles,
+                                                                 const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                                 const float* __restrict__ x, const float* __restrict__ bv,
+                                                                 float* __restrict__ r, const float* __restrict__ dinv,
+                                                                 const uint8_t* __restrict__ type, PcgState* st,
+                                                                 double* partials) {
+    if (st->done) return;
+    if (!st->pending && (st->true_every <= 0 || (st->iter % st->true_every) != 0)) return;
+    __shared__ double sh[32];
+    const uint32_t ntiles = *d_ntiles;
+    double rr = 0.0, rz = 0.0;
+    NAT_TILE_LOOP_BEGIN
+    double res = 0.0;
+    if (type[s] == kFluid) res = (double)bv[s] - nat_apply_A_f64(x, type, i, j, k, s, D);
+    float rs = (float)res;
+    r[s] = rs;
+    rr += res * res;
+    rz += (double)rs * (double)(rs * dinv[s]);
+    NAT_TILE_LOOP_END
+    double vals[2] = {rr, rz}, out[2];
+    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->rr = out[0];
+        st->rz = out[1];
+        st->beta = st->rz / st->rz_prev;
+        st->rr_true = out[0];
+        st->true_checks += 1;
+        if (out[0] <= st->tol2 * st->bb) st->done = 1;
+        else if (st->iter >= st->max_iter) st->done = 2;
+        st->pending = 0;
+    }
+}
+
+__global__ void __launch_bounds__(512) pcg_direction_kernel(const uint32_t* __restrict__ tiles,
+                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                             const float* __restrict__ r, const float* __restrict__ dinv,
+                                                             float* __restrict__ p, PcgState* st) {
+    if (st->done) return;
+    const uint32_t ntiles = *d_ntiles;
+    const float beta = (float)st->beta;
+    NAT_TILE_LOOP_BEGIN
+    p[s] = fmaf(beta, p[s], r[s] * dinv[s]);
+    NAT_TILE_LOOP_END
+}
+
+// --------------------------------------------------------- projection
+__global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_count,
+                                                           NatDims D, const float* __restrict__ phi,
+                                                           const uint8_t* __restrict__ type, float* __restrict__ u,
+                                                           float* __restrict__ v, float* __restrict__ w) {
+    const uint32_t ntiles = *d_count;
+    float* U[3] = {u, v, w};
+    NAT_TILE_LOOP_BEGIN
+    const uint8_t tb = type[s];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        int ia = i - (c == 0), ja = j - (c == 1), ka = k - (c == 2);
+        uint8_t ta = nat_type(type, ia, ja, ka, D);
+        if (ta == kSolid || tb == kSolid) continue;
+        if (ta != kFluid && tb != kFluid) continue;
+        float pb = (tb == kFluid) ? phi[s] : 0.0f;
+        float pa = (ta == kFluid) ? phi[nslot(ia, ja, ka, D)] : 0.0f;
+        U[c][s] -= (pb - pa);
+    }
+    NAT_TILE_LOOP_END
+}
+
+// ------------------------------------------------------- G2P + advect
+// FLIP/PIC blend of the grid velocity change, then RK2 (midpoint) through the
+// projected grid velocity; positions clamped inside the box.
+__global__ void __launch_bounds__(256) nat_g2p_kernel(uint64_t n, NatDims D, float dt, float flip,
+                                                       const float* __restrict__ u, const float* __restrict__ v,
+                                                       const float* __restrict__ w, const float* __restrict__ ou,
+                                                       const float* __restrict__ ov, const float* __restrict__ ow,
+                                                       float* __restrict__ px, float* __restrict__ py, float* __restrict__ pz,
+                                                       float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float* U[3] = {u, v, w};
+    const float* O[3] = {ou, ov, ow};
+    float X[3] = {px[p], py[p], pz[p]};
+    float V[3] = {vx[p], vy[p], vz[p]};
+    const float o[3] = {D.ox, D.oy, D.oz};
+    const int nn[3] = {D.nx, D.ny, D.nz};
+    float g[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] = __fdiv_rn(__fsub_rn(X[c], o[c]), D.h);
+    float un[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        un[c] = nat_sample(U[c], c, g[0], g[1], g[2], D);
+        float uo = nat_sample(O[c], c, g[0], g[1], g[2], D);
+        float vf = V[c] + (un[c] - uo);
+        V[c] = flip * vf + (1.0f - flip) * un[c];
+    }
+    float gm[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gm[c] = __fdiv_rn(__fsub_rn(fmaf(0.5f * dt, un[c], X[c]), o[c]), D.h);
+    const float eps = 1e-3f * D.h;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float um = nat_sample(U[c], c, gm[0], gm[1], gm[2], D);
+        float xn = fmaf(dt, um, X[c]);
+        float lo = o[c] + eps, hi = o[c] + (float)nn[c] * D.h - eps;
+        X[c] = fminf(fmaxf(xn, lo), hi);
+    }
+    px[p] = X[0]; py[p] = X[1]; pz[p] = X[2];
+    vx[p] = V[0]; vy[p] = V[1]; vz[p] = V[2];
+}
+
+// ----------------------------------------------------------- launchers
+static inline unsigned nb(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int nat_launch_keys(const float* px, const float* py, const float* pz, uint64_t n, const NatDims& D, uint32_t* keys,
+                    cudaStream_t s) {
+    if (n) nat_keys_kernel<<<nb(n, 256), 256, 0, s>>>(px, py, pz, n, D, keys);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src, float* const* dst, cudaStream_t s) {
+    if (n)
+        nat_gather_kernel<<<nb(n, 256), 256, 0, s>>>(perm, n, src[0], src[1], src[2], src[3], src[4], src[5], dst[0], dst[1],
+                                                     dst[2], dst[3], dst[4], dst[5]);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
+                   const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
+                   uint8_t* type, int grid, cudaStream_t s) {
+    nat_p2g_kernel<<<grid, kP2GThreads, 0, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0], vs[1], vs[2], D,
+                                                m[0], m[1], m[2], w[0], w[1], w[2], type);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
+                              uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s) {
+    nat_dilate_kernel<<<grid, 256, 0, s>>>(tile_keys, d_ntiles, D, flags);
+    nat_compact_kernel<<<1, kCompactThreads, 0, s>>>(flags, (uint32_t)(D.tx * D.ty * D.tz), list, d_count);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s) {
+    nat_apply_solids_kernel<<<nb(nslots, 256), 256, 0, s>>>(solid, type, nslots);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s) {
+    uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    nat_mask_to_tiles_kernel<<<nb(nc, 256), 256, 0, s>>>(lin, D, tiled);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
+                         const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s) {
+    nat_normalize_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, gdt, m[0], m[1], m[2], w[0], w[1], w[2], o[0], o[1], o[2], type);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
+                        const uint8_t* type, PcgBuffers& B, cudaStream_t s) {
+    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, B.b, B.x, B.r, B.p, B.dinv, B.st,
+                                               B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const uint8_t* type,
+                             PcgBuffers& B, cudaStream_t s) {
+    pcg_matvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.p, type, B.q, B.st, B.partials);
+    pcg_update_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.r, B.p, B.q, B.dinv, B.st, B.partials);
+    pcg_true_residual_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.b, B.r, B.dinv, type, B.st, B.partials);
+    pcg_direction_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.r, B.dinv, B.p, B.st);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const float* phi,
+                       const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
+    nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, type, U[0], U[1], U[2]);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
+                   float* const* P, float* const* V, cudaStream_t s) {
+    if (n)
+        nat_g2p_kernel<<<nb(n, 256), 256, 0, s>>>(n, D, dt, flip, U[0], U[1], U[2], O[0], O[1], O[2], P[0], P[1], P[2], V[0],
+                                                  V[1], V[2]);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+}  // namespace flip

@@ -1,0 +1,56 @@
+// native.cuh -- declarations shared by native.cu and the engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace flip {
+
+// cell types
+constexpr uint8_t kAir = 0, kFluid = 1, kSolid = 2;
+
+// voxel grid of the north-star step: nx*ny*nz voxels (multiples of 8) of size
+// h, tiles of 8^3 voxels
+struct NatDims {
+    int nx, ny, nz;
+    int tx, ty, tz;
+    float ox, oy, oz, h;
+};
+
+// device-resident Jacobi-PCG state (FP64 scalars)
+struct PcgState {
+    double bb, rz, rz_prev, pq, rr, rr_true, alpha, beta, tol2;
+    int iter, done, pending, max_iter, true_every, true_checks;
+    unsigned int ticket;
+    int pad;
+};
+
+constexpr int kPcgBlocks = 592;  // 148 SMs x 4 CTAs of 512 threads
+
+struct PcgBuffers {
+    float *b, *x, *r, *p, *q, *dinv;
+    PcgState* st;
+    double* partials;  // [4][kPcgBlocks]
+};
+
+int nat_launch_keys(const float* px, const float* py, const float* pz, uint64_t n, const NatDims& D, uint32_t* keys,
+                    cudaStream_t s);
+int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src, float* const* dst, cudaStream_t s);
+int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
+                   const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
+                   uint8_t* type, int grid, cudaStream_t s);
+int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
+                              uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s);
+int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s);
+int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s);
+int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
+                         const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s);
+int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
+                        const uint8_t* type, PcgBuffers& B, cudaStream_t s);
+int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const uint8_t* type,
+                             PcgBuffers& B, cudaStream_t s);
+int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const float* phi,
+                       const uint8_t* type, float* const* U, int grid, cudaStream_t s);
+int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
+                   float* const* P, float* const* V, cudaStream_t s);
+
+}  // namespace flip

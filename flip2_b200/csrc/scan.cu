@@ -1,0 +1,213 @@
+// scan.cu -- single-pass prefix sums with decoupled look-back (sm_100a).
+//
+//  * flip_inclusive_scan_u32 replaces cudaParallelPrefixSum
+//    (engine/algorithms/parallelPrefixSumKernels.cu:5-77), a recursive
+//    three-kernel Blelloch scan that allocates and frees its block sums on
+//    every call.  One kernel, one read and one write per element.
+//  * flip_segment_heads fuses markUniqueGridCells, the inclusive scan of the
+//    head flags and mapNodeIndicesToParticles
+//    (engine/algorithms/particleToGridFunctions.cu:303-345) into one pass
+//    over the sorted keys, and leaves the segment count on the device.
+//
+// Tiles of 4096 elements are claimed in launch order through an atomic
+// counter; each publishes (flag, value) in one 64-bit word, so a waiting CTA
+// only ever waits on a resident predecessor.  Waits are bounded.
+#include "common.cuh"
+
+namespace flip {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr unsigned long long kStAgg = 1ull << 62;
+constexpr unsigned long long kStPrefix = 2ull << 62;
+constexpr unsigned long long kStFlags = 3ull << 62;
+
+static inline size_t align_up_s(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct ScanLayout {
+    size_t err, ctr, status, total;
+};
+static ScanLayout scan_layout(uint64_t n) {
+    ScanLayout L;
+    uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    size_t o = 0;
+    L.err = o; o += 16;
+    L.ctr = o; o = align_up_s(o + 16, 256);
+    L.status = o; o = align_up_s(o + sizeof(unsigned long long) * (tiles ? tiles : 1), 256);
+    L.total = o;
+    return L;
+}
+
+__device__ __forceinline__ int pad_idx(int j) { return j + (j >> 5); }
+
+// Decoupled look-back by one thread: publishes the tile aggregate, walks the
+// predecessors and returns the tile's exclusive prefix (u32, wrapping).
+__device__ __forceinline__ uint32_t lookback_u32(unsigned long long* status, uint32_t tile, uint32_t agg, uint32_t* err) {
+    if (tile == 0) {
+        st_relaxed_u64(status, kStPrefix | agg);
+        return 0u;
+    }
+    st_relaxed_u64(status + tile, kStAgg | agg);
+    uint32_t excl = 0;
+    int64_t t = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (t >= 0) {
+        unsigned long long s = ld_relaxed_u64(status + t);
+        unsigned long long f = s & kStFlags;
+        if (f == 0ull) {
+            if (++spins > kSpinLimit) {
+                atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        excl += (uint32_t)s;
+        if (f == kStPrefix) break;
+        --t;
+    }
+    st_relaxed_u64(status + tile, kStPrefix | (uint32_t)(excl + agg));
+    return excl;
+}
+
+template <int MODE>  // 0: plain scan of `in`;  1: segment heads of sorted keys in `in`
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                            uint64_t n, unsigned long long* __restrict__ status,
+                                                            uint32_t* __restrict__ ctr, uint32_t* __restrict__ err,
+                                                            uint32_t* __restrict__ starts, uint32_t* __restrict__ node_keys,
+                                                            uint32_t* __restrict__ d_count) {
+    __shared__ uint32_t s_data[kScanTile + kScanTile / 32];
+    __shared__ uint32_t s_prev_key;
+    __shared__ uint32_t s_tile, s_excl;
+    __shared__ uint32_t s_scan[kScanThreads / 32 + 1];
+    const int tid = threadIdx.x;
+    if (tid == 0) s_tile = atomicAdd(ctr, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * kScanTile;
+    if (MODE == 1 && tid == 0) s_prev_key = (base > 0) ? in[base - 1] : 0u;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int j = i * kScanThreads + tid;
+        uint64_t g = base + j;
+        s_data[pad_idx(j)] = (g < n) ? in[g] : 0u;
+    }
+    __syncthreads();
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+    const int j0 = tid * kScanItems;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        uint32_t x;
+        if (MODE == 0) {
+            x = s_data[pad_idx(j0 + i)];
+        } else {
+            uint64_t g = base + j0 + i;
+            uint32_t k = s_data[pad_idx(j0 + i)];
+            uint32_t kp = (j0 + i == 0) ? s_prev_key : s_data[pad_idx(j0 + i - 1)];
+            x = (g < n) && (g == 0 || k != kp) ? 1u : 0u;
+        }
+        sum += x;
+        v[i] = sum;  // thread-local inclusive
+    }
+    uint32_t agg;
+    uint32_t texcl = block_exclusive_scan<kScanThreads>(sum, s_scan, &agg);
+    if (tid == 0) s_excl = lookback_u32(status, tile, agg, err);
+    __syncthreads();
+    const uint32_t pre = s_excl + texcl;
+    if (MODE == 0) {
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) s_data[pad_idx(j0 + i)] = pre + v[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            int j = i * kScanThreads + tid;
+            uint64_t g = base + j;
+            if (g < n) out[g] = s_data[pad_idx(j)];
+        }
+    } else {
+        // heads: write starts/keys from the thread-blocked view, then the scan
+        uint32_t prevv = pre;
+        uint32_t keys_local[kScanItems];
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) keys_local[i] = s_data[pad_idx(j0 + i)];
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            uint64_t g = base + j0 + i;
+            uint32_t sc = pre + v[i];
+            if (g < n && sc != prevv) {
+                starts[sc - 1] = (uint32_t)g;
+                if (node_keys) node_keys[sc - 1] = keys_local[i];
+            }
+            if (g == n - 1) *d_count = sc;
+            prevv = sc;
+        }
+        if (out) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < kScanItems; ++i) s_data[pad_idx(j0 + i)] = pre + v[i];
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < kScanItems; ++i) {
+                int j = i * kScanThreads + tid;
+                uint64_t g = base + j;
+                if (g < n) out[g] = s_data[pad_idx(j)];
+            }
+        }
+    }
+}
+
+int launch_scan(int mode, const uint32_t* in, uint32_t* out, uint64_t n, void* scratch, size_t bytes, cudaStream_t s,
+                uint32_t* starts, uint32_t* node_keys, uint32_t* d_count) {
+    ScanLayout L = scan_layout(n);
+    if (!scratch || bytes < L.total) {
+        set_error_text("scan: scratch too small");
+        return FLIP_ERR_ARG;
+    }
+    char* S = (char*)scratch;
+    uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    FLIP_CUDA_TRY(cudaMemsetAsync(S, 0, L.status + sizeof(unsigned long long) * tiles, s));
+    uint32_t* err = (uint32_t*)(S + L.err);
+    uint32_t* ctr = (uint32_t*)(S + L.ctr);
+    unsigned long long* st = (unsigned long long*)(S + L.status);
+    if (mode == 0)
+        scan_kernel<0><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, st, ctr, err, nullptr, nullptr, nullptr);
+    else
+        scan_kernel<1><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, st, ctr, err, starts, node_keys, d_count);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+size_t scan_scratch_bytes(uint64_t n) { return scan_layout(n).total; }
+
+}  // namespace flip
+
+using namespace flip;
+
+extern "C" size_t flip_inclusive_scan_scratch_bytes(uint64_t n) { return scan_layout(n).total; }
+
+extern "C" int flip_inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, void* scratch, size_t bytes,
+                                       void* stream) {
+    if (n == 0) return FLIP_OK;
+    if (!in || !out || n >= (1ull << 40)) {
+        set_error_text("flip_inclusive_scan_u32: bad argument");
+        return FLIP_ERR_ARG;
+    }
+    return launch_scan(0, in, out, n, scratch, bytes, as_stream(stream), nullptr, nullptr, nullptr);
+}
+
+extern "C" size_t flip_segment_heads_scratch_bytes(uint64_t n) { return scan_layout(n).total; }
+
+extern "C" int flip_segment_heads(const uint32_t* sorted_keys, uint64_t n, uint32_t* flags_scan, uint32_t* starts,
+                                  uint32_t* node_keys, uint32_t* d_count, void* scratch, size_t bytes, void* stream) {
+    if (!sorted_keys || !starts || !d_count || n >= (1ull << 32)) {
+        set_error_text("flip_segment_heads: bad argument");
+        return FLIP_ERR_ARG;
+    }
+    cudaStream_t s = as_stream(stream);
+    if (n == 0) {
+        FLIP_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint32_t), s));
+        return FLIP_OK;
+    }
+    return launch_scan(1, sorted_keys, flags_scan, n, scratch, bytes, s, starts, node_keys, d_count);
+}

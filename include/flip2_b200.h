@@ -1,0 +1,245 @@
+/*
+ * flip2_b200.h -- C ABI of libflip2_b200.so, a B200 (sm_100a) PIC/FLIP fluid
+ * step that can stand in for the flip2 engine library (libparticles.so).
+ *
+ * Two layers:
+ *   1. Primitive entry points on caller-owned device memory (plain pointers,
+ *      sizes and a cudaStream_t passed as void*).  Each replaces one host
+ *      wrapper of the reference's kernel library; the citation names it.
+ *      Those that need scratch take it from the caller: query the size with
+ *      the matching *_scratch_bytes() function.
+ *   2. An engine handle (flip_*) that owns all particle and grid state and
+ *      mirrors the reference's Particles class (engine/particles.hu:11-95):
+ *      setDomain, initialize, solveFrame and the per-stage methods.
+ *
+ * All functions return a flip_status; none of them exits the process (the
+ * reference's gpuErrchk calls exit(), engine/typedefs.h:12-20).  Device
+ * pointers are never freed by the library unless it allocated them.
+ */
+#ifndef FLIP2_B200_H
+#define FLIP2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FLIP_OK = 0,
+    FLIP_ERR_ARG = 1,           /* bad argument or size                       */
+    FLIP_ERR_CUDA = 2,          /* a CUDA runtime call failed                 */
+    FLIP_ERR_OOM = 3,           /* device allocation failed                   */
+    FLIP_ERR_TIMEOUT = 4,       /* a bounded device wait gave up              */
+    FLIP_ERR_STATE = 5,         /* call out of order (e.g. step before init)  */
+    FLIP_ERR_NOT_CONVERGED = 6, /* pressure solve hit its iteration cap       */
+    FLIP_ERR_DEVICE = 7         /* no usable sm_100 device                    */
+} flip_status;
+
+/* Domain descriptor, field for field the reference's Grid
+ * (engine/grid.hpp:8-38): float corner, uint root-cell counts, float
+ * root-cell size.  A root cell holds 4x4x4 voxels. */
+typedef struct {
+    float negX, negY, negZ;
+    uint32_t sizeX, sizeY, sizeZ;
+    float cellSize;
+} flip_grid;
+
+/* Library version and the status string of the last failure on this thread. */
+const char* flip_version(void);
+const char* flip_status_string(int status);
+
+/* ------------------------------------------------------------------ */
+/* 1. Primitives                                                       */
+/* ------------------------------------------------------------------ */
+
+/* rootCell + cudaFindGridCell (engine/algorithms/particleToGridFunctions.cu:19-45,216-219):
+ * clamp FP64 positions into the box in place and write the linear root-cell
+ * key x + y*sizeX + z*sizeX*sizeY of each particle.  If idx != NULL also
+ * writes idx[i] = i (the sort payload). */
+int flip_ref_keys(double* px, double* py, double* pz, uint64_t n, const flip_grid* grid,
+                  uint32_t* keys, uint32_t* idx, void* stream);
+
+/* Stable LSD radix sort of (u32 key, u32 value) pairs, 8-bit digits,
+ * onesweep passes with decoupled look-back.  Replaces cudaRadixSortUint /
+ * cudaSortParticlesByGridNode (engine/algorithms/radixSortKernels.cu:85-123,
+ * particleToGridFunctions.cu:270-301): with vals_in == NULL the payload is
+ * the index, so vals_out is the reference's reorderedGridIndices
+ * (keys_out[j] == keys_in[vals_out[j]]).  key_bits (1..32) bounds the keys:
+ * every key must be < 2^key_bits.  keys_in may equal keys_out. */
+size_t flip_sort_pairs_scratch_bytes(uint64_t n);
+int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                    uint64_t n, int key_bits, void* scratch, size_t scratch_bytes, void* stream);
+
+/* Inclusive prefix sum of u32 (wrapping), single pass with decoupled
+ * look-back.  Replaces cudaParallelPrefixSum
+ * (engine/algorithms/parallelPrefixSumKernels.cu:54-77).  In place allowed. */
+size_t flip_inclusive_scan_scratch_bytes(uint64_t n);
+int flip_inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, void* scratch, size_t scratch_bytes,
+                            void* stream);
+
+/* Segment heads of sorted keys, fused: replaces cudaMarkUniqueGridCellsAndCount
+ * + cudaMapNodeIndicesToParticles (particleToGridFunctions.cu:303-345).
+ * flags_scan (optional) receives the inclusive scan of the head flags
+ * (the reference's uniqueGridNodeIndices), starts[k] the first index of the
+ * k-th distinct key, node_keys[k] (optional) that key, *d_count (device) the
+ * number of distinct keys.  starts must hold up to n entries. */
+size_t flip_segment_heads_scratch_bytes(uint64_t n);
+int flip_segment_heads(const uint32_t* sorted_keys, uint64_t n, uint32_t* flags_scan, uint32_t* starts,
+                       uint32_t* node_keys, uint32_t* d_count, void* scratch, size_t scratch_bytes, void* stream);
+
+/* zeroYDimArray + getYDimPositionFirstInRow (particleToGridFunctions.cu:347-378):
+ * table[sizeY*sizeZ] of the first root-cell id of each (y,z) row, every
+ * entry initialised to `nodes`. */
+int flip_ref_ydim_rows(const uint32_t* starts, const uint32_t* sorted_keys, uint32_t nodes, const flip_grid* grid,
+                       uint32_t* table, void* stream);
+
+/* getNumberVoxelsUsedPerNode (engine/particles.cu:88-190): per occupied
+ * root cell, the number of used voxels of its 8^3 tile, plus the tile's
+ * 512-bit used mask (64 bytes per node) reused by flip_ref_voxel_ids. */
+int flip_ref_voxel_counts(const uint32_t* starts, const uint32_t* sorted_keys, uint32_t nodes, uint64_t n,
+                          const double* px, const double* py, const double* pz, const flip_grid* grid,
+                          uint32_t* counts, uint32_t* masks, void* stream);
+/* generateVoxelIDs (engine/particles.cu:192-321) from the masks and the
+ * inclusive scan of the counts (nodeIndexUsedVoxels). */
+int flip_ref_voxel_ids(const uint32_t* sorted_keys, uint32_t nodes, const uint32_t* masks,
+                       const uint32_t* node_voxels, const flip_grid* grid, uint32_t* voxel_ids, int8_t* solids,
+                       void* stream);
+
+/* gatherParticleVelsToVoxels for the three axes in one launch
+ * (engine/particles.cu:379-505), FP64, weight sums zero-initialised. */
+int flip_ref_p2g(const uint32_t* starts, const uint32_t* sorted_keys, uint32_t nodes, uint64_t n,
+                 const double* px, const double* py, const double* pz,
+                 const double* vx, const double* vy, const double* vz,
+                 const uint32_t* node_voxels, const uint32_t* voxel_ids, const int8_t* solids,
+                 const flip_grid* grid, double* ux, double* uy, double* uz, void* stream);
+
+/* gatherVoxelVelsToParticles for the three axes (engine/particles.cu:562-662,742-749). */
+int flip_ref_g2p(const uint32_t* starts, const uint32_t* sorted_keys, uint32_t nodes, uint64_t n,
+                 const double* px, const double* py, const double* pz,
+                 const uint32_t* node_voxels, const uint32_t* voxel_ids,
+                 const double* ux, const double* uy, const double* uz, const flip_grid* grid,
+                 double* vx, double* vy, double* vz, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* 2. Engine handle (mirrors class Particles)                          */
+/* ------------------------------------------------------------------ */
+
+typedef struct flip_engine flip_engine;
+
+typedef enum {
+    FLIP_MODE_REFERENCE = 0, /* the reference's math: FP64 state, tent P2G/G2P, PIC,
+                                forward Euler, tile-local red-black SOR            */
+    FLIP_MODE_NATIVE = 1     /* FP32 state, trilinear MAC P2G/G2P, FLIP blend, RK2,
+                                matrix-free Jacobi-PCG with FP64 reductions        */
+} flip_mode;
+
+typedef struct {
+    int32_t mode;                /* flip_mode                                       */
+    float flip_ratio;            /* NATIVE: FLIP/PIC blend (0.95)                   */
+    float gravity_y;             /* NATIVE: -9.8                                    */
+    double pcg_tol;              /* NATIVE: relative residual target (1e-6)         */
+    int32_t pcg_max_iter;        /* NATIVE: iteration cap                           */
+    int32_t pcg_check_every;     /* NATIVE: iterations between convergence reads    */
+    int32_t true_residual_every; /* NATIVE: FP64 r = b - A x recomputation period   */
+    int32_t permute_velocities;  /* REFERENCE: 0 = keep the reference's order (Q5)  */
+    int32_t device;              /* CUDA device ordinal                             */
+    int32_t reserved0;
+    double max_substep_dt;       /* NATIVE: largest sub-step of solveFrame (1/240)  */
+    int32_t reserved[4];
+} flip_params;
+
+/* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */
+void flip_default_params(int mode, flip_params* out);
+
+/* Particles::Particles(uint size) (engine/particles.cu:15-40). */
+int flip_create(uint64_t n, const flip_params* params, void* stream, flip_engine** out);
+/* Particles::setDomain (engine/particles.cu:42-46).  NATIVE needs the voxel
+ * counts 4*sizeX.. to be multiples of 8. */
+int flip_set_domain(flip_engine* e, double nx, double ny, double nz, uint32_t x, uint32_t y, uint32_t z,
+                    double cellSize);
+/* Host upload / download of particle state (CudaVec::upload/download,
+ * engine/cudaVec.cu:75-103).  The _f64 forms take the reference's double
+ * arrays; the _f32 forms float arrays.  Velocities may be NULL. */
+int flip_upload_particles_f64(flip_engine* e, const double* px, const double* py, const double* pz,
+                              const double* vx, const double* vy, const double* vz, uint64_t n);
+int flip_download_particles_f64(flip_engine* e, double* px, double* py, double* pz, double* vx, double* vy,
+                                double* vz, uint64_t n);
+int flip_upload_particles_f32(flip_engine* e, const float* px, const float* py, const float* pz,
+                              const float* vx, const float* vy, const float* vz, uint64_t n);
+int flip_download_particles_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy, float* vz,
+                                uint64_t n);
+/* Optional static solid cells (NATIVE): mask of nx*ny*nz voxels, x fastest. */
+int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uint64_t n_voxels);
+
+/* Per-stage methods of Particles (engine/particles.hu:17-43). */
+int flip_align_particles_to_grid(flip_engine* e);   /* alignParticlesToGrid, particles.cu:48-50    */
+int flip_sort_particles(flip_engine* e);            /* sortParticles, particles.cu:52-78           */
+int flip_generate_voxels(flip_engine* e);           /* generateVoxels, particles.cu:323-368        */
+int flip_particle_vel_to_voxels(flip_engine* e);    /* particleVelToVoxels, particles.cu:500-505   */
+int flip_pressure_solve(flip_engine* e);            /* pressureSolve, particles.cu:507-555         */
+int flip_update_voxel_velocities(flip_engine* e);   /* updateVoxelVelocities, particles.cu:557-560 */
+int flip_voxel_vels_to_particles(flip_engine* e);   /* voxelVelsToParticles, particles.cu:742-749  */
+int flip_advect_particles(flip_engine* e);          /* advectParticles, particles.cu:751-760       */
+int flip_move_solid_particles(flip_engine* e);      /* moveSolidParticles, particles.cu:762-769    */
+int flip_initialize(flip_engine* e);                /* initialize, particles.cu:805-812            */
+int flip_solve_frame(flip_engine* e, double fps);   /* solveFrame, particles.cu:784-803            */
+double flip_get_courant_dt(flip_engine* e);         /* getCourantDt, particles.cu:493-498          */
+/* writePositionsToFile (particles.cu:817-828): "x, y, z" per line. */
+int flip_write_positions_csv(flip_engine* e, const char* path);
+
+/* One fixed-dt step of the whole path (bin, P2G, pressure, projection,
+ * G2P + advection), asynchronous on the engine stream except for the
+ * convergence reads of the pressure solve. */
+int flip_step(flip_engine* e, double dt);
+int flip_sync(flip_engine* e);
+
+/* Buffers for inspection (device pointers lent, not transferred). */
+typedef enum {
+    FLIP_BUF_PX = 0, FLIP_BUF_PY, FLIP_BUF_PZ, FLIP_BUF_VX, FLIP_BUF_VY, FLIP_BUF_VZ,
+    FLIP_BUF_KEYS, FLIP_BUF_PERM, FLIP_BUF_FLAGS, FLIP_BUF_STARTS, FLIP_BUF_YTABLE,
+    FLIP_BUF_NODE_VOXELS, FLIP_BUF_VOXEL_IDS, FLIP_BUF_SOLIDS, FLIP_BUF_UX, FLIP_BUF_UY, FLIP_BUF_UZ,
+    FLIP_BUF_DIVU, FLIP_BUF_P, FLIP_BUF_RES,
+    /* NATIVE dense tile-blocked grids (slot = tile*512 + local voxel) */
+    FLIP_BUF_GRID_U, FLIP_BUF_GRID_V, FLIP_BUF_GRID_W, FLIP_BUF_CELL_TYPE, FLIP_BUF_PRESSURE,
+    FLIP_BUF_TILE_LIST,
+    /* NATIVE grid velocity right after P2G (the FLIP "old" grid) */
+    FLIP_BUF_GRID_U_P2G, FLIP_BUF_GRID_V_P2G, FLIP_BUF_GRID_W_P2G,
+    FLIP_BUF_COUNT
+} flip_buffer;
+/* elem_size: 1, 4 or 8 bytes; count: number of valid elements. */
+int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, uint32_t* elem_size);
+/* Copy a buffer of flip_get_buffer to host memory (bytes <= count*elem_size),
+ * synchronising the engine stream; CudaVec::download (cudaVec.cu:80-86). */
+int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint64_t bytes);
+
+typedef struct {
+    uint32_t nodes;          /* occupied root cells (REFERENCE) / tiles (NATIVE)   */
+    uint32_t voxels;         /* used voxels (REFERENCE) / grid tiles (NATIVE)      */
+    int32_t pressure_iters;  /* last solve                                        */
+    int32_t converged;       /* 1 if the last solve met its tolerance             */
+    double dt;               /* last dt                                           */
+    double residual;         /* last terminating residual (relative for NATIVE)  */
+    double elapsed_time;
+    uint64_t n;
+    uint32_t error_flags;    /* device error word (bit 0: look-back timeout)      */
+    uint32_t launches;       /* kernels this engine launched since creation      */
+} flip_info;
+int flip_get_info(flip_engine* e, flip_info* out);
+/* Per-stage device times of flip_step (CUDA events on the engine stream).
+ * With timing enabled every step synchronises at its end and adds its stage
+ * times to the running totals; flip_get_stage_ms returns the totals (ms) of
+ * FLIP_NUM_STAGES stages: keys, sort, gather, segment heads, grid clear, P2G,
+ * tile dilation, normalise+gravity, PCG setup, PCG iterations, projection,
+ * G2P+advection; and resets them when reset != 0. */
+#define FLIP_NUM_STAGES 12
+int flip_set_timing(flip_engine* e, int enable);
+int flip_get_stage_ms(flip_engine* e, double* ms, int n, int reset);
+const char* flip_last_error(flip_engine* e);
+int flip_destroy(flip_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLIP2_B200_H */

@@ -1,0 +1,124 @@
+"""The north-star step (FLIP_MODE_NATIVE, FP32 state) against the FP64 oracle
+of the same step: trilinear MAC P2G, Jacobi-PCG pressure with FP64
+reductions, projection, FLIP 0.95 blend and RK2 advection.  Tolerances are
+written per quantity below."""
+import numpy as np
+import pytest
+
+import flip2_b200 as F
+from flip2_b200 import scenes
+from oracle import oracle as O
+from tests.util import rel_err, tiled_to_linear
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as T
+    assert T.cuda.is_available()
+    F.lib()
+    return T
+
+
+def native(n, nc, **kw):
+    p = F.default_params(F.MODE_NATIVE, **kw)
+    P = F.Particles(n, mode=F.MODE_NATIVE, params=p)
+    P.setDomain(0.0, 0.0, 0.0, nc // 4, nc // 4, nc // 4, 4.0 / nc)
+    return P
+
+
+@pytest.mark.parametrize("vscale", [0.0, 1.0])
+def test_native_step_vs_fp64_oracle(torch, vscale):
+    nc, dt = 32, 1.0 / 240
+    pos, _ = scenes.dam_break(nc, seed=0)
+    vel = scenes.random_velocities(pos.shape[0], seed=7, scale=vscale)
+    P = native(pos.shape[0], nc)
+    P.upload(pos, vel)
+    P.step(dt)
+    info = P.info()
+    perm = P.read(F.BUF_PERM)
+    Po = O.nat_params(nc, nc, nc, 1.0 / nc, dt=dt)
+    ref = O.nat_step(pos, vel, Po)
+    # cell classification: bit-exact
+    typ = tiled_to_linear(P.read(F.BUF_CELL_TYPE, np.uint8), nc, nc, nc)
+    assert int((typ == 1).sum()) == ref["fluid_cells"]
+    # P2G grids (FP32 accumulation vs FP64): 2e-6 of the largest face velocity
+    if vscale > 0:
+        for which, key in ((F.BUF_GRID_U_P2G, "u"), (F.BUF_GRID_V_P2G, "v"), (F.BUF_GRID_W_P2G, "w")):
+            g = tiled_to_linear(P.read(which, np.float32), nc, nc, nc)
+            assert rel_err(g, ref[key]) < 2e-6, key
+    # pressure: converged to the relative residual target, measured by the
+    # FP64 oracle operator on the FP64 right-hand side
+    assert info.converged == 1
+    assert info.residual <= 1e-6
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE, np.float32), nc, nc, nc).astype(np.float64)
+    assert rel_err(phi, ref["phi"]) < 2e-3
+    assert abs(info.pressure_iters - ref["iters"]) <= max(3, ref["iters"] // 10)
+    # particles (GPU order is sorted: particle j is input particle perm[j])
+    pg, vg = P.download()
+    po, vo = ref["pos"][perm], ref["vel"][perm]
+    h = 1.0 / nc
+    assert np.max(np.abs(pg - po)) < 1e-3 * h
+    assert rel_err(vg, vo, floor=1.0) < 2e-3
+    P.close()
+
+
+def test_native_twenty_steps(torch):
+    nc, dt = 32, 1.0 / 240
+    pos, vel = scenes.dam_break(nc, seed=0)
+    P = native(pos.shape[0], nc)
+    P.upload(pos, vel)
+    for _ in range(20):
+        P.step(dt)
+        info = P.info()
+        assert info.converged == 1 and info.residual <= 1e-6
+        assert info.error_flags == 0
+    pg, vg = P.download()
+    assert np.all(np.isfinite(pg)) and np.all(np.isfinite(vg))
+    assert pg.min() > 0.0 and pg.max() < 1.0
+    # the block falls and spreads: centre of mass goes down, mean vy < 0
+    assert pg[:, 1].mean() < pos[:, 1].mean()
+    assert vg[:, 1].mean() < 0.0
+    P.close()
+
+
+def test_native_solid_sphere(torch):
+    """Interior solid cells (the learned-preconditioner problems carry solid
+    spheres): faces touching solid cells stay zero, the solve converges, and
+    the result matches the oracle run with the same mask."""
+    nc, dt = 32, 1.0 / 240
+    pos, _ = scenes.dam_break(nc, block=(1.0, 0.5, 1.0), seed=3)
+    vel = scenes.random_velocities(pos.shape[0], seed=4, scale=0.5)
+    k, j, i = np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij")
+    c = (np.stack([i, j, k], -1) + 0.5) / nc
+    solid = (np.sum((c - np.array([0.5, 0.25, 0.5])) ** 2, -1) < 0.15 ** 2).astype(np.uint8).ravel()
+    P = native(pos.shape[0], nc)
+    P.set_solid_mask(solid)
+    P.upload(pos, vel)
+    P.step(dt)
+    info = P.info()
+    assert info.converged == 1
+    Po = O.nat_params(nc, nc, nc, 1.0 / nc, dt=dt)
+    ref = O.nat_step(pos, vel, Po, solid=solid)
+    typ = tiled_to_linear(P.read(F.BUF_CELL_TYPE, np.uint8), nc, nc, nc)
+    assert np.array_equal(typ == 2, solid == 1)
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE, np.float32), nc, nc, nc).astype(np.float64)
+    assert rel_err(phi, ref["phi"]) < 2e-3
+    u = tiled_to_linear(P.read(F.BUF_GRID_U, np.float32), nc, nc, nc)
+    solid3 = solid.reshape(nc, nc, nc)
+    s_b = solid3.ravel() == 1
+    s_a = np.roll(solid3, 1, axis=2).ravel() == 1
+    assert np.all(u[s_b | s_a] == 0.0)
+    P.close()
+
+
+def test_native_engine_errors(torch):
+    P = F.Particles(64, mode=F.MODE_NATIVE)
+    with pytest.raises(F.FlipError) as ei:
+        P.step(0.01)
+    assert ei.value.status == 5
+    with pytest.raises(F.FlipError) as ei:
+        P.setDomain(0, 0, 0, 3, 4, 4, 0.25)  # 12 voxels: not a multiple of 8
+    assert ei.value.status == 1
+    P.close()
