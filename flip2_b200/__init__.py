@@ -89,6 +89,8 @@ def lib():
         "flip_ref_voxel_ids": (i32, [vp, u32, vp, vp, gp, vp, vp, vp]),
         "flip_ref_p2g": (i32, [vp, vp, u32, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, gp, vp, vp, vp, vp]),
         "flip_ref_g2p": (i32, [vp, vp, u32, u64, vp, vp, vp, vp, vp, vp, vp, vp, gp, vp, vp, vp, vp]),
+        "flip_ref_getmax_scratch_bytes": (sz, [u64]),
+        "flip_ref_getmax_f64": (i32, [vp, u64, i32, vp, sz, C.POINTER(d), vp]),
         "flip_default_params": (None, [i32, C.POINTER(Params)]),
         "flip_create": (i32, [u64, C.POINTER(Params), vp, C.POINTER(vp)]),
         "flip_set_domain": (i32, [vp, d, d, d, u32, u32, u32, d]),

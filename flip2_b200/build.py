@@ -76,6 +76,15 @@ def build(verbose=False, extra=()):
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError("link failed:\n" + r.stderr[-4000:])
+    drv_src = os.path.join(HERE, "driver", "main.cpp")
+    drv = os.path.join(LIBDIR, "flip2_main")
+    if os.path.exists(drv_src) and (_stale(drv, [drv_src, lib] + _headers()) or extra):
+        cmd = [nvcc(), "-O2", "-std=c++17", "-x", "cu"] + ARCH + ["-I" + os.path.join(ROOT, "include"), drv_src,
+                                                                   "-o", drv, "-L" + LIBDIR, "-lflip2_b200",
+                                                                   "-Xlinker", "-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("driver build failed:\n" + r.stderr[-4000:])
     return lib
 
 

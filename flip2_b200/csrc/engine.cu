@@ -238,8 +238,10 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         add((void**)&e->type, e->nslots);
         add((void**)&e->tile_flags, e->ntiles_total);
         add((void**)&e->grid_tiles, 4 * e->ntiles_total);
-        float** pv[6] = {&e->pcg.b, &e->pcg.x, &e->pcg.r, &e->pcg.p, &e->pcg.q, &e->pcg.dinv};
+        float** pv[5] = {&e->pcg.b, &e->pcg.r, &e->pcg.p0, &e->pcg.p1, &e->pcg.q};
         for (float** q : pv) add((void**)q, 4 * e->nslots);
+        add((void**)&e->pcg.x, 8 * e->nslots);
+        add((void**)&e->pcg.cell, e->nslots);
         add((void**)&e->pcg.st, sizeof(PcgState));
         add((void**)&e->pcg.partials, sizeof(double) * 4 * kPcgBlocks);
     }
@@ -580,6 +582,7 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
         E_CUDA(cudaMemsetAsync(e->w[c], 0, fb, e->stream));
     }
     E_CUDA(cudaMemsetAsync(e->type, 0, e->nslots, e->stream));
+    E_CUDA(cudaMemsetAsync(e->pcg.cell, 0, e->nslots, e->stream));
     E_CUDA(cudaMemsetAsync(e->tile_flags, 0, e->ntiles_total, e->stream));
     E_TRY(e->mark(5));
     E_TRY(nat_launch_p2g(e->node_keys, e->starts, e->d_counts, e->n, (const float* const*)e->fp,
@@ -604,7 +607,8 @@ static int nat_pcg_graph(flip_engine* e, int iters) {
     E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = FLIP_OK;
     for (int k = 0; k < iters && rc == FLIP_OK; ++k)
-        rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->type, e->pcg, e->stream);
+        rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+    if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     E_CUDA(ce);
@@ -620,6 +624,7 @@ static int nat_pressure(flip_engine* e) {
     init.tol2 = e->P.pcg_tol * e->P.pcg_tol;
     init.max_iter = e->P.pcg_max_iter;
     init.true_every = e->P.true_residual_every;
+    init.next_check = e->P.true_residual_every;
     *e->h_state = init;
     E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
     E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, (const float* const*)e->m, e->type, e->pcg, e->stream));
@@ -630,7 +635,7 @@ static int nat_pressure(flip_engine* e) {
     int launched = 0;
     for (;;) {
         E_CUDA(cudaGraphLaunch(e->pcg_graph, e->stream));
-        e->launches += 4u * (uint32_t)chunk;
+        e->launches += 2u * (uint32_t)chunk + 1u;
         launched += chunk;
         E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
         E_CUDA(cudaStreamSynchronize(e->stream));
@@ -851,13 +856,13 @@ extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64
     case FLIP_BUF_UY: p = ref ? (void*)e->uy : (void*)e->m[1]; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
     case FLIP_BUF_UZ: p = ref ? (void*)e->uz : (void*)e->m[2]; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
     case FLIP_BUF_DIVU: p = ref ? (void*)e->divU : (void*)e->pcg.b; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
-    case FLIP_BUF_P: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_P: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = 8; break;
     case FLIP_BUF_RES: p = ref ? (void*)e->res : (void*)e->pcg.r; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
     case FLIP_BUF_GRID_U: p = e->m[0]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_GRID_V: p = e->m[1]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_GRID_W: p = e->m[2]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_CELL_TYPE: p = e->type; c = ref ? 0 : e->nslots; es = 1; break;
-    case FLIP_BUF_PRESSURE: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = ref ? 8 : 4; break;
+    case FLIP_BUF_PRESSURE: p = ref ? (void*)e->p : (void*)e->pcg.x; c = ref ? e->voxels : e->nslots; es = 8; break;
     case FLIP_BUF_TILE_LIST: p = e->node_keys; c = ref ? 0 : e->nodes; break;
     case FLIP_BUF_GRID_U_P2G: p = e->o[0]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_GRID_V_P2G: p = e->o[1]; c = ref ? 0 : e->nslots; break;

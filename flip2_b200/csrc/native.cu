@@ -250,36 +250,9 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
 }
 
 // ---------------------------------------------------------------- PCG
-// q = A p on fluid cells: A has diagonal = number of non-solid neighbours and
-// -1 for each fluid neighbour (air neighbours are Dirichlet zero).
-__device__ __forceinline__ float nat_apply_A(const float* __restrict__ x, const uint8_t* __restrict__ type, int i, int j,
-                                             int k, uint32_t s, const NatDims& D) {
-    const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-    float d = 0.0f, sum = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        int a = i + oi[q], b = j + oj[q], c = k + ok[q];
-        uint8_t t = nat_type(type, a, b, c, D);
-        if (t == kSolid) continue;
-        d += 1.0f;
-        if (t == kFluid) sum += __ldg(x + nslot(a, b, c, D));
-    }
-    return fmaf(d, x[s], -sum);
-}
-__device__ __forceinline__ double nat_apply_A_f64(const float* __restrict__ x, const uint8_t* __restrict__ type, int i, int j,
-                                                  int k, uint32_t s, const NatDims& D) {
-    const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-    double d = 0.0, sum = 0.0;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        int a = i + oi[q], b = j + oj[q], c = k + ok[q];
-        uint8_t t = nat_type(type, a, b, c, D);
-        if (t == kSolid) continue;
-        d += 1.0;
-        if (t == kFluid) sum += (double)x[nslot(a, b, c, D)];
-    }
-    return d * (double)x[s] - sum;
-}
+// Jacobi-preconditioned CG on A phi = -div over fluid cells: A has the
+// number of non-solid neighbours on the diagonal and -1 for each fluid
+// neighbour (air neighbours are Dirichlet zero, solid ones Neumann).
 
 // last CTA to finish sums the per-CTA partials (fixed order: deterministic)
 template <int NV>
@@ -317,61 +290,96 @@ __device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* parti
         (void)i; (void)j; (void)k;
 #define NAT_TILE_LOOP_END }
 
-// divergence -> b = -div; PCG start x = 0, r = b, p = z = D^-1 r
+__device__ __forceinline__ float jacobi_inv(uint8_t c) {
+    uint32_t d = c & 7u;
+    return d ? __frcp_rn((float)d) : 0.0f;
+}
+
+// divergence -> b = -div; cell codes; x = 0, r = b, p = 0 (the first
+// direction update turns p into D^-1 r)
 __global__ void __launch_bounds__(512) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
-                                                        float* __restrict__ bv, float* __restrict__ x, float* __restrict__ r,
-                                                        float* __restrict__ p, float* __restrict__ dinv, PcgState* st,
-                                                        double* partials) {
+                                                        PcgBuffers B) {
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
     double bb = 0.0, rz = 0.0;
     NAT_TILE_LOOP_BEGIN
-    float b = 0.0f, di = 0.0f;
+    float b = 0.0f;
+    uint8_t code = 0;
     if (type[s] == kFluid) {
         float up = (i + 1 < D.nx) ? u[nslot(i + 1, j, k, D)] : 0.0f;
         float vp = (j + 1 < D.ny) ? v[nslot(i, j + 1, k, D)] : 0.0f;
         float wp = (k + 1 < D.nz) ? w[nslot(i, j, k + 1, D)] : 0.0f;
         float div = ((up - u[s]) + (vp - v[s])) + (wp - w[s]);
         b = -div;
-        int dcount = 0;
+        uint32_t dcount = 0;
         dcount += nat_type(type, i - 1, j, k, D) != kSolid;
         dcount += nat_type(type, i + 1, j, k, D) != kSolid;
         dcount += nat_type(type, i, j - 1, k, D) != kSolid;
         dcount += nat_type(type, i, j + 1, k, D) != kSolid;
         dcount += nat_type(type, i, j, k - 1, D) != kSolid;
         dcount += nat_type(type, i, j, k + 1, D) != kSolid;
-        di = dcount ? 1.0f / (float)dcount : 0.0f;
+        code = (uint8_t)(kCellFluid | dcount);
     }
-    float z = b * di;
-    bv[s] = b; x[s] = 0.0f; r[s] = b; p[s] = z; dinv[s] = di;
+    B.cell[s] = code;
+    B.b[s] = b;
+    B.x[s] = 0.0;
+    B.r[s] = b;
+    B.p0[s] = 0.0f;
+    const float z = b * jacobi_inv(code);
     bb += (double)b * (double)b;
     rz += (double)b * (double)z;
     NAT_TILE_LOOP_END
     double vals[2] = {bb, rz}, out[2];
-    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+    if (last_block_reduce<2>(vals, B.partials, &B.st->ticket, sh, out) && threadIdx.x == 0) {
+        PcgState* st = B.st;
         st->bb = out[0];
         st->rz = out[1];
         st->rz_prev = out[1];
         st->rr = out[0];
+        st->beta = 0.0;
+        st->pcur = 0;
         st->iter = 0;
         st->pending = 0;
         st->done = (out[0] == 0.0) ? 1 : 0;
     }
 }
 
-__global__ void __launch_bounds__(512) pcg_matvec_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
-                                                          NatDims D, const float* __restrict__ p, const uint8_t* __restrict__ type,
-                                                          float* __restrict__ q, PcgState* st, double* partials) {
-    if (st->done) return;
+// fused: p' = D^-1 r + beta p at the cell and its six neighbours, q = A p',
+// partial p'.q; p' goes to the other p buffer (neighbours still read p)
+__global__ void __launch_bounds__(512) pcg_dirmatvec_kernel(const uint32_t* __restrict__ tiles,
+                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                             const float* __restrict__ r, float* p0, float* p1,
+                                                             const uint8_t* __restrict__ cell, float* __restrict__ q,
+                                                             PcgState* st, double* partials) {
+    if (st->done || st->pending) return;
+    const float* __restrict__ p = st->pcur ? p1 : p0;
+    float* __restrict__ pn = st->pcur ? p0 : p1;
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
+    const float beta = (float)st->beta;
     double pq = 0.0;
     NAT_TILE_LOOP_BEGIN
-    float qq = (type[s] == kFluid) ? nat_apply_A(p, type, i, j, k, s, D) : 0.0f;
-    q[s] = qq;
-    pq += (double)p[s] * (double)qq;
+    const uint8_t c = cell[s];
+    float pc = 0.0f, qc = 0.0f;
+    if (c & kCellFluid) {
+        pc = fmaf(beta, p[s], r[s] * jacobi_inv(c));
+        const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+        float sum = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            const int a = i + oi[m], bb = j + oj[m], cc = k + ok[m];
+            if (a < 0 || bb < 0 || cc < 0 || a >= D.nx || bb >= D.ny || cc >= D.nz) continue;
+            const uint32_t sn = nslot(a, bb, cc, D);
+            const uint8_t cn = __ldg(cell + sn);
+            if (cn & kCellFluid) sum += fmaf(beta, __ldg(p + sn), __ldg(r + sn) * jacobi_inv(cn));
+        }
+        qc = fmaf((float)(c & 7u), pc, -sum);
+    }
+    pn[s] = pc;
+    q[s] = qc;
+    pq += (double)pc * (double)qc;
     NAT_TILE_LOOP_END
     double vals[1] = {pq}, out[1];
     if (last_block_reduce<1>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
@@ -381,27 +389,33 @@ __global__ void __launch_bounds__(512) pcg_matvec_kernel(const uint32_t* __restr
     }
 }
 
+// x += alpha p (FP64), r -= alpha q, partial r.r and r.z
 __global__ void __launch_bounds__(512) pcg_update_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
-                                                          NatDims D, float* __restrict__ x, float* __restrict__ r,
-                                                          const float* __restrict__ p, const float* __restrict__ q,
-                                                          const float* __restrict__ dinv, PcgState* st, double* partials) {
-    if (st->done) return;
+                                                          NatDims D, double* __restrict__ x, float* __restrict__ r,
+                                                          const float* p0, const float* p1, const float* __restrict__ q,
+                                                          const uint8_t* __restrict__ cell, PcgState* st, double* partials) {
+    if (st->done || st->pending) return;
+    const float* __restrict__ p = st->pcur ? p0 : p1;  // the direction the matvec just wrote
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
-    const float a = (float)st->alpha;
+    const double ad = st->alpha;
+    const float a = (float)ad;
     double rr = 0.0, rz = 0.0;
     NAT_TILE_LOOP_BEGIN
-    float xs = fmaf(a, p[s], x[s]);
-    float rs = fmaf(-a, q[s], r[s]);
-    x[s] = xs;
-    r[s] = rs;
-    float z = rs * dinv[s];
-    rr += (double)rs * (double)rs;
-    rz += (double)rs * (double)z;
+    const uint8_t c = cell[s];
+    if (c & kCellFluid) {
+        x[s] = fma(ad, (double)p[s], x[s]);
+        const float rs = fmaf(-a, q[s], r[s]);
+        r[s] = rs;
+        const float z = rs * jacobi_inv(c);
+        rr += (double)rs * (double)rs;
+        rz += (double)rs * (double)z;
+    }
     NAT_TILE_LOOP_END
     double vals[2] = {rr, rz}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->iter += 1;
+        st->pcur ^= 1;
         st->rr = out[0];
         st->rz_prev = st->rz;
         st->rz = out[1];
@@ -411,55 +425,57 @@ __global__ void __launch_bounds__(512) pcg_update_kernel(const uint32_t* __restr
     }
 }
 
-// true residual r = b - A x in FP64 every `true_every` iterations and
-// whenever the recursive residual claims convergence
-__global__ void __launch_bounds__(512) pcg_true_residual_kernel(const uint32_t* __restrict__ tiles,
-                                                                 const uint32_t* __restrict__ d_ntiles, NatDims D,
-                                                                 const float* __restrict__ x, const float* __restrict__ bv,
-                                                                 float* __restrict__ r, const float* __restrict__ dinv,
-                                                                 const uint8_t* __restrict__ type, PcgState* st,
-                                                                 double* partials) {
+// true residual r = b - A x in FP64, run at the end of each launch chunk:
+// when the recursive residual claimed convergence, or every true_every
+// iterations; it replaces r and decides convergence on the true value
+__global__ void __launch_bounds__(512) pcg_check_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
+                                                         NatDims D, const double* __restrict__ x, const float* __restrict__ bv,
+                                                         float* __restrict__ r, const uint8_t* __restrict__ cell,
+                                                         PcgState* st, double* partials) {
     if (st->done) return;
-    if (!st->pending && (st->true_every <= 0 || (st->iter % st->true_every) != 0)) return;
+    if (!st->pending && (st->true_every <= 0 || st->iter < st->next_check)) return;
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
     double rr = 0.0, rz = 0.0;
     NAT_TILE_LOOP_BEGIN
-    double res = 0.0;
-    if (type[s] == kFluid) res = (double)bv[s] - nat_apply_A_f64(x, type, i, j, k, s, D);
-    float rs = (float)res;
-    r[s] = rs;
-    rr += res * res;
-    rz += (double)rs * (double)(rs * dinv[s]);
+    const uint8_t c = cell[s];
+    if (c & kCellFluid) {
+        const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+        double sum = 0.0;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            const int a = i + oi[m], bb = j + oj[m], cc = k + ok[m];
+            if (a < 0 || bb < 0 || cc < 0 || a >= D.nx || bb >= D.ny || cc >= D.nz) continue;
+            const uint32_t sn = nslot(a, bb, cc, D);
+            if (cell[sn] & kCellFluid) sum += x[sn];
+        }
+        const double res = (double)bv[s] - ((double)(c & 7u) * x[s] - sum);
+        const float rs = (float)res;
+        r[s] = rs;
+        rr += res * res;
+        rz += (double)rs * (double)(rs * jacobi_inv(c));
+    }
     NAT_TILE_LOOP_END
     double vals[2] = {rr, rz}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->rr = out[0];
-        st->rz = out[1];
-        st->beta = st->rz / st->rz_prev;
         st->rr_true = out[0];
         st->true_checks += 1;
-        if (out[0] <= st->tol2 * st->bb) st->done = 1;
-        else if (st->iter >= st->max_iter) st->done = 2;
+        st->next_check = st->iter + st->true_every;
+        if (out[0] <= st->tol2 * st->bb) {
+            st->done = 1;
+        } else {
+            st->rz = out[1];
+            st->beta = st->rz / st->rz_prev;
+            if (st->iter >= st->max_iter) st->done = 2;
+        }
         st->pending = 0;
     }
 }
 
-__global__ void __launch_bounds__(512) pcg_direction_kernel(const uint32_t* __restrict__ tiles,
-                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
-                                                             const float* __restrict__ r, const float* __restrict__ dinv,
-                                                             float* __restrict__ p, PcgState* st) {
-    if (st->done) return;
-    const uint32_t ntiles = *d_ntiles;
-    const float beta = (float)st->beta;
-    NAT_TILE_LOOP_BEGIN
-    p[s] = fmaf(beta, p[s], r[s] * dinv[s]);
-    NAT_TILE_LOOP_END
-}
-
 // --------------------------------------------------------- projection
 __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_count,
-                                                           NatDims D, const float* __restrict__ phi,
+                                                           NatDims D, const double* __restrict__ phi,
                                                            const uint8_t* __restrict__ type, float* __restrict__ u,
                                                            float* __restrict__ v, float* __restrict__ w) {
     const uint32_t ntiles = *d_count;
@@ -472,9 +488,9 @@ __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __rest
         uint8_t ta = nat_type(type, ia, ja, ka, D);
         if (ta == kSolid || tb == kSolid) continue;
         if (ta != kFluid && tb != kFluid) continue;
-        float pb = (tb == kFluid) ? phi[s] : 0.0f;
-        float pa = (ta == kFluid) ? phi[nslot(ia, ja, ka, D)] : 0.0f;
-        U[c][s] -= (pb - pa);
+        double pb = (tb == kFluid) ? phi[s] : 0.0;
+        double pa = (ta == kFluid) ? phi[nslot(ia, ja, ka, D)] : 0.0;
+        U[c][s] -= (float)(pb - pa);
     }
     NAT_TILE_LOOP_END
 }
@@ -572,21 +588,24 @@ int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const N
 }
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s) {
-    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, B.b, B.x, B.r, B.p, B.dinv, B.st,
-                                               B.partials);
+    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, B);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const uint8_t* type,
-                             PcgBuffers& B, cudaStream_t s) {
-    pcg_matvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.p, type, B.q, B.st, B.partials);
-    pcg_update_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.r, B.p, B.q, B.dinv, B.st, B.partials);
-    pcg_true_residual_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.b, B.r, B.dinv, type, B.st, B.partials);
-    pcg_direction_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.r, B.dinv, B.p, B.st);
+int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                             cudaStream_t s) {
+    pcg_dirmatvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.st, B.partials);
+    pcg_update_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.r, B.p0, B.p1, B.q, B.cell, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const float* phi,
+int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                         cudaStream_t s) {
+    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st, B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
     nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, type, U[0], U[1], U[2]);
     FLIP_CUDA_TRY(cudaGetLastError());

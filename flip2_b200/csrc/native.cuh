@@ -19,18 +19,28 @@ struct NatDims {
 // device-resident Jacobi-PCG state (FP64 scalars)
 struct PcgState {
     double bb, rz, rz_prev, pq, rr, rr_true, alpha, beta, tol2;
-    int iter, done, pending, max_iter, true_every, true_checks;
+    int iter, done, pending, max_iter, true_every, true_checks, next_check;
+    int pcur;  // which p buffer holds the current direction
     unsigned int ticket;
     int pad;
 };
 
 constexpr int kPcgBlocks = 592;  // 148 SMs x 4 CTAs of 512 threads
 
+// PCG vectors on the tile-blocked slots.  x accumulates in FP64: an FP32
+// solution vector bounds the attainable true residual near eps_32 * cond(A)
+// (2.5e-5 on the 32^3 dam-break), above the 1e-6 target.  r, p, q and the
+// stencil arithmetic stay FP32; every dot product is FP64.
+// cell: bit 7 = fluid, bits 0-2 = number of non-solid neighbours (the
+// Jacobi diagonal), 0 for every other cell.
 struct PcgBuffers {
-    float *b, *x, *r, *p, *q, *dinv;
+    double* x;
+    float *b, *r, *p0, *p1, *q;
+    uint8_t* cell;
     PcgState* st;
     double* partials;  // [4][kPcgBlocks]
 };
+constexpr uint8_t kCellFluid = 0x80;
 
 int nat_launch_keys(const float* px, const float* py, const float* pz, uint64_t n, const NatDims& D, uint32_t* keys,
                     cudaStream_t s);
@@ -46,9 +56,15 @@ int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const N
                          const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s);
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s);
-int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const uint8_t* type,
-                             PcgBuffers& B, cudaStream_t s);
-int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const float* phi,
+// one PCG iteration: fused direction update + matvec (+ p.Ap), then the
+// x/r update (+ r.r, r.z); the two p buffers alternate under device control
+int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                             cudaStream_t s);
+// true residual r = b - A x in FP64 when convergence is claimed or every
+// true_every iterations; decides convergence
+int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                         cudaStream_t s);
+int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const uint8_t* type, float* const* U, int grid, cudaStream_t s);
 int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
                    float* const* P, float* const* V, cudaStream_t s);

@@ -704,3 +704,23 @@ extern "C" int flip_ref_g2p(const uint32_t* starts, const uint32_t* sorted_keys,
     return ref_launch_g2p(starts, sorted_keys, nodes, n, px, py, pz, node_voxels, voxel_ids, ux, uy, uz, *grid, vx, vy, vz,
                           as_stream(stream));
 }
+
+extern "C" size_t flip_ref_getmax_scratch_bytes(uint64_t n) { return 2 * sizeof(double) * (n / 512 + 2); }
+
+extern "C" int flip_ref_getmax_f64(const double* data, uint64_t n, int absolute, void* scratch, size_t scratch_bytes,
+                                   double* result, void* stream) {
+    if (!data || !result || !scratch || scratch_bytes < flip_ref_getmax_scratch_bytes(n)) return FLIP_ERR_ARG;
+    cudaStream_t s = as_stream(stream);
+    double* b0 = (double*)scratch;
+    double* b1 = b0 + (n / 512 + 2);
+    int rc = ref_launch_getmax_level(n, data, b0, absolute, s);
+    if (rc) return rc;
+    for (uint64_t i = n / 512 + 1; i > 1; i = i / 512 + 1) {
+        rc = ref_launch_getmax_level(i, b0, b1, absolute, s);
+        if (rc) return rc;
+        double* t = b0; b0 = b1; b1 = t;
+    }
+    FLIP_CUDA_TRY(cudaMemcpyAsync(result, b0, sizeof(double), cudaMemcpyDeviceToHost, s));
+    FLIP_CUDA_TRY(cudaStreamSynchronize(s));
+    return FLIP_OK;
+}

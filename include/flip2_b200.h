@@ -122,6 +122,13 @@ int flip_ref_g2p(const uint32_t* starts, const uint32_t* sorted_keys, uint32_t n
                  const double* ux, const double* uy, const double* uz, const flip_grid* grid,
                  double* vx, double* vy, double* vz, void* stream);
 
+/* CudaVec<double>::getMax(stream, abs) (engine/cudaVec.cu:173-233) with the
+ * reference's reduction, which compares element t with t+256 of each
+ * 512-element block only; synchronous, result written to *result (host). */
+size_t flip_ref_getmax_scratch_bytes(uint64_t n);
+int flip_ref_getmax_f64(const double* data, uint64_t n, int absolute, void* scratch, size_t scratch_bytes,
+                        double* result, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* 2. Engine handle (mirrors class Particles)                          */
 /* ------------------------------------------------------------------ */

@@ -52,7 +52,7 @@ def test_native_step_vs_fp64_oracle(torch, vscale):
     # FP64 oracle operator on the FP64 right-hand side
     assert info.converged == 1
     assert info.residual <= 1e-6
-    phi = tiled_to_linear(P.read(F.BUF_PRESSURE, np.float32), nc, nc, nc).astype(np.float64)
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE), nc, nc, nc).astype(np.float64)
     assert rel_err(phi, ref["phi"]) < 2e-3
     assert abs(info.pressure_iters - ref["iters"]) <= max(3, ref["iters"] // 10)
     # particles (GPU order is sorted: particle j is input particle perm[j])
@@ -103,7 +103,7 @@ def test_native_solid_sphere(torch):
     ref = O.nat_step(pos, vel, Po, solid=solid)
     typ = tiled_to_linear(P.read(F.BUF_CELL_TYPE, np.uint8), nc, nc, nc)
     assert np.array_equal(typ == 2, solid == 1)
-    phi = tiled_to_linear(P.read(F.BUF_PRESSURE, np.float32), nc, nc, nc).astype(np.float64)
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE), nc, nc, nc).astype(np.float64)
     assert rel_err(phi, ref["phi"]) < 2e-3
     u = tiled_to_linear(P.read(F.BUF_GRID_U, np.float32), nc, nc, nc)
     solid3 = solid.reshape(nc, nc, nc)

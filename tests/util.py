@@ -24,3 +24,38 @@ def rel_err(a, b, floor=0.0):
 def u32(t):
     """torch int32 tensor holding u32 bits -> numpy uint32."""
     return t.cpu().numpy().view(np.uint32)
+
+
+def zapron_race_voxels(b, g):
+    """Voxels whose reference divergence is not deterministic.
+
+    The reference's z-apron copy writes target (tz, y, tz) -- x replaced by z
+    (voxelSolveFunctions.cu:85) -- so up to eight source voxels of one row land
+    on one shared-memory word through plain `+=` from different threads
+    (voxelSolveFunctions.cu:48-93): the surviving sum depends on the warp
+    schedule.  Returns a bool mask over the compacted voxels whose divergence
+    reads such a word."""
+    nv, ids, keys, st, yt = b["node_voxels"], b["voxel_ids"], b["sorted_keys"], b["starts"], b["ytable"]
+    nodes = int(b["nodes"])
+    X, Y = g.sizeX, g.sizeY
+    aff = np.zeros(int(b["voxels"]), bool)
+    for nd in range(nodes):
+        vs = int(nv[nd - 1]) if nd else 0
+        ve = int(nv[nd])
+        cur = int(keys[st[nd]])
+        cy, cz = (cur % (X * Y)) // X, cur // (X * Y)
+        if cz < 1 or yt[(cz - 1) * Y + cy] >= nodes:
+            continue
+        nid = int(yt[(cz - 1) * Y + cy])
+        s0 = int(nv[nid - 1]) if nid else 0
+        src = ids[s0:int(nv[nid])].astype(np.int64)
+        sy, sz = (src % 64) // 8, src // 64
+        t = (sz - 4) + sy * 8 + (sz - 4) * 64
+        t = t[sz >= 4]
+        u, c = np.unique(t, return_counts=True)
+        T = set(u[c >= 2].tolist())
+        if not T:
+            continue
+        v = ids[vs:ve].astype(np.int64)
+        aff[vs:ve] = [(a in T) or (a + 1 in T) or (a + 8 in T) or (a + 64 in T) for a in v]
+    return aff
