@@ -374,9 +374,12 @@ class Particles:
         dt = np.float64 if self.mode == MODE_REFERENCE else np.float32
         P = cols(pos, dt)
         V = cols(vel, dt)
+        n = P[0].size
+        if any(c is not None and c.size != n for c in P + V):
+            raise FlipError(1, "upload: position and velocity columns differ in length")
         ptrs = [c.ctypes.data_as(C.c_void_p) if c is not None else None for c in P + V]
         fn = "flip_upload_particles_f64" if dt == np.float64 else "flip_upload_particles_f32"
-        self._call(fn, *ptrs, self.size)
+        self._call(fn, *ptrs, n)  # the engine rejects n != its size (FLIP_ERR_ARG)
         self._keep = P + V
 
     def upload_ptrs(self, ptrs, f64=False):
