@@ -82,6 +82,7 @@ def lib():
         "flip_sort_pairs": (i32, [vp, vp, vp, vp, u64, i32, vp, sz, vp]),
         "flip_inclusive_scan_scratch_bytes": (sz, [u64]),
         "flip_inclusive_scan_u32": (i32, [vp, vp, u64, vp, sz, vp]),
+        "flip_inclusive_scan_u32_noalloc": (i32, [vp, vp, u64, vp]),
         "flip_segment_heads_scratch_bytes": (sz, [u64]),
         "flip_segment_heads": (i32, [vp, u64, vp, vp, vp, vp, vp, sz, vp]),
         "flip_ref_ydim_rows": (i32, [vp, vp, u32, gp, vp, vp]),

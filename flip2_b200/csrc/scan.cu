@@ -12,6 +12,7 @@
 // Tiles of 4096 elements are claimed in launch order through an atomic
 // counter; each publishes (flag, value) in one 64-bit word, so a waiting CTA
 // only ever waits on a resident predecessor.  Waits are bounded.
+#include <mutex>
 #include "common.cuh"
 
 namespace flip {
@@ -210,4 +211,78 @@ extern "C" int flip_segment_heads(const uint32_t* sorted_keys, uint64_t n, uint3
         return FLIP_OK;
     }
     return launch_scan(1, sorted_keys, flags_scan, n, scratch, bytes, s, starts, node_keys, d_count);
+}
+
+// ---------------------------------------------------------------------------
+// Inclusive scan that allocates nothing.
+//
+// flip_inclusive_scan_u32 asks the caller for scratch, which most callers get
+// from cudaMalloc.  Some callers cannot allocate: a host application that
+// hands this library a fixed device-memory budget and owns every allocation
+// (a DCC plug-in host, say), or a per-frame callback where cudaMalloc's
+// implicit device synchronisation would stall the frame.  This variant keeps
+// its look-back scratch in a file-scope device array instead, so the caller
+// passes only the input and output buffers.
+//
+// The array holds the status words of at most kNoAllocScanMaxTiles tiles of
+// 4096 elements, so n is limited to kNoAllocScanMaxN (2^28) elements; it is
+// 512 KiB plus a 256-byte header on every GPU that loads the library, kept
+// until the process exits.  Every call shares it and it keeps the previous
+// call's contents, so each call first clears the words it will use; two
+// calls whose kernels overlap on the GPU (different streams, or different
+// host threads on one device) race on it and must be serialised by the
+// caller.  The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, with that device current); make that first call
+// before any stream capture.
+namespace flip {
+constexpr uint64_t kNoAllocScanMaxN = 1ull << 28;
+constexpr uint64_t kNoAllocScanMaxTiles = kNoAllocScanMaxN / kScanTile;  // 65536
+constexpr int kNoAllocHeaderWords = 32;                                   // err + tile counter, 256 bytes
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocHeaderWords + kNoAllocScanMaxTiles];
+
+static void* g_noalloc_scan_ptr[kNoAllocMaxDevices];
+static cudaError_t g_noalloc_scan_err[kNoAllocMaxDevices];
+static std::once_flag g_noalloc_scan_once[kNoAllocMaxDevices];
+
+__global__ void noalloc_scan_clear_kernel(unsigned long long* words, uint64_t count) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) words[i] = 0ull;
+}
+}  // namespace flip
+
+extern "C" int flip_inclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint64_t n, void* stream) {
+    using namespace flip;
+    if (n == 0) return FLIP_OK;
+    if (!in || !out) {
+        set_error_text("flip_inclusive_scan_u32_noalloc: null buffer");
+        return FLIP_ERR_ARG;
+    }
+    if (n > kNoAllocScanMaxN) {
+        set_error_text("flip_inclusive_scan_u32_noalloc: n exceeds the maximum of 2^28 elements its static scratch covers;"
+                       " use flip_inclusive_scan_u32 with caller scratch");
+        return FLIP_ERR_ARG;
+    }
+    int dev = 0;
+    FLIP_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error_text("flip_inclusive_scan_u32_noalloc: device ordinal beyond 63");
+        return FLIP_ERR_DEVICE;
+    }
+    std::call_once(g_noalloc_scan_once[dev], [dev] {
+        g_noalloc_scan_err[dev] = cudaGetSymbolAddress(&g_noalloc_scan_ptr[dev], g_noalloc_scan_scratch);
+    });
+    if (g_noalloc_scan_err[dev] != cudaSuccess) return set_cuda_error(g_noalloc_scan_err[dev], "cudaGetSymbolAddress");
+    unsigned long long* words = (unsigned long long*)g_noalloc_scan_ptr[dev];
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    const uint64_t used = kNoAllocHeaderWords + tiles;
+    cudaStream_t s = as_stream(stream);
+    noalloc_scan_clear_kernel<<<(unsigned)((used + 255) / 256), 256, 0, s>>>(words, used);
+    uint32_t* err = (uint32_t*)words;
+    uint32_t* ctr = (uint32_t*)(words + 2);
+    unsigned long long* status = words + kNoAllocHeaderWords;
+    scan_kernel<0><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, status, ctr, err, nullptr, nullptr, nullptr);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
 }

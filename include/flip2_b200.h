@@ -79,6 +79,15 @@ size_t flip_inclusive_scan_scratch_bytes(uint64_t n);
 int flip_inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, void* scratch, size_t scratch_bytes,
                             void* stream);
 
+/* flip_inclusive_scan_u32 for callers that cannot allocate device memory
+ * (no counterpart in the reference): the look-back scratch is a static
+ * device array of the library (512 KiB per GPU, held until exit), so only
+ * in and out are passed.  n <= 2^28, else FLIP_ERR_ARG.  Calls share that
+ * array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on each device resolves the array's address; make it before any
+ * stream capture. */
+int flip_inclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint64_t n, void* stream);
+
 /* Segment heads of sorted keys, fused: replaces cudaMarkUniqueGridCellsAndCount
  * + cudaMapNodeIndicesToParticles (particleToGridFunctions.cu:303-345).
  * flags_scan (optional) receives the inclusive scan of the head flags
