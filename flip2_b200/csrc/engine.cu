@@ -117,7 +117,7 @@ extern "C" void flip_default_params(int mode, flip_params* out) {
     out->pcg_tol = 1e-6;
     out->pcg_max_iter = 5000;
     out->pcg_check_every = 16;
-    out->true_residual_every = 50;
+    out->true_residual_every = 32;
     out->permute_velocities = 0;
     out->device = 0;
     out->max_substep_dt = 1.0 / 240.0;
@@ -238,10 +238,11 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         add((void**)&e->type, e->nslots);
         add((void**)&e->tile_flags, e->ntiles_total);
         add((void**)&e->grid_tiles, 4 * e->ntiles_total);
-        float** pv[5] = {&e->pcg.b, &e->pcg.r, &e->pcg.p0, &e->pcg.p1, &e->pcg.q};
+        float** pv[6] = {&e->pcg.xg, &e->pcg.b, &e->pcg.r, &e->pcg.p0, &e->pcg.p1, &e->pcg.q};
         for (float** q : pv) add((void**)q, 4 * e->nslots);
         add((void**)&e->pcg.x, 8 * e->nslots);
         add((void**)&e->pcg.cell, e->nslots);
+        add((void**)&e->pcg.tcoord, 4 * e->ntiles_total);
         add((void**)&e->pcg.st, sizeof(PcgState));
         add((void**)&e->pcg.partials, sizeof(double) * 4 * kPcgBlocks);
     }
@@ -591,11 +592,12 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
     E_TRY(e->mark(6));
     E_TRY(nat_launch_dilate_compact(e->node_keys, e->d_counts, e->D, e->tile_flags, e->grid_tiles, e->d_counts + 1,
                                     nat_grid(e, 2), e->stream));
+    E_TRY(nat_launch_tile_coords(e->node_keys, e->d_counts, e->D, e->pcg.tcoord, nat_grid(e, 2), e->stream));
     E_TRY(e->mark(7));
     E_TRY(nat_launch_normalize(e->grid_tiles, e->d_counts + 1, e->D, (float)(e->P.gravity_y * dt), e->m,
                                (const float* const*)e->w, e->o, e->type, nat_grid(e, 4), e->stream));
     E_TRY(e->mark(8));
-    e->launches += 1 + (e->has_solid ? 1 : 0) + 2 + 1;
+    e->launches += 1 + (e->has_solid ? 1 : 0) + 3 + 1;
     e->have_voxels = true;
     return FLIP_OK;
 }
@@ -655,7 +657,7 @@ static int nat_step(flip_engine* e, double dt) {
     E_TRY(nat_bin(e));
     E_TRY(nat_p2g_stage(e, dt));
     E_TRY(nat_pressure(e));
-    E_TRY(nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->type, e->m, nat_grid(e, 4), e->stream));
+    E_TRY(nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->pcg.xg, e->type, e->m, nat_grid(e, 4), e->stream));
     E_TRY(e->mark(11));
     E_TRY(nat_launch_g2p(e->n, e->D, (float)dt, e->P.flip_ratio, (const float* const*)e->m, (const float* const*)e->o,
                          e->fp, e->fp + 3, e->stream));
@@ -715,7 +717,7 @@ extern "C" int flip_pressure_solve(flip_engine* e) {
 extern "C" int flip_update_voxel_velocities(flip_engine* e) {
     CHECK_E();
     if (e->P.mode == FLIP_MODE_REFERENCE) return ref_update_vel(e);
-    return nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->type, e->m, nat_grid(e, 4), e->stream);
+    return nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->pcg.xg, e->type, e->m, nat_grid(e, 4), e->stream);
 }
 extern "C" int flip_voxel_vels_to_particles(flip_engine* e) {
     CHECK_E();

@@ -168,6 +168,16 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
     }
 }
 
+// packed coordinates tx | ty << 10 | tz << 20 of each occupied tile
+__global__ void nat_tile_coords_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ d_ntiles,
+                                       NatDims D, uint32_t* __restrict__ coords) {
+    const uint32_t ntiles = *d_ntiles;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+        const uint32_t key = tile_keys[t];
+        coords[t] = (key % D.tx) | (((key / D.tx) % D.ty) << 10) | ((key / (D.tx * D.ty)) << 20);
+    }
+}
+
 // tiles touched by the stencils of occupied tiles: 3x3x3 dilation
 __global__ void nat_dilate_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ d_ntiles, NatDims D,
                                   uint8_t* __restrict__ flags) {
@@ -290,14 +300,18 @@ __device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* parti
         (void)i; (void)j; (void)k;
 #define NAT_TILE_LOOP_END }
 
+// 1/d for d = 0..7 (0 for d = 0), the Jacobi inverse diagonal
+__constant__ float kJacobiInv[8] = {0.0f, 1.0f, 0.5f, 1.0f / 3.0f, 0.25f, 0.2f, 1.0f / 6.0f, 1.0f / 7.0f};
 __device__ __forceinline__ float jacobi_inv(uint8_t c) {
     uint32_t d = c & 7u;
     return d ? __frcp_rn((float)d) : 0.0f;
 }
+// the same values from a per-CTA shared copy (no MUFU, no divergence on the constant bank)
+__device__ __forceinline__ float jacobi_inv_s(const float* tab, uint8_t c) { return tab[c & 7u]; }
 
 // divergence -> b = -div; cell codes; x = 0, r = b, p = 0 (the first
 // direction update turns p into D^-1 r)
-__global__ void __launch_bounds__(512) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
+__global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
                                                         PcgBuffers B) {
@@ -325,6 +339,7 @@ __global__ void __launch_bounds__(512) pcg_init_kernel(const uint32_t* __restric
     B.cell[s] = code;
     B.b[s] = b;
     B.x[s] = 0.0;
+    B.xg[s] = 0.0f;
     B.r[s] = b;
     B.p0[s] = 0.0f;
     const float z = b * jacobi_inv(code);
@@ -340,78 +355,184 @@ __global__ void __launch_bounds__(512) pcg_init_kernel(const uint32_t* __restric
         st->rr = out[0];
         st->beta = 0.0;
         st->pcur = 0;
+        st->flush = 0;
         st->iter = 0;
         st->pending = 0;
         st->done = (out[0] == 0.0) ? 1 : 0;
     }
 }
 
-// fused: p' = D^-1 r + beta p at the cell and its six neighbours, q = A p',
-// partial p'.q; p' goes to the other p buffer (neighbours still read p)
-__global__ void __launch_bounds__(512) pcg_dirmatvec_kernel(const uint32_t* __restrict__ tiles,
-                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
-                                                             const float* __restrict__ r, float* p0, float* p1,
-                                                             const uint8_t* __restrict__ cell, float* __restrict__ q,
-                                                             PcgState* st, double* partials) {
+// fused direction update + matvec, one 8^3 tile at a time: p' = D^-1 r +
+// beta p is computed for the tile and its one-cell halo into shared memory
+// (the halo cells belong to neighbouring tiles, which compute the same values
+// for themselves), then q = A p' is read from shared memory.  p' goes to the
+// other p buffer because neighbouring tiles still read p.  The loads of the
+// next tile (centre and halo, all independent) are issued before the current
+// tile's stencil, so their latency overlaps it.  After a true-residual check
+// this kernel also folds xg into x (no neighbour reads of x happen here).
+__device__ __forceinline__ float dir_value(const float* tab, uint8_t c, float r, float p, float beta) {
+    return (c & kCellFluid) ? fmaf(beta, p, r * jacobi_inv_s(tab, c)) : 0.0f;
+}
+
+struct DirLoads {
+    uint32_t key;
+    float r, p, hr, hp;
+    uint8_t c, hc;
+};
+
+__device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ tcoord,
+                                         uint32_t t, const NatDims& D, const float* __restrict__ r,
+                                         const float* __restrict__ p, const uint8_t* __restrict__ cell, int face, int hx,
+                                         int hy, int hz) {
+    const uint32_t key = tiles[t];
+    L.key = key;
+    const uint32_t s = (key << 9) | threadIdx.x;
+    L.c = cell[s];
+    L.r = r[s];
+    L.p = p[s];
+    L.hc = 0;
+    L.hr = 0.0f;
+    L.hp = 0.0f;
+    if (face < 6) {
+        const uint32_t tc = tcoord[t];
+        const int i = 8 * (int)(tc & 1023u) + hx, j = 8 * (int)((tc >> 10) & 1023u) + hy, k = 8 * (int)(tc >> 20) + hz;
+        if (i >= 0 && j >= 0 && k >= 0 && i < D.nx && j < D.ny && k < D.nz) {
+            const uint32_t sn = nslot(i, j, k, D);
+            L.hc = cell[sn];
+            L.hr = r[sn];
+            L.hp = p[sn];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* __restrict__ tiles,
+                                                                const uint32_t* __restrict__ tcoord,
+                                                                const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                                const float* __restrict__ r, float* p0, float* p1,
+                                                                const uint8_t* __restrict__ cell, float* __restrict__ q,
+                                                                double* __restrict__ x, float* __restrict__ xg,
+                                                                PcgState* st, double* partials) {
     if (st->done || st->pending) return;
     const float* __restrict__ p = st->pcur ? p1 : p0;
     float* __restrict__ pn = st->pcur ? p0 : p1;
+    __shared__ float P[1000];  // 10^3 box: tile + halo, index (x+1) + 10 (y+1) + 100 (z+1)
     __shared__ double sh[32];
+    __shared__ float tab[8];
+    if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
+    __syncthreads();
     const uint32_t ntiles = *d_ntiles;
     const float beta = (float)st->beta;
+    const bool flush = st->flush != 0;
+    const int tid = threadIdx.x;
+    const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
+    const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
+    // halo cell handled by this thread (384 of them: 6 faces x 64)
+    const int face = tid >> 6, e0 = tid & 7, e1 = (tid >> 3) & 7;
+    int hx = 0, hy = 0, hz = 0;  // offsets from the tile origin, -1..8
+    if (face == 0) { hx = -1; hy = e0; hz = e1; }
+    else if (face == 1) { hx = 8; hy = e0; hz = e1; }
+    else if (face == 2) { hx = e0; hy = -1; hz = e1; }
+    else if (face == 3) { hx = e0; hy = 8; hz = e1; }
+    else if (face == 4) { hx = e0; hy = e1; hz = -1; }
+    else if (face == 5) { hx = e0; hy = e1; hz = 8; }
+    const int bh = (hx + 1) + 10 * ((hy + 1) + 10 * (hz + 1));
     double pq = 0.0;
-    NAT_TILE_LOOP_BEGIN
-    const uint8_t c = cell[s];
-    float pc = 0.0f, qc = 0.0f;
-    if (c & kCellFluid) {
-        pc = fmaf(beta, p[s], r[s] * jacobi_inv(c));
-        const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-        float sum = 0.0f;
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            const int a = i + oi[m], bb = j + oj[m], cc = k + ok[m];
-            if (a < 0 || bb < 0 || cc < 0 || a >= D.nx || bb >= D.ny || cc >= D.nz) continue;
-            const uint32_t sn = nslot(a, bb, cc, D);
-            const uint8_t cn = __ldg(cell + sn);
-            if (cn & kCellFluid) sum += fmaf(beta, __ldg(p + sn), __ldg(r + sn) * jacobi_inv(cn));
+    DirLoads cur;
+    uint32_t t = blockIdx.x;
+    if (t < ntiles) dir_load(cur, tiles, tcoord, t, D, r, p, cell, face, hx, hy, hz);
+    for (; t < ntiles; t += gridDim.x) {
+        const uint32_t s = (cur.key << 9) | tid;
+        const uint8_t c = cur.c;
+        const float pc = dir_value(tab, c, cur.r, cur.p, beta);
+        P[bc] = pc;
+        pn[s] = pc;
+        if (face < 6) P[bh] = dir_value(tab, cur.hc, cur.hr, cur.hp, beta);
+        if (flush && (c & kCellFluid)) {
+            x[s] += (double)xg[s];
+            xg[s] = 0.0f;
         }
-        qc = fmaf((float)(c & 7u), pc, -sum);
+        DirLoads nxt;
+        const uint32_t tn = t + gridDim.x;
+        if (tn < ntiles) dir_load(nxt, tiles, tcoord, tn, D, r, p, cell, face, hx, hy, hz);
+        __syncthreads();
+        float qc = 0.0f;
+        if (c & kCellFluid) {
+            const float sum = ((P[bc - 1] + P[bc + 1]) + (P[bc - 10] + P[bc + 10])) + (P[bc - 100] + P[bc + 100]);
+            qc = fmaf((float)(c & 7u), pc, -sum);
+        }
+        q[s] = qc;
+        pq += (double)pc * (double)qc;
+        __syncthreads();
+        cur = nxt;
     }
-    pn[s] = pc;
-    q[s] = qc;
-    pq += (double)pc * (double)qc;
-    NAT_TILE_LOOP_END
     double vals[1] = {pq}, out[1];
     if (last_block_reduce<1>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->pq = out[0];
+        st->flush = 0;
         if (out[0] > 0.0) st->alpha = st->rz / out[0];
         else { st->alpha = 0.0; st->done = 3; }  // breakdown
     }
 }
 
-// x += alpha p (FP64), r -= alpha q, partial r.r and r.z
-__global__ void __launch_bounds__(512) pcg_update_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
-                                                          NatDims D, double* __restrict__ x, float* __restrict__ r,
-                                                          const float* p0, const float* p1, const float* __restrict__ q,
-                                                          const uint8_t* __restrict__ cell, PcgState* st, double* partials) {
-    if (st->done || st->pending) return;
-    const float* __restrict__ p = st->pcur ? p0 : p1;  // the direction the matvec just wrote
-    __shared__ double sh[32];
-    const uint32_t ntiles = *d_ntiles;
-    const double ad = st->alpha;
-    const float a = (float)ad;
-    double rr = 0.0, rz = 0.0;
-    NAT_TILE_LOOP_BEGIN
-    const uint8_t c = cell[s];
-    if (c & kCellFluid) {
-        x[s] = fma(ad, (double)p[s], x[s]);
-        const float rs = fmaf(-a, q[s], r[s]);
-        r[s] = rs;
-        const float z = rs * jacobi_inv(c);
+// xg += alpha p, r -= alpha q, partial r.r and r.z; eight cells per thread
+// per round (two 16-byte quads per array, all loads issued before use)
+__device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const float4& p4, const float4& q4, float4& r4,
+                                         float4& g4, float a, double& rr, double& rz) {
+    float* rv = &r4.x;
+    float* gv = &g4.x;
+    const float* pv = &p4.x;
+    const float* qv = &q4.x;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const uint8_t c = (uint8_t)(c4 >> (8 * m));
+        if (!(c & kCellFluid)) continue;
+        gv[m] = fmaf(a, pv[m], gv[m]);
+        const float rs = fmaf(-a, qv[m], rv[m]);
+        rv[m] = rs;
+        const float z = rs * jacobi_inv_s(tab, c);
         rr += (double)rs * (double)rs;
         rz += (double)rs * (double)z;
     }
-    NAT_TILE_LOOP_END
+}
+
+__global__ void __launch_bounds__(512, 3) pcg_update_kernel(const uint32_t* __restrict__ tiles,
+                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                             float* __restrict__ xg, float* __restrict__ r,
+                                                             const float* p0, const float* p1, const float* __restrict__ q,
+                                                             const uint8_t* __restrict__ cell, PcgState* st,
+                                                             double* partials) {
+    if (st->done || st->pending) return;
+    const float* __restrict__ p = st->pcur ? p0 : p1;  // the direction the matvec just wrote
+    __shared__ double sh[32];
+    __shared__ float tab[8];
+    if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
+    __syncthreads();
+    const uint32_t nquads = *d_ntiles * 128u;
+    const float a = (float)st->alpha;
+    double rr = 0.0, rz = 0.0;
+    const uint32_t stride = gridDim.x * 512u;
+    for (uint32_t qd = blockIdx.x * 512u + threadIdx.x; qd < nquads; qd += 2u * stride) {
+        const uint32_t qe = qd + stride;
+        const bool two = qe < nquads;
+        const uint32_t s0 = (tiles[qd >> 7] << 9) | ((qd & 127u) << 2);
+        const uint32_t s1 = two ? ((tiles[qe >> 7] << 9) | ((qe & 127u) << 2)) : s0;
+        const uint32_t c0 = *reinterpret_cast<const uint32_t*>(cell + s0);
+        const uint32_t c1 = two ? *reinterpret_cast<const uint32_t*>(cell + s1) : 0u;
+        const float4 pa = *reinterpret_cast<const float4*>(p + s0), pb = *reinterpret_cast<const float4*>(p + s1);
+        const float4 qa = *reinterpret_cast<const float4*>(q + s0), qb = *reinterpret_cast<const float4*>(q + s1);
+        float4 ra = *reinterpret_cast<const float4*>(r + s0), rb = *reinterpret_cast<const float4*>(r + s1);
+        float4 ga = *reinterpret_cast<const float4*>(xg + s0), gb = *reinterpret_cast<const float4*>(xg + s1);
+        if (c0) {
+            upd_quad(tab, c0, pa, qa, ra, ga, a, rr, rz);
+            *reinterpret_cast<float4*>(r + s0) = ra;
+            *reinterpret_cast<float4*>(xg + s0) = ga;
+        }
+        if (c1) {
+            upd_quad(tab, c1, pb, qb, rb, gb, a, rr, rz);
+            *reinterpret_cast<float4*>(r + s1) = rb;
+            *reinterpret_cast<float4*>(xg + s1) = gb;
+        }
+    }
     double vals[2] = {rr, rz}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->iter += 1;
@@ -425,37 +546,63 @@ __global__ void __launch_bounds__(512) pcg_update_kernel(const uint32_t* __restr
     }
 }
 
-// true residual r = b - A x in FP64, run at the end of each launch chunk:
-// when the recursive residual claimed convergence, or every true_every
-// iterations; it replaces r and decides convergence on the true value
-__global__ void __launch_bounds__(512) pcg_check_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
-                                                         NatDims D, const double* __restrict__ x, const float* __restrict__ bv,
-                                                         float* __restrict__ r, const uint8_t* __restrict__ cell,
-                                                         PcgState* st, double* partials) {
+// true residual r = b - A (x + xg) in FP64 at the end of a launch chunk: when
+// the recursive residual claimed convergence, or every true_every
+// iterations.  Replaces r, decides convergence on the true value and asks
+// the next direction kernel to fold xg into x.  The FP64 solution of the tile
+// and its halo is staged in shared memory like the matvec.
+__global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __restrict__ tiles,
+                                                            const uint32_t* __restrict__ tcoord,
+                                                            const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                            const double* __restrict__ x, const float* __restrict__ xg,
+                                                            const float* __restrict__ bv, float* __restrict__ r,
+                                                            const uint8_t* __restrict__ cell, PcgState* st,
+                                                            double* partials) {
     if (st->done) return;
     if (!st->pending && (st->true_every <= 0 || st->iter < st->next_check)) return;
+    __shared__ double X[1000];
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
+    const int tid = threadIdx.x;
+    const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
+    const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
+    const int face = tid >> 6, e0 = tid & 7, e1 = (tid >> 3) & 7;
+    int hx = 0, hy = 0, hz = 0;
+    if (face == 0) { hx = -1; hy = e0; hz = e1; }
+    else if (face == 1) { hx = 8; hy = e0; hz = e1; }
+    else if (face == 2) { hx = e0; hy = -1; hz = e1; }
+    else if (face == 3) { hx = e0; hy = 8; hz = e1; }
+    else if (face == 4) { hx = e0; hy = e1; hz = -1; }
+    else if (face == 5) { hx = e0; hy = e1; hz = 8; }
+    const int bh = (hx + 1) + 10 * ((hy + 1) + 10 * (hz + 1));
     double rr = 0.0, rz = 0.0;
-    NAT_TILE_LOOP_BEGIN
-    const uint8_t c = cell[s];
-    if (c & kCellFluid) {
-        const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-        double sum = 0.0;
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            const int a = i + oi[m], bb = j + oj[m], cc = k + ok[m];
-            if (a < 0 || bb < 0 || cc < 0 || a >= D.nx || bb >= D.ny || cc >= D.nz) continue;
-            const uint32_t sn = nslot(a, bb, cc, D);
-            if (cell[sn] & kCellFluid) sum += x[sn];
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t key = tiles[t];
+        const uint32_t s = (key << 9) | tid;
+        const uint8_t c = cell[s];
+        const double xs = (c & kCellFluid) ? x[s] + (double)xg[s] : 0.0;
+        X[bc] = xs;
+        if (face < 6) {
+            const uint32_t tc = tcoord[t];
+            const int i = 8 * (int)(tc & 1023u) + hx, j = 8 * (int)((tc >> 10) & 1023u) + hy, k = 8 * (int)(tc >> 20) + hz;
+            double v = 0.0;
+            if (i >= 0 && j >= 0 && k >= 0 && i < D.nx && j < D.ny && k < D.nz) {
+                const uint32_t sn = nslot(i, j, k, D);
+                if (cell[sn] & kCellFluid) v = x[sn] + (double)xg[sn];
+            }
+            X[bh] = v;
         }
-        const double res = (double)bv[s] - ((double)(c & 7u) * x[s] - sum);
-        const float rs = (float)res;
-        r[s] = rs;
-        rr += res * res;
-        rz += (double)rs * (double)(rs * jacobi_inv(c));
+        __syncthreads();
+        if (c & kCellFluid) {
+            const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
+            const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
+            const float rs = (float)res;
+            r[s] = rs;
+            rr += res * res;
+            rz += (double)rs * (double)(rs * jacobi_inv(c));
+        }
+        __syncthreads();
     }
-    NAT_TILE_LOOP_END
     double vals[2] = {rr, rz}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->rr = out[0];
@@ -465,6 +612,7 @@ __global__ void __launch_bounds__(512) pcg_check_kernel(const uint32_t* __restri
         if (out[0] <= st->tol2 * st->bb) {
             st->done = 1;
         } else {
+            st->flush = 1;
             st->rz = out[1];
             st->beta = st->rz / st->rz_prev;
             if (st->iter >= st->max_iter) st->done = 2;
@@ -475,7 +623,7 @@ __global__ void __launch_bounds__(512) pcg_check_kernel(const uint32_t* __restri
 
 // --------------------------------------------------------- projection
 __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_count,
-                                                           NatDims D, const double* __restrict__ phi,
+                                                           NatDims D, const double* __restrict__ phi, const float* __restrict__ phig,
                                                            const uint8_t* __restrict__ type, float* __restrict__ u,
                                                            float* __restrict__ v, float* __restrict__ w) {
     const uint32_t ntiles = *d_count;
@@ -488,8 +636,9 @@ __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __rest
         uint8_t ta = nat_type(type, ia, ja, ka, D);
         if (ta == kSolid || tb == kSolid) continue;
         if (ta != kFluid && tb != kFluid) continue;
-        double pb = (tb == kFluid) ? phi[s] : 0.0;
-        double pa = (ta == kFluid) ? phi[nslot(ia, ja, ka, D)] : 0.0;
+        double pb = (tb == kFluid) ? phi[s] + (double)phig[s] : 0.0;
+        const uint32_t sa = (ta == kFluid) ? nslot(ia, ja, ka, D) : 0u;
+        double pa = (ta == kFluid) ? phi[sa] + (double)phig[sa] : 0.0;
         U[c][s] -= (float)(pb - pa);
     }
     NAT_TILE_LOOP_END
@@ -562,6 +711,12 @@ int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+int nat_launch_tile_coords(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint32_t* coords,
+                           int grid, cudaStream_t s) {
+    nat_tile_coords_kernel<<<grid, 256, 0, s>>>(tile_keys, d_ntiles, D, coords);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
                               uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s) {
     nat_dilate_kernel<<<grid, 256, 0, s>>>(tile_keys, d_ntiles, D, flags);
@@ -594,20 +749,22 @@ int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const N
 }
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                              cudaStream_t s) {
-    pcg_dirmatvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.st, B.partials);
-    pcg_update_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.r, B.p0, B.p1, B.q, B.cell, B.st, B.partials);
+    pcg_dirmatvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
+                                                    B.st, B.partials);
+    pcg_update_kernel<<<kPcgUpdateBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell, B.st,
+                                                       B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s) {
-    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st, B.partials);
+    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
-                       const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
-    nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, type, U[0], U[1], U[2]);
+                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
+    nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, phig, type, U[0], U[1], U[2]);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -20,23 +20,29 @@ struct NatDims {
 struct PcgState {
     double bb, rz, rz_prev, pq, rr, rr_true, alpha, beta, tol2;
     int iter, done, pending, max_iter, true_every, true_checks, next_check;
-    int pcur;  // which p buffer holds the current direction
+    int pcur;   // which p buffer holds the current direction
+    int flush;  // fold xg into x at the next direction update
     unsigned int ticket;
-    int pad;
 };
 
-constexpr int kPcgBlocks = 592;  // 148 SMs x 4 CTAs of 512 threads
+constexpr int kPcgBlocks = 592;        // 148 SMs x 4 CTAs of 512 threads
+constexpr int kPcgUpdateBlocks = 444;  // 148 SMs x 3 CTAs (the update keeps two quads per thread live)
 
-// PCG vectors on the tile-blocked slots.  x accumulates in FP64: an FP32
-// solution vector bounds the attainable true residual near eps_32 * cond(A)
-// (2.5e-5 on the 32^3 dam-break), above the 1e-6 target.  r, p, q and the
-// stencil arithmetic stay FP32; every dot product is FP64.
+// PCG vectors on the tile-blocked slots.  The solution is x + xg: x in FP64
+// holds everything up to the last true-residual check, xg (FP32) the
+// increments since then.  An FP32 solution alone bounds the attainable true
+// residual near eps_32 * cond(A) (2.5e-5 on the 32^3 dam-break), above the
+// 1e-6 target; the FP64 part removes that floor while each iteration moves
+// only FP32 data.  At every check r is replaced by b - A(x + xg) computed in
+// FP64, and the next direction update folds xg into x.  r, p, q and the stencil
+// arithmetic are FP32; every dot product is FP64.
 // cell: bit 7 = fluid, bits 0-2 = number of non-solid neighbours (the
 // Jacobi diagonal), 0 for every other cell.
 struct PcgBuffers {
     double* x;
-    float *b, *r, *p0, *p1, *q;
+    float *xg, *b, *r, *p0, *p1, *q;
     uint8_t* cell;
+    uint32_t* tcoord;  // packed tile coordinates of the occupied tiles
     PcgState* st;
     double* partials;  // [4][kPcgBlocks]
 };
@@ -48,6 +54,8 @@ int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src,
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s);
+int nat_launch_tile_coords(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint32_t* coords,
+                           int grid, cudaStream_t s);
 int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
                               uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s);
 int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s);
@@ -65,7 +73,7 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s);
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
-                       const uint8_t* type, float* const* U, int grid, cudaStream_t s);
+                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s);
 int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
                    float* const* P, float* const* V, cudaStream_t s);
 
