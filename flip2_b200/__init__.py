@@ -54,8 +54,19 @@ class Grid(C.Structure):
 class Params(C.Structure):
     _fields_ = [("mode", C.c_int32), ("flip_ratio", C.c_float), ("gravity_y", C.c_float), ("pcg_tol", C.c_double),
                 ("pcg_max_iter", C.c_int32), ("pcg_check_every", C.c_int32), ("true_residual_every", C.c_int32),
-                ("permute_velocities", C.c_int32), ("device", C.c_int32), ("reserved0", C.c_int32),
-                ("max_substep_dt", C.c_double), ("reserved", C.c_int32 * 4)]
+                ("permute_velocities", C.c_int32), ("device", C.c_int32), ("pressure_method", C.c_int32),
+                ("max_substep_dt", C.c_double), ("learned_max_iter", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+class PoissonSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("surface_min", C.c_double), ("surface_max", C.c_double),
+                ("solid_fraction", C.c_double), ("radius_min", C.c_double), ("radius_max", C.c_double),
+                ("impulses", C.c_int32), ("reserved", C.c_int32), ("gravity_dt", C.c_double)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int32), ("converged", C.c_int32), ("fell_back", C.c_int32), ("plain_iters", C.c_int32),
+                ("rel_residual", C.c_double), ("ms", C.c_double)]
 
 
 class Info(C.Structure):
@@ -118,6 +129,18 @@ def lib():
         "flip_get_buffer": (i32, [vp, i32, C.POINTER(vp), C.POINTER(u64), C.POINTER(u32)]),
         "flip_read_buffer": (i32, [vp, i32, vp, u64]),
         "flip_get_info": (i32, [vp, C.POINTER(Info)]),
+        "flip_get_solve_info": (i32, [vp, C.POINTER(SolveInfo)]),
+        "flip_lp_num_weights": (u64, []),
+        "flip_lp_init": (i32, [vp, u64]),
+        "flip_lp_set_weights": (i32, [vp, vp, u64]),
+        "flip_lp_get_weights": (i32, [vp, vp, u64]),
+        "flip_lp_get_grad": (i32, [vp, vp, u64]),
+        "flip_poisson_generate": (i32, [vp, C.POINTER(PoissonSpec)]),
+        "flip_poisson_set": (i32, [vp, vp, vp]),
+        "flip_poisson_solve": (i32, [vp, i32, d, i32, C.POINTER(SolveInfo)]),
+        "flip_poisson_read_solution": (i32, [vp, vp]),
+        "flip_lp_train_step": (i32, [vp, i32, C.c_float, C.POINTER(d)]),
+        "flip_lp_eval": (i32, [vp, vp, vp, C.POINTER(d), i32]),
         "flip_set_timing": (i32, [vp, i32]),
         "flip_get_stage_ms": (i32, [vp, C.POINTER(C.c_double), i32, i32]),
         "flip_last_error": (C.c_char_p, [vp]),
@@ -316,6 +339,7 @@ class Particles:
     # Particles API
     def setDomain(self, nx, ny, nz, x, y, z, cellSize):
         self._call("flip_set_domain", nx, ny, nz, x, y, z, cellSize)
+        self.params_grid_cells = 64 * x * y * z
 
     def alignParticlesToGrid(self):
         self._call("flip_align_particles_to_grid")
@@ -426,6 +450,65 @@ class Particles:
         a = (C.c_double * len(self.STAGES))()
         self._call("flip_get_stage_ms", a, len(self.STAGES), 1 if reset else 0)
         return dict(zip(self.STAGES, list(a)))
+
+    # learned preconditioner and standalone pressure problems
+    def lp_init(self, seed=0):
+        self._call("flip_lp_init", seed)
+
+    def lp_weights(self):
+        n = lib().flip_lp_num_weights()
+        w = np.empty(n, np.float32)
+        self._call("flip_lp_get_weights", w.ctypes.data_as(C.c_void_p), n)
+        return w
+
+    def lp_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._call("flip_lp_set_weights", w.ctypes.data_as(C.c_void_p), w.size)
+
+    def lp_grad(self):
+        n = lib().flip_lp_num_weights()
+        g = np.empty(n, np.float32)
+        self._call("flip_lp_get_grad", g.ctypes.data_as(C.c_void_p), n)
+        return g
+
+    def poisson_generate(self, seed, surface=(0.5, 0.85), solid_fraction=0.10, radius=(4.0, 16.0), impulses=6,
+                         gravity_dt=-9.8 / 480.0):
+        spec = PoissonSpec(seed, surface[0], surface[1], solid_fraction, radius[0], radius[1], impulses, 0, gravity_dt)
+        self._call("flip_poisson_generate", C.byref(spec))
+
+    def poisson_set(self, type_lin, b_lin):
+        t = np.ascontiguousarray(type_lin, np.uint8)
+        b = np.ascontiguousarray(b_lin, np.float32)
+        self._call("flip_poisson_set", t.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p))
+
+    def poisson_solve(self, method=0, tol=1e-6, max_iter=10000):
+        i = SolveInfo()
+        self._call("flip_poisson_solve", method, tol, max_iter, C.byref(i))
+        return i
+
+    def solve_info(self):
+        i = SolveInfo()
+        self._call("flip_get_solve_info", C.byref(i))
+        return i
+
+    def poisson_solution(self):
+        nc = int(self.params_grid_cells)
+        x = np.empty(nc, np.float64)
+        self._call("flip_poisson_read_solution", x.ctypes.data_as(C.c_void_p))
+        return x
+
+    def lp_train_step(self, pcg_iters, lr):
+        loss = C.c_double()
+        self._call("flip_lp_train_step", pcg_iters, lr, C.byref(loss))
+        return loss.value
+
+    def lp_eval(self, r_lin, want_grad=False):
+        r = np.ascontiguousarray(r_lin, np.float32)
+        z = np.empty_like(r)
+        loss = C.c_double()
+        self._call("flip_lp_eval", r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p), C.byref(loss),
+                   1 if want_grad else 0)
+        return z, loss.value
 
     def info(self):
         i = Info()

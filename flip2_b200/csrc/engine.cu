@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 #include "common.cuh"
+#include "lprec.cuh"
 #include "native.cuh"
 #include "ref_kernels.cuh"
 
@@ -73,6 +74,20 @@ struct flip_engine {
     int sms = 148;
     int last_iters = 0, last_converged = 0;
     double last_rel = 0.0;
+    flip_solve_info last_solve{};
+    // learned preconditioner: weights survive flip_set_domain, the
+    // activation buffers are per domain and allocated on first use
+    LpNet lp{};
+    char* lp_warena = nullptr;   // w, g, m, v, wb
+    char* lp_aarena = nullptr;   // act[3], gact, gact2, z, scalars
+    double* lp_scalar = nullptr; // [0] loss sum, [1] r.r sum
+    bool lp_have_weights = false;
+    cudaGraphExec_t fpcg_graph = nullptr;
+    int fpcg_graph_iters = 0;
+    bool poisson_ready = false;  // a standalone pressure problem is in place
+    float4* gen_sph = nullptr;   // generator inputs (device)
+    float* gen_imp = nullptr;
+    cudaEvent_t solve_ev[2] = {};
     uint32_t launches = 0;
     // stage timing
     bool timing = false;
@@ -107,6 +122,8 @@ struct flip_engine {
 #define E_CUDA(expr) E_TRY(e->cuda((expr), #expr))
 
 static size_t al(size_t v) { return (v + 255) / 256 * 256; }
+constexpr int kGenMaxSpheres = 4096;
+constexpr int kGenMaxImpulses = 64;
 
 extern "C" void flip_default_params(int mode, flip_params* out) {
     if (!out) return;
@@ -121,6 +138,8 @@ extern "C" void flip_default_params(int mode, flip_params* out) {
     out->permute_velocities = 0;
     out->device = 0;
     out->max_substep_dt = 1.0 / 240.0;
+    out->pressure_method = 0;
+    out->learned_max_iter = 1000;
 }
 
 extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, flip_engine** out) {
@@ -155,11 +174,26 @@ extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, 
     if (rc) { flip_destroy(e); return rc; }
     rc = e->cuda(cudaMallocHost((void**)&e->h_state, sizeof(PcgState)), "cudaMallocHost");
     if (rc) { flip_destroy(e); return rc; }
+    for (auto& v : e->solve_ev) {
+        rc = e->cuda(cudaEventCreate(&v), "cudaEventCreate");
+        if (rc) { flip_destroy(e); return rc; }
+    }
     *out = e;
     return FLIP_OK;
 }
 
+static void free_lp_activations(flip_engine* e) {
+    if (e->fpcg_graph) { cudaGraphExecDestroy(e->fpcg_graph); e->fpcg_graph = nullptr; }
+    if (e->lp_aarena) cudaFree(e->lp_aarena);
+    e->lp_aarena = nullptr;
+    for (auto& a : e->lp.act) a = nullptr;
+    e->lp.gact = e->lp.gact2 = nullptr;
+    e->pcg.z = nullptr;
+    e->lp_scalar = nullptr;
+}
 static void free_arena(flip_engine* e) {
+    free_lp_activations(e);
+    e->poisson_ready = false;
     if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
     if (e->arena) cudaFree(e->arena);
     e->arena = nullptr;
@@ -228,7 +262,9 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         e->nslots = e->ntiles_total * 512;
         if (e->nslots >= (1ull << 32)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: grid above 2^32 voxels");
         e->key_bits = bits_for(e->ntiles_total - 1);
-        add((void**)&e->node_keys, 4 * std::min<uint64_t>(n, e->ntiles_total));
+        add((void**)&e->node_keys, 4 * e->ntiles_total);  // occupied tiles, or fluid tiles of a pressure problem
+        add((void**)&e->gen_sph, sizeof(float4) * kGenMaxSpheres);
+        add((void**)&e->gen_imp, sizeof(float) * 7 * kGenMaxImpulses);
         for (int a = 0; a < 6; ++a) { add((void**)&e->fp[a], 4 * n); add((void**)&e->fq[a], 4 * n); }
         for (int c = 0; c < 3; ++c) {
             add((void**)&e->m[c], 4 * e->nslots);
@@ -621,35 +657,175 @@ static int nat_pcg_graph(flip_engine* e, int iters) {
     return FLIP_OK;
 }
 
-static int nat_pressure(flip_engine* e) {
+// ------------------------------------------------ learned preconditioner
+static int lp_alloc_weights(flip_engine* e) {
+    if (e->lp_warena) return FLIP_OK;
+    const size_t fw = al(sizeof(float) * kLpNumW), bw = al(sizeof(__nv_bfloat16) * kLpNumW);
+    E_CUDA(cudaMalloc((void**)&e->lp_warena, 4 * fw + bw));
+    E_CUDA(cudaMemsetAsync(e->lp_warena, 0, 4 * fw + bw, e->stream));
+    e->lp.w = (float*)e->lp_warena;
+    e->lp.g = (float*)(e->lp_warena + fw);
+    e->lp.m = (float*)(e->lp_warena + 2 * fw);
+    e->lp.v = (float*)(e->lp_warena + 3 * fw);
+    e->lp.wb = (__nv_bfloat16*)(e->lp_warena + 4 * fw);
+    const int dil[kLpLayers] = {1, 2, 4, 1};
+    for (int l = 0; l < kLpLayers; ++l) e->lp.dil[l] = dil[l];
+    e->lp.adam_t = 0;
+    return FLIP_OK;
+}
+// activations for every slot of the grid: 3 x 16 BF16 + 2 x 16 FP32 + z
+static int lp_alloc_activations(flip_engine* e) {
+    if (e->lp_aarena) return FLIP_OK;
+    if (e->P.mode != FLIP_MODE_NATIVE) return e->fail(FLIP_ERR_STATE, "learned preconditioner: native mode only");
+    const size_t ab = al(e->nslots * 16 * sizeof(__nv_bfloat16)), gb = al(e->nslots * 16 * sizeof(float)),
+                 zb = al(e->nslots * sizeof(float));
+    const size_t total = 3 * ab + 2 * gb + zb + 256;
+    E_CUDA(cudaMalloc((void**)&e->lp_aarena, total));
+    E_CUDA(cudaMemsetAsync(e->lp_aarena, 0, total, e->stream));
+    for (int l = 0; l < 3; ++l) e->lp.act[l] = (__nv_bfloat16*)(e->lp_aarena + l * ab);
+    e->lp.gact = (float*)(e->lp_aarena + 3 * ab);
+    e->lp.gact2 = (float*)(e->lp_aarena + 3 * ab + gb);
+    e->pcg.z = (float*)(e->lp_aarena + 3 * ab + 2 * gb);
+    e->lp_scalar = (double*)(e->lp_aarena + 3 * ab + 2 * gb + zb);
+    return FLIP_OK;
+}
+// the network's view of the current problem: activations on the dilated
+// tile list, outputs on the occupied (fluid) tiles
+static LpGrid lp_grid(flip_engine* e, const int* halt) {
+    LpGrid G{};
+    G.r = e->pcg.r;
+    G.type = e->type;
+    G.tile_active = e->tile_flags;
+    G.act_tiles = e->grid_tiles;
+    G.d_nact = e->d_counts + 1;
+    G.out_tiles = e->node_keys;
+    G.d_nout = e->d_counts;
+    G.halt = halt;
+    G.D = e->D;
+    return G;
+}
+static int lp_ready(flip_engine* e) {
+    if (!e->lp_have_weights) return e->fail(FLIP_ERR_STATE, "learned preconditioner: no weights (flip_lp_init or flip_lp_set_weights)");
+    return lp_alloc_activations(e);
+}
+
+// ------------------------------------------------------ pressure solves
+static void pcg_state_host(flip_engine* e, double tol, int max_iter, int flexible) {
     PcgState init{};
-    init.tol2 = e->P.pcg_tol * e->P.pcg_tol;
-    init.max_iter = e->P.pcg_max_iter;
+    init.tol2 = tol * tol;
+    init.max_iter = max_iter;
     init.true_every = e->P.true_residual_every;
     init.next_check = e->P.true_residual_every;
+    init.flexible = flexible;
     *e->h_state = init;
-    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
-    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, (const float* const*)e->m, e->type, e->pcg, e->stream));
-    e->launches += 1;
-    E_TRY(e->mark(9));
-    const int chunk = e->P.pcg_check_every;
-    E_TRY(nat_pcg_graph(e, chunk));
+}
+
+static int nat_fpcg_graph(flip_engine* e, int iters) {
+    if (e->fpcg_graph && e->fpcg_graph_iters == iters) return FLIP_OK;
+    if (e->fpcg_graph) { cudaGraphExecDestroy(e->fpcg_graph); e->fpcg_graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    const LpGrid G = lp_grid(e, &e->pcg.st->halt);
+    const float* inv_s = &e->pcg.st->inv_s;
+    int rc = FLIP_OK;
+    for (int k = 0; k < iters && rc == FLIP_OK; ++k) {
+        rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        if (rc == FLIP_OK && k == iters - 1) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        if (rc == FLIP_OK) rc = lp_forward_dev(e->lp, G, inv_s, e->pcg.z, nat_grid(e, 2), e->stream);
+        if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream);
+    }
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    E_CUDA(ce);
+    ce = cudaGraphInstantiate(&e->fpcg_graph, g, 0);
+    cudaGraphDestroy(g);
+    E_CUDA(ce);
+    e->fpcg_graph_iters = iters;
+    return FLIP_OK;
+}
+
+// launch a chunk graph until the device state says done; bounded on the host
+static int run_chunks(flip_engine* e, cudaGraphExec_t g, int chunk, uint32_t launches_per_chunk, int max_iter) {
     int launched = 0;
     for (;;) {
-        E_CUDA(cudaGraphLaunch(e->pcg_graph, e->stream));
-        e->launches += 2u * (uint32_t)chunk + 1u;
+        E_CUDA(cudaGraphLaunch(g, e->stream));
+        e->launches += launches_per_chunk;
         launched += chunk;
         E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
         E_CUDA(cudaStreamSynchronize(e->stream));
         if (e->h_state->done) break;
-        if (launched > e->P.pcg_max_iter + 2 * chunk) break;  // host-side bound as well
+        if (launched > max_iter + 2 * chunk) break;  // host-side bound as well
+    }
+    return FLIP_OK;
+}
+
+// Solve A x = b on the occupied tiles.  U: face velocities giving b = -div U,
+// or nullptr when b is already in pcg.b.  method 1 runs learned FPCG first and,
+// if it stops without meeting tol (iteration cap or a non-positive r.z),
+// restarts Jacobi-PCG from x = 0.
+static int nat_solve(flip_engine* e, const float* const* U, int method, double tol, int max_plain, int max_learned,
+                     flip_solve_info* out) {
+    flip_solve_info info{};
+    const int chunk = e->P.pcg_check_every;
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    if (e->timing || out) E_CUDA(cudaEventRecord(e->solve_ev[0], e->stream));
+    bool need_plain = true;
+    if (method == 1) {
+        E_TRY(lp_ready(e));
+        pcg_state_host(e, tol, max_learned, 1);
+        E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
+        const LpGrid G = lp_grid(e, &e->pcg.st->halt);
+        E_TRY(lp_forward_dev(e->lp, G, &e->pcg.st->inv_s, e->pcg.z, nat_grid(e, 2), e->stream));
+        E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream));
+        e->launches += 6;
+        E_TRY(e->mark(9));
+        E_TRY(nat_fpcg_graph(e, chunk));
+        E_TRY(run_chunks(e, e->fpcg_graph, chunk, 7u * (uint32_t)chunk + 1u, max_learned));
+        const PcgState& s = *e->h_state;
+        info.iters = s.iter;
+        double rr = s.true_checks ? s.rr_true : s.rr;
+        info.rel_residual = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
+        info.converged = s.done == 1;
+        need_plain = s.done != 1;
+        if (need_plain) { info.fell_back = 1; U = nullptr; }  // b stays in pcg.b
+    }
+    if (need_plain) {
+        pcg_state_host(e, tol, max_plain, 0);
+        E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
+        e->launches += 1;
+        if (method != 1) E_TRY(e->mark(9));
+        E_TRY(nat_pcg_graph(e, chunk));
+        E_TRY(run_chunks(e, e->pcg_graph, chunk, 2u * (uint32_t)chunk + 1u, max_plain));
+        const PcgState& s = *e->h_state;
+        if (method == 1) info.plain_iters = s.iter;
+        else info.iters = s.iter;
+        double rr = s.true_checks ? s.rr_true : s.rr;
+        info.rel_residual = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
+        info.converged = s.done == 1;
     }
     E_TRY(e->mark(10));
-    const PcgState& s = *e->h_state;
-    e->last_iters = s.iter;
-    e->last_converged = (s.done == 1) ? 1 : 0;
-    double rr = s.true_checks ? s.rr_true : s.rr;
-    e->last_rel = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
+    if (e->timing || out) {
+        E_CUDA(cudaEventRecord(e->solve_ev[1], e->stream));
+        E_CUDA(cudaEventSynchronize(e->solve_ev[1]));
+        float ms = 0.0f;
+        E_CUDA(cudaEventElapsedTime(&ms, e->solve_ev[0], e->solve_ev[1]));
+        info.ms = ms;
+    }
+    e->last_iters = info.iters + info.plain_iters;
+    e->last_converged = info.converged;
+    e->last_rel = info.rel_residual;
+    e->last_solve = info;
+    if (out) *out = info;
+    return FLIP_OK;
+}
+
+static int nat_pressure(flip_engine* e) {
+    const int learned = e->P.learned_max_iter > 0 ? e->P.learned_max_iter : e->P.pcg_max_iter;
+    E_TRY(nat_solve(e, (const float* const*)e->m, e->P.pressure_method, e->P.pcg_tol, e->P.pcg_max_iter, learned,
+                    e->timing ? &e->last_solve : nullptr));
+    e->poisson_ready = true;  // b, the cell types and the tile lists of this solve stay in place
     return FLIP_OK;
 }
 
@@ -925,6 +1101,257 @@ extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
     return FLIP_OK;
 }
 
+// ============================== learned preconditioner and pressure problems
+namespace {
+// splitmix64 (Steele, Lea and Flood, 2014) for the host-side problem generator
+struct HostRng {
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uni() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+    double uni(double a, double b) { return a + (b - a) * uni(); }
+    double normal() {  // Box-Muller
+        double u1 = uni(), u2 = uni();
+        if (u1 < 1e-300) u1 = 1e-300;
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    }
+};
+}  // namespace
+
+#define CHECK_NATIVE(name)                                                                   \
+    do {                                                                                     \
+        CHECK_E();                                                                           \
+        if (e->P.mode != FLIP_MODE_NATIVE) return e->fail(FLIP_ERR_STATE, name ": native mode only"); \
+    } while (0)
+
+extern "C" uint64_t flip_lp_num_weights(void) { return (uint64_t)kLpNumW; }
+
+static int lp_upload(flip_engine* e, const float* w) {
+    E_CUDA(cudaSetDevice(e->P.device));
+    E_TRY(lp_alloc_weights(e));
+    E_CUDA(cudaMemcpyAsync(e->lp.w, w, sizeof(float) * kLpNumW, cudaMemcpyHostToDevice, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp.m, 0, sizeof(float) * kLpNumW, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp.v, 0, sizeof(float) * kLpNumW, e->stream));
+    E_TRY(lp_sync_bf16(e->lp, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->lp.adam_t = 0;
+    e->lp_have_weights = true;
+    return FLIP_OK;
+}
+
+extern "C" int flip_lp_init(flip_engine* e, uint64_t seed) {
+    if (!e) return FLIP_ERR_ARG;
+    e->err.clear();
+    HostRng rng{seed};
+    std::vector<float> w(kLpNumW);
+    for (int l = 0; l < kLpLayers; ++l) {
+        const double sd = std::sqrt(2.0 / (27.0 * kLpCin[l]));  // He-normal over the 27 taps x Cin inputs
+        for (int i = kLpWOff[l]; i < kLpWOff[l + 1]; ++i) w[i] = (float)(sd * rng.normal());
+    }
+    return lp_upload(e, w.data());
+}
+
+extern "C" int flip_lp_set_weights(flip_engine* e, const float* w, uint64_t n) {
+    if (!e) return FLIP_ERR_ARG;
+    e->err.clear();
+    if (!w || n != (uint64_t)kLpNumW) return e->fail(FLIP_ERR_ARG, "flip_lp_set_weights: need flip_lp_num_weights() floats");
+    for (uint64_t i = 0; i < n; ++i)
+        if (!std::isfinite(w[i])) return e->fail(FLIP_ERR_ARG, "flip_lp_set_weights: non-finite weight");
+    return lp_upload(e, w);
+}
+
+static int lp_download(flip_engine* e, const float* src, float* dst, uint64_t n, const char* name) {
+    if (!e) return FLIP_ERR_ARG;
+    e->err.clear();
+    if (!dst || n != (uint64_t)kLpNumW) return e->fail(FLIP_ERR_ARG, std::string(name) + ": need flip_lp_num_weights() floats");
+    if (!e->lp_have_weights) return e->fail(FLIP_ERR_STATE, std::string(name) + ": no weights");
+    E_CUDA(cudaSetDevice(e->P.device));
+    E_CUDA(cudaMemcpyAsync(dst, src, sizeof(float) * kLpNumW, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    return FLIP_OK;
+}
+extern "C" int flip_lp_get_weights(flip_engine* e, float* w, uint64_t n) {
+    return lp_download(e, e ? e->lp.w : nullptr, w, n, "flip_lp_get_weights");
+}
+extern "C" int flip_lp_get_grad(flip_engine* e, float* g, uint64_t n) {
+    return lp_download(e, e ? e->lp.g : nullptr, g, n, "flip_lp_get_grad");
+}
+
+// fluid tiles -> node_keys, their dilation -> tile_flags / grid_tiles, cell codes cleared
+static int poisson_tiles(flip_engine* e) {
+    E_CUDA(cudaMemsetAsync(e->pcg.cell, 0, e->nslots, e->stream));
+    E_TRY(nat_launch_fluid_tiles(e->type, e->tile_flags, (uint32_t)e->ntiles_total, e->node_keys, e->d_counts, e->nslots,
+                                 e->stream));
+    E_TRY(nat_launch_dilate_compact(e->node_keys, e->d_counts, e->D, e->tile_flags, e->grid_tiles, e->d_counts + 1,
+                                    nat_grid(e, 2), e->stream));
+    E_TRY(nat_launch_tile_coords(e->node_keys, e->d_counts, e->D, e->pcg.tcoord, nat_grid(e, 2), e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->launches += 6;
+    e->poisson_ready = true;
+    e->have_voxels = false;
+    return FLIP_OK;
+}
+
+extern "C" int flip_poisson_generate(flip_engine* e, const flip_poisson_spec* spec) {
+    CHECK_NATIVE("flip_poisson_generate");
+    if (!spec) return e->fail(FLIP_ERR_ARG, "flip_poisson_generate: null spec");
+    if (!(spec->surface_min >= 0.0 && spec->surface_min <= spec->surface_max && spec->surface_max <= 1.0) ||
+        !(spec->solid_fraction >= 0.0 && spec->solid_fraction <= 0.5) ||
+        !(spec->radius_min > 0.0 && spec->radius_min <= spec->radius_max) || spec->impulses < 0 ||
+        spec->impulses > kGenMaxImpulses || !std::isfinite(spec->gravity_dt))
+        return e->fail(FLIP_ERR_ARG, "flip_poisson_generate: spec out of range");
+    const NatDims& D = e->D;
+    HostRng rng{spec->seed};
+    const double surface = rng.uni(spec->surface_min, spec->surface_max) * D.ny;
+    // spheres until their summed volume reaches the solid fraction of the box
+    std::vector<float4> sph;
+    const double target = spec->solid_fraction * (double)D.nx * D.ny * D.nz;
+    double vol = 0.0;
+    while (vol < target && (int)sph.size() < kGenMaxSpheres) {
+        const double cx = rng.uni(0.0, D.nx), cy = rng.uni(0.0, D.ny), cz = rng.uni(0.0, D.nz);
+        const double r = rng.uni(spec->radius_min, spec->radius_max);
+        sph.push_back(make_float4((float)cx, (float)cy, (float)cz, (float)r));
+        vol += 4.18879020478639 * r * r * r;
+    }
+    // Gaussian impulses: centre, width 1/12..1/4 of the smallest extent, N(0,1) amplitudes
+    const double ext = std::min(D.nx, std::min(D.ny, D.nz));
+    std::vector<float> imp(7 * (size_t)std::max(spec->impulses, 1));
+    for (int q = 0; q < spec->impulses; ++q) {
+        float* m = imp.data() + 7 * q;
+        m[0] = (float)rng.uni(0.0, D.nx);
+        m[1] = (float)rng.uni(0.0, D.ny);
+        m[2] = (float)rng.uni(0.0, D.nz);
+        m[3] = (float)(ext * rng.uni(1.0 / 12.0, 0.25));
+        for (int c = 0; c < 3; ++c) m[4 + c] = (float)rng.normal();
+    }
+    if (!sph.empty())
+        E_CUDA(cudaMemcpyAsync(e->gen_sph, sph.data(), sizeof(float4) * sph.size(), cudaMemcpyHostToDevice, e->stream));
+    if (spec->impulses > 0)
+        E_CUDA(cudaMemcpyAsync(e->gen_imp, imp.data(), sizeof(float) * 7 * spec->impulses, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_poisson_gen(D, (float)surface, e->gen_sph, (int)sph.size(), e->gen_imp, spec->impulses,
+                                 (float)spec->gravity_dt, e->type, e->pcg.b, e->nslots, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));  // the host vectors above are pageable
+    e->launches += 1;
+    return poisson_tiles(e);
+}
+
+extern "C" int flip_poisson_set(flip_engine* e, const uint8_t* type_lin, const float* b_lin) {
+    CHECK_NATIVE("flip_poisson_set");
+    if (!type_lin || !b_lin) return e->fail(FLIP_ERR_ARG, "flip_poisson_set: null array");
+    // pcg.cell and pcg.q stage the linear arrays (nslots == cells)
+    E_CUDA(cudaMemcpyAsync(e->pcg.cell, type_lin, e->nslots, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_mask_to_tiles(e->pcg.cell, e->D, e->type, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->pcg.q, b_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_lin_tiles_f32(e->pcg.q, e->pcg.b, e->D, 1, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->launches += 2;
+    return poisson_tiles(e);
+}
+
+extern "C" int flip_poisson_solve(flip_engine* e, int method, double tol, int max_iter, flip_solve_info* info) {
+    CHECK_NATIVE("flip_poisson_solve");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_poisson_solve: no problem (flip_poisson_generate/set)");
+    if ((method != 0 && method != 1) || !(tol > 0.0) || max_iter <= 0)
+        return e->fail(FLIP_ERR_ARG, "flip_poisson_solve: method 0/1, tol > 0, max_iter > 0");
+    flip_solve_info local{};
+    const int plain = method == 1 ? e->P.pcg_max_iter : max_iter;
+    E_TRY(nat_solve(e, nullptr, method, tol, plain, max_iter, &local));
+    if (info) *info = local;
+    return FLIP_OK;
+}
+
+extern "C" int flip_poisson_read_solution(flip_engine* e, double* x_lin) {
+    CHECK_NATIVE("flip_poisson_read_solution");
+    if (!x_lin) return e->fail(FLIP_ERR_ARG, "flip_poisson_read_solution: null array");
+    double* tmp = nullptr;
+    E_CUDA(cudaMalloc((void**)&tmp, 8 * e->nslots));
+    int rc = nat_launch_solution_lin(e->pcg.x, e->pcg.xg, e->pcg.cell, e->D, tmp, e->stream);
+    if (rc == FLIP_OK) rc = e->cuda(cudaMemcpyAsync(x_lin, tmp, 8 * e->nslots, cudaMemcpyDeviceToHost, e->stream), "cudaMemcpyAsync");
+    if (rc == FLIP_OK) rc = e->cuda(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    cudaFree(tmp);
+    e->launches += 1;
+    return rc;
+}
+
+// read back the loss sum and the state; loss = sum / n_fluid
+static int lp_read_loss(flip_engine* e, double* loss) {
+    double l2 = 0.0;
+    E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_small, e->lp_scalar, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    memcpy(&l2, e->h_small, sizeof(double));
+    if (loss) *loss = l2 / std::max(e->h_state->nfluid, 1.0);
+    return FLIP_OK;
+}
+
+extern "C" int flip_lp_train_step(flip_engine* e, int pcg_iters, float lr, double* loss) {
+    CHECK_NATIVE("flip_lp_train_step");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_train_step: no problem (flip_poisson_generate/set)");
+    if (pcg_iters < 0 || pcg_iters > 100000 || !(lr >= 0.0f)) return e->fail(FLIP_ERR_ARG, "flip_lp_train_step: bad arguments");
+    E_TRY(lp_ready(e));
+    // the sample: the residual after pcg_iters Jacobi-PCG iterations from x = 0
+    pcg_state_host(e, 0.0, pcg_iters + 1, 0);
+    e->h_state->true_every = 0;
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));
+    for (int k = 0; k < pcg_iters; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+    const LpGrid G = lp_grid(e, nullptr);
+    const float* inv_s = &e->pcg.st->inv_s;
+    const int grid = nat_grid(e, 2);
+    E_TRY(lp_forward_dev(e->lp, G, inv_s, e->pcg.z, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, sizeof(double), e->stream));
+    E_TRY(lp_loss_grad(G, inv_s, e->pcg.z, e->pcg.q, e->pcg.p1, e->lp_scalar, &e->pcg.st->nfluid, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
+    E_TRY(lp_backward_dev(e->lp, G, inv_s, e->pcg.p1, grid, e->stream));
+    E_TRY(lp_adam(e->lp, lr, e->stream));
+    e->launches += 1 + 2 * (uint32_t)pcg_iters + 4 + 2 + 7 + 1;
+    return lp_read_loss(e, loss);
+}
+
+extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, float* z_lin, double* loss, int want_grad) {
+    CHECK_NATIVE("flip_lp_eval");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_eval: no problem (flip_poisson_generate/set)");
+    if (!r_lin) return e->fail(FLIP_ERR_ARG, "flip_lp_eval: null residual");
+    E_TRY(lp_ready(e));
+    pcg_state_host(e, 0.0, 0, 0);
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));  // cell codes, n_fluid
+    E_CUDA(cudaMemcpyAsync(e->pcg.p0, r_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_lin_tiles_f32(e->pcg.p0, e->pcg.r, e->D, 1, e->stream));
+    const LpGrid G = lp_grid(e, nullptr);
+    float* inv_s = &e->pcg.st->inv_s;
+    const int grid = nat_grid(e, 2);
+    E_TRY(lp_input_scale(G, e->lp_scalar + 1, &e->pcg.st->nfluid, inv_s, grid, e->stream));
+    E_TRY(lp_forward_dev(e->lp, G, inv_s, e->pcg.z, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, sizeof(double), e->stream));
+    E_TRY(lp_loss_grad(G, inv_s, e->pcg.z, e->pcg.q, e->pcg.p1, e->lp_scalar, &e->pcg.st->nfluid, grid, e->stream));
+    e->launches += 1 + 1 + 2 + 4 + 2;
+    if (want_grad) {
+        E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
+        E_TRY(lp_backward_dev(e->lp, G, inv_s, e->pcg.p1, grid, e->stream));
+        e->launches += 7;
+    }
+    if (z_lin) {
+        E_TRY(nat_launch_lin_tiles_f32(e->pcg.z, e->pcg.p0, e->D, 0, e->stream));
+        E_CUDA(cudaMemcpyAsync(z_lin, e->pcg.p0, 4 * e->nslots, cudaMemcpyDeviceToHost, e->stream));
+        e->launches += 1;
+    }
+    return lp_read_loss(e, loss);
+}
+
+extern "C" int flip_get_solve_info(flip_engine* e, flip_solve_info* out) {
+    if (!e || !out) return FLIP_ERR_ARG;
+    *out = e->last_solve;
+    return FLIP_OK;
+}
+
 extern "C" int flip_set_timing(flip_engine* e, int enable) {
     if (!e) return FLIP_ERR_ARG;
     if (enable && !e->ev[0])
@@ -956,6 +1383,8 @@ extern "C" int flip_destroy(flip_engine* e) {
     if (e->h_small) cudaFreeHost(e->h_small);
     if (e->h_state) cudaFreeHost(e->h_state);
     for (auto& v : e->ev) if (v) cudaEventDestroy(v);
+    for (auto& v : e->solve_ev) if (v) cudaEventDestroy(v);
+    if (e->lp_warena) cudaFree(e->lp_warena);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
     return FLIP_OK;

@@ -1,0 +1,69 @@
+// lprec.cuh -- the learned pressure preconditioner: a 4-layer 3^3
+// convolution network (3 -> 16 -> 16 -> 16 -> 1 channels, ReLU after the
+// first three layers, no biases), BF16 weights and activations with FP32
+// accumulation, applied on the tile-blocked grid.  No reference counterpart.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "native.cuh"
+
+namespace flip {
+
+constexpr int kLpLayers = 4;
+constexpr int kLpCh = 16;
+constexpr int kLpCin[kLpLayers] = {3, kLpCh, kLpCh, kLpCh};
+constexpr int kLpCout[kLpLayers] = {kLpCh, kLpCh, kLpCh, 1};
+// weights of layer l: [27 taps][Cin][Cout], taps ordered dz, dy, dx in -1..1
+constexpr int kLpW[kLpLayers] = {27 * 3 * kLpCh, 27 * kLpCh * kLpCh, 27 * kLpCh * kLpCh, 27 * kLpCh};
+constexpr int kLpWOff[kLpLayers + 1] = {0, kLpW[0], kLpW[0] + kLpW[1], kLpW[0] + kLpW[1] + kLpW[2],
+                                        kLpW[0] + kLpW[1] + kLpW[2] + kLpW[3]};
+constexpr int kLpNumW = kLpWOff[kLpLayers];
+
+struct LpNet {
+    int dil[kLpLayers];   // dilation of each layer
+    float* w;             // FP32 master weights [kLpNumW]
+    float* g;             // gradient [kLpNumW]
+    float* m;             // Adam first moment
+    float* v;             // Adam second moment
+    __nv_bfloat16* wb;    // BF16 copy used by the kernels
+    __nv_bfloat16* act[3];  // activations after layers 0..2: [slot][16]
+    float* gact;          // gradient of one activation layer: [slot][16]
+    float* gact2;         // second gradient buffer: [slot][16]
+    int adam_t;
+};
+
+// Inputs the network reads: residual r (FP32, read only at fluid cells),
+// cell types (0 air, 1 fluid, 2 solid), the per-tile active flags and the
+// tile lists (the layers 0..2 run on the dilated list, layer 3 on the fluid
+// tile list).
+struct LpGrid {
+    const float* r;
+    const uint8_t* type;
+    const uint8_t* tile_active;  // [tiles] nonzero where activations are valid
+    const uint32_t* act_tiles;   // tiles where activations are computed
+    const uint32_t* d_nact;
+    const uint32_t* out_tiles;   // tiles with fluid cells (outputs)
+    const uint32_t* d_nout;
+    const int* halt;             // optional: nonzero stops the kernels (a converged FPCG)
+    NatDims D;
+};
+
+// z = s * N([r/s, fluid, solid]) on fluid cells, 0 elsewhere; s = 1/(*d_inv_s)
+int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* z, int grid, cudaStream_t st);
+// gradient of the loss with respect to the weights given dL/dz (gz, FP32 on
+// the slots of the active tiles, zero off fluid cells); accumulates into
+// net.g (caller zeroes it)
+int lp_backward_dev(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz, int grid, cudaStream_t st);
+// training loss L = |A z - r|^2 / |r|^2 over the fluid cells, with
+// |r|^2 = s^2 n_fluid: e = (A z - r)/s, *d_loss2 += |e|^2 (caller zeroes it),
+// gz = dL/dz = 2 A e / (s n_fluid) (A is symmetric on the fluid cells)
+int lp_loss_grad(const LpGrid& G, const float* d_inv_s, const float* z, float* e, float* gz, double* d_loss2,
+                 const double* d_nfluid, int grid, cudaStream_t st);
+// *d_inv_s = 1 / rms(r) over the fluid cells of the output tiles
+int lp_input_scale(const LpGrid& G, double* d_acc, const double* d_nfluid, float* d_inv_s, int grid, cudaStream_t st);
+// Adam step on the FP32 master weights, then the BF16 copy
+int lp_adam(LpNet& net, float lr, cudaStream_t st);
+int lp_sync_bf16(LpNet& net, cudaStream_t st);
+
+}  // namespace flip

@@ -178,6 +178,89 @@ __global__ void nat_tile_coords_kernel(const uint32_t* __restrict__ tile_keys, c
     }
 }
 
+// ------------------------------------------------ standalone Poisson problems
+// Cell types and right-hand side of a pressure problem on the whole box:
+// solid inside any sphere (cx, cy, cz, r in voxels), fluid below the surface
+// height, air above; b = -div(u) on fluid cells for u = sum of Gaussian
+// velocity impulses (cx, cy, cz, sigma, ax, ay, az) plus gravity*dt on the
+// y faces next to fluid, with faces touching a solid cell or a wall at zero.
+__device__ __forceinline__ bool gen_solid(float x, float y, float z, const float4* sph, int nsph) {
+    for (int q = 0; q < nsph; ++q) {
+        const float4 s = sph[q];
+        const float dx = x - s.x, dy = y - s.y, dz = z - s.z;
+        if (dx * dx + dy * dy + dz * dz < s.w * s.w) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ uint8_t gen_type(int i, int j, int k, const NatDims& D, float surface, const float4* sph,
+                                            int nsph) {
+    if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return kSolid;
+    if (gen_solid(i + 0.5f, j + 0.5f, k + 0.5f, sph, nsph)) return kSolid;
+    return (j + 0.5f < surface) ? kFluid : kAir;
+}
+__device__ __forceinline__ float gen_face(int c, int i, int j, int k, const NatDims& D, float surface, const float4* sph,
+                                          int nsph, const float* imp, int nimp, float gdt) {
+    // face c of cell (i,j,k): between (i,j,k) - e_c and (i,j,k)
+    const uint8_t tb = gen_type(i, j, k, D, surface, sph, nsph);
+    const uint8_t ta = gen_type(i - (c == 0), j - (c == 1), k - (c == 2), D, surface, sph, nsph);
+    if (ta == kSolid || tb == kSolid) return 0.0f;
+    const float x = i + (c == 0 ? 0.0f : 0.5f), y = j + (c == 1 ? 0.0f : 0.5f), z = k + (c == 2 ? 0.0f : 0.5f);
+    float u = 0.0f;
+    for (int q = 0; q < nimp; ++q) {
+        const float* m = imp + 7 * q;
+        const float dx = x - m[0], dy = y - m[1], dz = z - m[2];
+        u += m[4 + c] * __expf(-(dx * dx + dy * dy + dz * dz) / (2.0f * m[3] * m[3]));
+    }
+    if (c == 1 && (ta == kFluid || tb == kFluid)) u += gdt;
+    return u;
+}
+__global__ void nat_poisson_gen_kernel(NatDims D, float surface, const float4* __restrict__ sph, int nsph,
+                                       const float* __restrict__ imp, int nimp, float gdt, uint8_t* __restrict__ type,
+                                       float* __restrict__ b, uint64_t nslots) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const uint32_t tile = (uint32_t)(s >> 9), l = (uint32_t)(s & 511u);
+    const int i = 8 * (int)(tile % D.tx) + (int)(l & 7u), j = 8 * (int)((tile / D.tx) % D.ty) + (int)((l >> 3) & 7u),
+              k = 8 * (int)(tile / (D.tx * D.ty)) + (int)(l >> 6);
+    const uint8_t t = gen_type(i, j, k, D, surface, sph, nsph);
+    type[s] = t;
+    float bv = 0.0f;
+    if (t == kFluid) {
+        float div = 0.0f;
+        for (int c = 0; c < 3; ++c)
+            div += gen_face(c, i + (c == 0), j + (c == 1), k + (c == 2), D, surface, sph, nsph, imp, nimp, gdt) -
+                   gen_face(c, i, j, k, D, surface, sph, nsph, imp, nimp, gdt);
+        bv = -div;
+    }
+    b[s] = bv;
+}
+// tiles holding at least one fluid cell
+__global__ void nat_mark_fluid_tiles_kernel(const uint8_t* __restrict__ type, uint8_t* __restrict__ flags, uint64_t nslots) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nslots && type[s] == kFluid) flags[s >> 9] = 1;
+}
+// x-fastest linear array -> tile-blocked slots (and back)
+__global__ void nat_lin_tiles_f32_kernel(const float* __restrict__ src, float* __restrict__ dst, NatDims D, int to_tiles) {
+    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    if (id >= nc) return;
+    const int i = (int)(id % D.nx), j = (int)((id / D.nx) % D.ny), k = (int)(id / ((uint64_t)D.nx * D.ny));
+    const uint32_t s = nslot(i, j, k, D);
+    if (to_tiles) dst[s] = src[id];
+    else dst[id] = src[s];
+}
+
+// solution x + xg of the fluid cells in x-fastest order (0 elsewhere)
+__global__ void nat_solution_lin_kernel(const double* __restrict__ x, const float* __restrict__ xg,
+                                        const uint8_t* __restrict__ cell, NatDims D, double* __restrict__ out) {
+    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    if (id >= nc) return;
+    const int i = (int)(id % D.nx), j = (int)((id / D.nx) % D.ny), k = (int)(id / ((uint64_t)D.nx * D.ny));
+    const uint32_t s = nslot(i, j, k, D);
+    out[id] = (cell[s] & kCellFluid) ? x[s] + (double)xg[s] : 0.0;
+}
+
 // tiles touched by the stencils of occupied tiles: 3x3x3 dilation
 __global__ void nat_dilate_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ d_ntiles, NatDims D,
                                   uint8_t* __restrict__ flags) {
@@ -317,16 +400,21 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
                                                         PcgBuffers B) {
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
-    double bb = 0.0, rz = 0.0;
+    double bb = 0.0, rz = 0.0, nf = 0.0;
     NAT_TILE_LOOP_BEGIN
     float b = 0.0f;
     uint8_t code = 0;
     if (type[s] == kFluid) {
-        float up = (i + 1 < D.nx) ? u[nslot(i + 1, j, k, D)] : 0.0f;
-        float vp = (j + 1 < D.ny) ? v[nslot(i, j + 1, k, D)] : 0.0f;
-        float wp = (k + 1 < D.nz) ? w[nslot(i, j, k + 1, D)] : 0.0f;
-        float div = ((up - u[s]) + (vp - v[s])) + (wp - w[s]);
-        b = -div;
+        if (u) {
+            float up = (i + 1 < D.nx) ? u[nslot(i + 1, j, k, D)] : 0.0f;
+            float vp = (j + 1 < D.ny) ? v[nslot(i, j + 1, k, D)] : 0.0f;
+            float wp = (k + 1 < D.nz) ? w[nslot(i, j, k + 1, D)] : 0.0f;
+            float div = ((up - u[s]) + (vp - v[s])) + (wp - w[s]);
+            b = -div;
+        } else {
+            b = B.b[s];
+        }
+        nf += 1.0;
         uint32_t dcount = 0;
         dcount += nat_type(type, i - 1, j, k, D) != kSolid;
         dcount += nat_type(type, i + 1, j, k, D) != kSolid;
@@ -346,10 +434,13 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     bb += (double)b * (double)b;
     rz += (double)b * (double)z;
     NAT_TILE_LOOP_END
-    double vals[2] = {bb, rz}, out[2];
-    if (last_block_reduce<2>(vals, B.partials, &B.st->ticket, sh, out) && threadIdx.x == 0) {
+    double vals[3] = {bb, rz, nf}, out[3];
+    if (last_block_reduce<3>(vals, B.partials, &B.st->ticket, sh, out) && threadIdx.x == 0) {
         PcgState* st = B.st;
         st->bb = out[0];
+        st->nfluid = out[2];
+        st->inv_s = out[0] > 0.0 ? (float)(1.0 / sqrt(out[0] / fmax(out[2], 1.0))) : 1.0f;
+        st->zq = 0.0;
         st->rz = out[1];
         st->rz_prev = out[1];
         st->rr = out[0];
@@ -359,6 +450,7 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
         st->iter = 0;
         st->pending = 0;
         st->done = (out[0] == 0.0) ? 1 : 0;
+        st->halt = st->done;
     }
 }
 
@@ -372,6 +464,10 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
 // this kernel also folds xg into x (no neighbour reads of x happen here).
 __device__ __forceinline__ float dir_value(const float* tab, uint8_t c, float r, float p, float beta) {
     return (c & kCellFluid) ? fmaf(beta, p, r * jacobi_inv_s(tab, c)) : 0.0f;
+}
+// flexible PCG: the preconditioned residual z is given
+__device__ __forceinline__ float dir_value_z(uint8_t c, float z, float p, float beta) {
+    return (c & kCellFluid) ? fmaf(beta, p, z) : 0.0f;
 }
 
 struct DirLoads {
@@ -405,6 +501,7 @@ __device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict
     }
 }
 
+template <bool kFlex>
 __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* __restrict__ tiles,
                                                                 const uint32_t* __restrict__ tcoord,
                                                                 const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -443,10 +540,10 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
     for (; t < ntiles; t += gridDim.x) {
         const uint32_t s = (cur.key << 9) | tid;
         const uint8_t c = cur.c;
-        const float pc = dir_value(tab, c, cur.r, cur.p, beta);
+        const float pc = kFlex ? dir_value_z(c, cur.r, cur.p, beta) : dir_value(tab, c, cur.r, cur.p, beta);
         P[bc] = pc;
         pn[s] = pc;
-        if (face < 6) P[bh] = dir_value(tab, cur.hc, cur.hr, cur.hp, beta);
+        if (face < 6) P[bh] = kFlex ? dir_value_z(cur.hc, cur.hr, cur.hp, beta) : dir_value(tab, cur.hc, cur.hr, cur.hp, beta);
         if (flush && (c & kCellFluid)) {
             x[s] += (double)xg[s];
             xg[s] = 0.0f;
@@ -538,11 +635,15 @@ __global__ void __launch_bounds__(512, 3) pcg_update_kernel(const uint32_t* __re
         st->iter += 1;
         st->pcur ^= 1;
         st->rr = out[0];
-        st->rz_prev = st->rz;
-        st->rz = out[1];
-        st->beta = st->rz / st->rz_prev;
+        if (!st->flexible) {
+            st->rz_prev = st->rz;
+            st->rz = out[1];
+            st->beta = st->rz / st->rz_prev;
+        }
+        st->inv_s = out[0] > 0.0 ? (float)(1.0 / sqrt(out[0] / fmax(st->nfluid, 1.0))) : 1.0f;
         if (out[0] <= st->tol2 * st->bb) st->pending = 1;  // confirm with the true residual
         else if (st->iter >= st->max_iter) st->done = 2;
+        st->halt = st->done || st->pending;
     }
 }
 
@@ -613,11 +714,58 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
             st->done = 1;
         } else {
             st->flush = 1;
-            st->rz = out[1];
-            st->beta = st->rz / st->rz_prev;
+            if (!st->flexible) {
+                st->rz = out[1];
+                st->beta = st->rz / st->rz_prev;
+            }
+            st->inv_s = (float)(1.0 / sqrt(out[0] / fmax(st->nfluid, 1.0)));
             if (st->iter >= st->max_iter) st->done = 2;
         }
         st->pending = 0;
+        st->halt = st->done;
+    }
+}
+
+// flexible CG (Notay's FCG(1), the same recurrence as Polak-Ribiere PCG):
+// after z = N(r), the new direction p' = z + beta p is A-orthogonal to p for
+// beta = -z.q / p.q (q = A p), and alpha = r.z / p'.q' is the exact line
+// search along p' (r is orthogonal to p).  A nonlinear N may give r.z < 0;
+// alpha is then negative and the step still minimises the A-norm error along
+// p', so only r.z = 0 (no progress possible) or a non-finite value ends the
+// solve.  init: beta = 0.
+__global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __restrict__ tiles,
+                                                           const uint32_t* __restrict__ d_ntiles, const float* __restrict__ r,
+                                                           const float* __restrict__ z, const float* __restrict__ q,
+                                                           const uint8_t* __restrict__ cell, int init, PcgState* st,
+                                                           double* partials) {
+    if (st->halt) return;
+    __shared__ double sh[32];
+    const uint32_t nquads = *d_ntiles * 128u;
+    double rz = 0.0, zq = 0.0;
+    for (uint32_t qd = blockIdx.x * 512u + threadIdx.x; qd < nquads; qd += gridDim.x * 512u) {
+        const uint32_t s = (tiles[qd >> 7] << 9) | ((qd & 127u) << 2);
+        const uint32_t c4 = *reinterpret_cast<const uint32_t*>(cell + s);
+        if (!c4) continue;
+        const float4 r4 = *reinterpret_cast<const float4*>(r + s);
+        const float4 z4 = *reinterpret_cast<const float4*>(z + s);
+        const float4 q4 = *reinterpret_cast<const float4*>(q + s);
+        const float* rv = &r4.x;
+        const float* zv = &z4.x;
+        const float* qv = &q4.x;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (!((c4 >> (8 * m)) & kCellFluid)) continue;
+            rz += (double)rv[m] * (double)zv[m];
+            zq += (double)zv[m] * (double)qv[m];
+        }
+    }
+    double vals[2] = {rz, zq}, out[2];
+    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->beta = init ? 0.0 : (st->pq > 0.0 ? -out[1] / st->pq : 0.0);
+        st->rz = out[0];
+        st->rz_prev = out[0];
+        st->zq = out[1];
+        if (out[0] == 0.0 || !isfinite(out[0]) || !isfinite(out[1])) { st->done = 3; st->halt = 1; }
     }
 }
 
@@ -717,6 +865,33 @@ int nat_launch_tile_coords(const uint32_t* tile_keys, const uint32_t* d_ntiles, 
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+int nat_launch_poisson_gen(const NatDims& D, float surface, const float4* sph, int nsph, const float* imp, int nimp,
+                           float gdt, uint8_t* type, float* b, uint64_t nslots, cudaStream_t s) {
+    nat_poisson_gen_kernel<<<nb(nslots, 256), 256, 0, s>>>(D, surface, sph, nsph, imp, nimp, gdt, type, b, nslots);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_total, uint32_t* list, uint32_t* d_count,
+                           uint64_t nslots, cudaStream_t s) {
+    FLIP_CUDA_TRY(cudaMemsetAsync(flags, 0, ntiles_total, s));
+    nat_mark_fluid_tiles_kernel<<<nb(nslots, 256), 256, 0, s>>>(type, flags, nslots);
+    nat_compact_kernel<<<1, kCompactThreads, 0, s>>>(flags, ntiles_total, list, d_count);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_lin_tiles_f32(const float* src, float* dst, const NatDims& D, int to_tiles, cudaStream_t s) {
+    uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    nat_lin_tiles_f32_kernel<<<nb(nc, 256), 256, 0, s>>>(src, dst, D, to_tiles);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_solution_lin(const double* x, const float* xg, const uint8_t* cell, const NatDims& D, double* out,
+                            cudaStream_t s) {
+    uint64_t nc = (uint64_t)D.nx * D.ny * D.nz;
+    nat_solution_lin_kernel<<<nb(nc, 256), 256, 0, s>>>(x, xg, cell, D, out);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
                               uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s) {
     nat_dilate_kernel<<<grid, 256, 0, s>>>(tile_keys, d_ntiles, D, flags);
@@ -747,9 +922,23 @@ int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const N
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                                     cudaStream_t s) {
+    pcg_dirmatvec_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell, B.q, B.x,
+                                                          B.xg, B.st, B.partials);
+    pcg_update_kernel<<<kPcgUpdateBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell, B.st,
+                                                       B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s) {
+    fpcg_dot_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, B.r, B.z, B.q, B.cell, init, B.st, B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                              cudaStream_t s) {
-    pcg_dirmatvec_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
+    pcg_dirmatvec_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
                                                     B.st, B.partials);
     pcg_update_kernel<<<kPcgUpdateBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell, B.st,
                                                        B.partials);

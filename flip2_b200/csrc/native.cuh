@@ -23,6 +23,10 @@ struct PcgState {
     int pcur;   // which p buffer holds the current direction
     int flush;  // fold xg into x at the next direction update
     unsigned int ticket;
+    int halt;   // done || pending: the network and dot kernels of FPCG stop too
+    float inv_s;  // 1 / rms(r) over fluid cells: input scale of the learned preconditioner
+    int flexible; // 1: FPCG (z = N(r) given), 0: Jacobi PCG
+    double zq, nfluid;
 };
 
 constexpr int kPcgBlocks = 592;        // 148 SMs x 4 CTAs of 512 threads
@@ -40,7 +44,7 @@ constexpr int kPcgUpdateBlocks = 444;  // 148 SMs x 3 CTAs (the update keeps two
 // Jacobi diagonal), 0 for every other cell.
 struct PcgBuffers {
     double* x;
-    float *xg, *b, *r, *p0, *p1, *q;
+    float *xg, *b, *r, *p0, *p1, *q, *z;
     uint8_t* cell;
     uint32_t* tcoord;  // packed tile coordinates of the occupied tiles
     PcgState* st;
@@ -58,12 +62,24 @@ int nat_launch_tile_coords(const uint32_t* tile_keys, const uint32_t* d_ntiles, 
                            int grid, cudaStream_t s);
 int nat_launch_dilate_compact(const uint32_t* tile_keys, const uint32_t* d_ntiles, const NatDims& D, uint8_t* flags,
                               uint32_t* list, uint32_t* d_count, int grid, cudaStream_t s);
+int nat_launch_poisson_gen(const NatDims& D, float surface, const float4* sph, int nsph, const float* imp, int nimp,
+                           float gdt, uint8_t* type, float* b, uint64_t nslots, cudaStream_t s);
+int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_total, uint32_t* list, uint32_t* d_count,
+                           uint64_t nslots, cudaStream_t s);
+int nat_launch_lin_tiles_f32(const float* src, float* dst, const NatDims& D, int to_tiles, cudaStream_t s);
+int nat_launch_solution_lin(const double* x, const float* xg, const uint8_t* cell, const NatDims& D, double* out,
+                            cudaStream_t s);
 int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s);
 int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s);
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
                          const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s);
+// U == nullptr: the right-hand side is already in B.b (standalone Poisson problems)
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s);
+// flexible PCG: direction from z (B.z), and the r.z / z.q reduction giving beta
+int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                                     cudaStream_t s);
+int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s);
 // one PCG iteration: fused direction update + matvec (+ p.Ap), then the
 // x/r update (+ r.r, r.z); the two p buffers alternate under device control
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,

@@ -161,9 +161,10 @@ typedef struct {
     int32_t true_residual_every; /* NATIVE: FP64 r = b - A x recomputation period   */
     int32_t permute_velocities;  /* REFERENCE: 0 = keep the reference's order (Q5)  */
     int32_t device;              /* CUDA device ordinal                             */
-    int32_t reserved0;
+    int32_t pressure_method;     /* NATIVE: 0 Jacobi-PCG, 1 learned-preconditioned FPCG */
     double max_substep_dt;       /* NATIVE: largest sub-step of solveFrame (1/240)  */
-    int32_t reserved[4];
+    int32_t learned_max_iter;    /* NATIVE: FPCG cap before the Jacobi-PCG restart   */
+    int32_t reserved[3];
 } flip_params;
 
 /* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */
@@ -229,6 +230,62 @@ int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, 
 /* Copy a buffer of flip_get_buffer to host memory (bytes <= count*elem_size),
  * synchronising the engine stream; CudaVec::download (cudaVec.cu:80-86). */
 int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint64_t bytes);
+
+/* ------------------------------------------------------------------ */
+/* 3. Learned pressure preconditioner and standalone pressure problems  */
+/*    (north-star additions: no reference counterpart)                  */
+/* ------------------------------------------------------------------ */
+/* The network: 3^3 convolutions 3 -> 16 -> 16 -> 16 -> 1 channels with
+ * dilations 1, 2, 4, 1, ReLU after the first three, no biases; inputs are
+ * [r / rms(r), fluid flag, solid flag], the output is scaled by rms(r) and
+ * kept on fluid cells.  BF16 weights and activations, FP32 accumulation.
+ * Weights: FP32, layer after layer, each [27 taps][Cin][Cout]. */
+uint64_t flip_lp_num_weights(void);
+int flip_lp_init(flip_engine* e, uint64_t seed);                      /* He-normal init, Adam reset */
+int flip_lp_set_weights(flip_engine* e, const float* w, uint64_t n);
+int flip_lp_get_weights(flip_engine* e, float* w, uint64_t n);
+int flip_lp_get_grad(flip_engine* e, float* g, uint64_t n);           /* last weight gradient       */
+
+/* A pressure problem on the whole native grid (the learned-preconditioner
+ * configuration): solid spheres, fluid below a surface, air above, and
+ * b = -div(u) of Gaussian velocity impulses plus gravity. */
+typedef struct {
+    uint64_t seed;
+    double surface_min, surface_max;   /* fluid surface height, fraction of ny        */
+    double solid_fraction;             /* target solid volume fraction (0.10)         */
+    double radius_min, radius_max;     /* sphere radii in voxels (4..16)              */
+    int32_t impulses;                  /* Gaussian velocity impulses                  */
+    int32_t reserved;
+    double gravity_dt;                 /* gravity * dt added on fluid y faces         */
+} flip_poisson_spec;
+int flip_poisson_generate(flip_engine* e, const flip_poisson_spec* spec);
+/* explicit problem: cell types (0 air, 1 fluid, 2 solid) and b, x fastest */
+int flip_poisson_set(flip_engine* e, const uint8_t* type_lin, const float* b_lin);
+typedef struct {
+    int32_t iters;          /* iterations of the method asked for             */
+    int32_t converged;      /* 1: true relative residual <= tol               */
+    int32_t fell_back;      /* 1: FPCG missed its cap and Jacobi-PCG restarted */
+    int32_t plain_iters;    /* iterations of that restart                     */
+    double rel_residual;    /* FP64 true residual / |b|                       */
+    double ms;              /* device time of the solve                       */
+} flip_solve_info;
+/* the last pressure solve: flip_poisson_solve's or a native step's (ms is
+ * measured for a step only while stage timing is on).  After a native step
+ * its pressure problem stays in place for flip_poisson_solve,
+ * flip_lp_train_step and flip_lp_eval until the next step. */
+int flip_get_solve_info(flip_engine* e, flip_solve_info* out);
+/* method 0: Jacobi-PCG; 1: learned FPCG with Jacobi-PCG fallback */
+int flip_poisson_solve(flip_engine* e, int method, double tol, int max_iter, flip_solve_info* info);
+/* solution (FP64) in x-fastest order */
+int flip_poisson_read_solution(flip_engine* e, double* x_lin);
+/* one training step on the current problem: Jacobi-PCG runs pcg_iters
+ * iterations from b, its residual r is the sample, loss
+ * |A N(r) - r|^2 / |r|^2, one Adam step at rate lr; *loss before the step */
+int flip_lp_train_step(flip_engine* e, int pcg_iters, float lr, double* loss);
+/* evaluate N on a given residual (x fastest) of the current problem: z out
+ * (x fastest, may be NULL), the loss, and with want_grad the weight
+ * gradient (flip_lp_get_grad) without updating the weights */
+int flip_lp_eval(flip_engine* e, const float* r_lin, float* z_lin, double* loss, int want_grad);
 
 typedef struct {
     uint32_t nodes;          /* occupied root cells (REFERENCE) / tiles (NATIVE)   */

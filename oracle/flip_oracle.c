@@ -896,3 +896,297 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
     free(type); free(b); free(x);
     return 0;
 }
+
+/* ============================================ learned preconditioner (CPU)
+ * The product's pressure-preconditioner network, restated for the parity
+ * tests (it has no reference counterpart).  Grids are x fastest, nx*ny*nz.
+ * Four 3^3 convolutions, channels 3 -> 16 -> 16 -> 16 -> 1, dilations dil[],
+ * ReLU after the first three, zero padding outside the box.  Weights are
+ * [27 taps][Cin][Cout] per layer with tap = 9 (dz+1) + 3 (dy+1) + (dx+1) and
+ * the neighbour at (i + dil dx, j + dil dy, k + dil dz).  Inputs at a cell:
+ * r/s (fluid only), fluid flag, solid flag with s = rms of r over the fluid
+ * cells; the output is s * N and zero off fluid cells.
+ * round_bf16 = 1 rounds the weights and the three hidden activations to
+ * BF16 (round to nearest even), as the CUDA kernels store them; sums are
+ * FP64 here and FP32 on the GPU. */
+static const int LP_CIN[4] = {3, 16, 16, 16}, LP_COUT[4] = {16, 16, 16, 1};
+static const int LP_OFF[5] = {0, 27 * 3 * 16, 27 * 3 * 16 + 27 * 256, 27 * 3 * 16 + 2 * 27 * 256,
+                              27 * 3 * 16 + 2 * 27 * 256 + 27 * 16};
+
+static float bf16_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u) return x; /* inf / nan unchanged */
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    u &= 0xFFFF0000u;
+    float y;
+    memcpy(&y, &u, 4);
+    return y;
+}
+
+typedef struct {
+    int nx, ny, nz;
+    int64_t nc;
+} lp_dims;
+
+static inline int64_t lp_at(const lp_dims* D, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= D->nx || j >= D->ny || k >= D->nz) return -1;
+    return i + (int64_t)D->nx * (j + (int64_t)D->ny * k);
+}
+
+/* 7-point operator on the fluid cells, as the PCG uses it (walls solid) */
+static void lp_apply_A(const lp_dims* D, const uint8_t* type, const double* x, double* y) {
+    static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < D->nz; ++k)
+        for (int j = 0; j < D->ny; ++j)
+            for (int i = 0; i < D->nx; ++i) {
+                int64_t id = lp_at(D, i, j, k);
+                if (type[id] != NAT_FLUID) { y[id] = 0.0; continue; }
+                double d = 0.0, s = 0.0;
+                for (int q = 0; q < 6; ++q) {
+                    int64_t n = lp_at(D, i + off[q][0], j + off[q][1], k + off[q][2]);
+                    if (n < 0 || type[n] == NAT_SOLID) continue;
+                    d += 1.0;
+                    if (type[n] == NAT_FLUID) s += x[n];
+                }
+                y[id] = d * x[id] - s;
+            }
+}
+
+/* one convolution layer: out[v][co] = sum_tap sum_ci W[tap][ci][co] in[v+dil*off][ci] */
+static void lp_conv(const lp_dims* D, const float* in, int cin, const float* W, int cout, int dil, double* out) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < D->nz; ++k)
+        for (int j = 0; j < D->ny; ++j)
+            for (int i = 0; i < D->nx; ++i) {
+                int64_t v = lp_at(D, i, j, k);
+                double acc[16] = {0};
+                for (int tap = 0; tap < 27; ++tap) {
+                    int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                    int64_t u = lp_at(D, i + dil * dx, j + dil * dy, k + dil * dz);
+                    if (u < 0) continue;
+                    for (int ci = 0; ci < cin; ++ci) {
+                        double x = in[u * cin + ci];
+                        if (x == 0.0) continue;
+                        const float* w = W + (tap * cin + ci) * cout;
+                        for (int co = 0; co < cout; ++co) acc[co] += (double)w[co] * x;
+                    }
+                }
+                for (int co = 0; co < cout; ++co) out[v * cout + co] = acc[co];
+            }
+}
+
+/* forward pass; keeps the inputs and activations for the backward pass */
+typedef struct {
+    float* in;      /* [nc][3]  */
+    float* act[3];  /* [nc][16] */
+    float* wr;      /* weights as used (rounded or not) */
+    float inv_s, s;
+} lp_fwd;
+
+static void lp_forward_keep(const lp_dims* D, const uint8_t* type, const float* r, const float* w, const int* dil,
+                            int round_bf16, float* z, lp_fwd* F) {
+    const int64_t nc = D->nc;
+    F->wr = (float*)malloc(sizeof(float) * LP_OFF[4]);
+    for (int i = 0; i < LP_OFF[4]; ++i) F->wr[i] = round_bf16 ? bf16_round(w[i]) : w[i];
+    double rr = 0.0, nf = 0.0;
+    for (int64_t v = 0; v < nc; ++v)
+        if (type[v] == NAT_FLUID) { rr += (double)r[v] * (double)r[v]; nf += 1.0; }
+    F->inv_s = rr > 0.0 ? (float)(1.0 / sqrt(rr / (nf > 1.0 ? nf : 1.0))) : 1.0f;
+    F->s = 1.0f / F->inv_s;
+    F->in = (float*)malloc(sizeof(float) * 3 * nc);
+    for (int64_t v = 0; v < nc; ++v) {
+        int fl = type[v] == NAT_FLUID;
+        F->in[3 * v] = fl ? r[v] * F->inv_s : 0.0f;
+        F->in[3 * v + 1] = fl ? 1.0f : 0.0f;
+        F->in[3 * v + 2] = type[v] == NAT_SOLID ? 1.0f : 0.0f;
+    }
+    double* tmp = (double*)malloc(sizeof(double) * 16 * nc);
+    const float* cur = F->in;
+    for (int l = 0; l < 3; ++l) {
+        lp_conv(D, cur, LP_CIN[l], F->wr + LP_OFF[l], 16, dil[l], tmp);
+        F->act[l] = (float*)malloc(sizeof(float) * 16 * nc);
+        for (int64_t q = 0; q < 16 * nc; ++q) {
+            float a = (float)(tmp[q] > 0.0 ? tmp[q] : 0.0);
+            F->act[l][q] = round_bf16 ? bf16_round(a) : a;
+        }
+        cur = F->act[l];
+    }
+    lp_conv(D, cur, 16, F->wr + LP_OFF[3], 1, dil[3], tmp);
+    for (int64_t v = 0; v < nc; ++v) z[v] = type[v] == NAT_FLUID ? (float)tmp[v] * F->s : 0.0f;
+    free(tmp);
+}
+
+static void lp_fwd_free(lp_fwd* F) {
+    free(F->in);
+    for (int l = 0; l < 3; ++l) free(F->act[l]);
+    free(F->wr);
+}
+
+int orc_lp_num_weights(void) { return LP_OFF[4]; }
+
+void orc_lp_forward(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                    int round_bf16, float* z, double* inv_s) {
+    lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
+    lp_fwd F;
+    lp_forward_keep(&D, type, r, w, dil, round_bf16, z, &F);
+    if (inv_s) *inv_s = F.inv_s;
+    lp_fwd_free(&F);
+}
+
+/* dW[tap][ci][co] += sum_v g[v][co] in[v+dil*off][ci] */
+static void lp_wgrad(const lp_dims* D, const double* g, int cout, const float* in, int cin, int dil, double* dw) {
+    const int nw = 27 * cin * cout;
+#pragma omp parallel
+    {
+        double* loc = (double*)calloc((size_t)nw, sizeof(double));
+#pragma omp for schedule(static)
+        for (int k = 0; k < D->nz; ++k)
+            for (int j = 0; j < D->ny; ++j)
+                for (int i = 0; i < D->nx; ++i) {
+                    int64_t v = lp_at(D, i, j, k);
+                    for (int tap = 0; tap < 27; ++tap) {
+                        int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                        int64_t u = lp_at(D, i + dil * dx, j + dil * dy, k + dil * dz);
+                        if (u < 0) continue;
+                        for (int co = 0; co < cout; ++co) {
+                            double gv = g[v * cout + co];
+                            if (gv == 0.0) continue;
+                            for (int ci = 0; ci < cin; ++ci) loc[(tap * cin + ci) * cout + co] += gv * in[u * cin + ci];
+                        }
+                    }
+                }
+#pragma omp critical
+        for (int q = 0; q < nw; ++q) dw[q] += loc[q];
+        free(loc);
+    }
+}
+
+/* gin[u][ci] = mask(u,ci) * sum_tap sum_co W[tap][ci][co] g[u - dil*off][co] */
+static void lp_dgrad(const lp_dims* D, const double* g, int cout, const float* W, int cin, int dil, const float* act,
+                     double* gin) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < D->nz; ++k)
+        for (int j = 0; j < D->ny; ++j)
+            for (int i = 0; i < D->nx; ++i) {
+                int64_t u = lp_at(D, i, j, k);
+                double acc[16] = {0};
+                for (int tap = 0; tap < 27; ++tap) {
+                    int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                    int64_t v = lp_at(D, i - dil * dx, j - dil * dy, k - dil * dz);
+                    if (v < 0) continue;
+                    for (int co = 0; co < cout; ++co) {
+                        double gv = g[v * cout + co];
+                        if (gv == 0.0) continue;
+                        for (int ci = 0; ci < cin; ++ci) acc[ci] += (double)W[(tap * cin + ci) * cout + co] * gv;
+                    }
+                }
+                for (int ci = 0; ci < cin; ++ci) gin[u * cin + ci] = act[u * cin + ci] > 0.0f ? acc[ci] : 0.0;
+            }
+}
+
+/* loss L = |A z - r|^2 / |r|^2 over the fluid cells and its gradient with
+ * respect to the (unrounded) weights; the BF16 roundings pass the gradient
+ * straight through.  Returns L; z and grad (orc_lp_num_weights()) out. */
+double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                        int round_bf16, float* z, double* grad) {
+    lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
+    const int64_t nc = D.nc;
+    lp_fwd F;
+    lp_forward_keep(&D, type, r, w, dil, round_bf16, z, &F);
+    double* zd = (double*)malloc(sizeof(double) * nc);
+    double* e = (double*)malloc(sizeof(double) * nc);
+    double* gz = (double*)malloc(sizeof(double) * nc);
+    for (int64_t v = 0; v < nc; ++v) zd[v] = z[v];
+    lp_apply_A(&D, type, zd, e);
+    double l2 = 0.0, nf = 0.0;
+    for (int64_t v = 0; v < nc; ++v) {
+        if (type[v] != NAT_FLUID) { e[v] = 0.0; continue; }
+        e[v] = (e[v] - (double)r[v]) * (double)F.inv_s;
+        l2 += e[v] * e[v];
+        nf += 1.0;
+    }
+    if (nf < 1.0) nf = 1.0;
+    const double loss = l2 / nf;
+    if (grad) {
+        memset(grad, 0, sizeof(double) * LP_OFF[4]);
+        lp_apply_A(&D, type, e, gz);
+        /* dL/d(out of layer 3) = s * dL/dz, dL/dz = 2 A e inv_s / nf on fluid cells */
+        for (int64_t v = 0; v < nc; ++v)
+            gz[v] = type[v] == NAT_FLUID ? gz[v] * 2.0 * (double)F.inv_s / nf * (double)F.s : 0.0;
+        double* g = (double*)malloc(sizeof(double) * 16 * nc);
+        double* g2 = (double*)malloc(sizeof(double) * 16 * nc);
+        lp_wgrad(&D, gz, 1, F.act[2], 16, dil[3], grad + LP_OFF[3]);
+        lp_dgrad(&D, gz, 1, F.wr + LP_OFF[3], 16, dil[3], F.act[2], g);
+        lp_wgrad(&D, g, 16, F.act[1], 16, dil[2], grad + LP_OFF[2]);
+        lp_dgrad(&D, g, 16, F.wr + LP_OFF[2], 16, dil[2], F.act[1], g2);
+        lp_wgrad(&D, g2, 16, F.act[0], 16, dil[1], grad + LP_OFF[1]);
+        lp_dgrad(&D, g2, 16, F.wr + LP_OFF[1], 16, dil[1], F.act[0], g);
+        lp_wgrad(&D, g, 16, F.in, 3, dil[0], grad + LP_OFF[0]);
+        free(g);
+        free(g2);
+    }
+    free(zd);
+    free(e);
+    free(gz);
+    lp_fwd_free(&F);
+    return loss;
+}
+
+/* flexible CG (FCG(1)) with the network as preconditioner, in
+ * FP64 apart from the network; returns iterations (max_iter + 1 if not
+ * converged), x out, *rel_res = |b - A x| / |b| */
+int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
+                int round_bf16, double tol, int max_iter, double* x, double* rel_res) {
+    lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
+    const int64_t nc = D.nc;
+    double *r = (double*)calloc((size_t)nc, 8), *p = (double*)calloc((size_t)nc, 8), *q = (double*)calloc((size_t)nc, 8),
+           *zd = (double*)calloc((size_t)nc, 8);
+    float *rf = (float*)calloc((size_t)nc, 4), *zf = (float*)calloc((size_t)nc, 4);
+    double bb = 0.0;
+    for (int64_t v = 0; v < nc; ++v) {
+        x[v] = 0.0;
+        r[v] = type[v] == NAT_FLUID ? b[v] : 0.0;
+        bb += r[v] * r[v];
+    }
+    const double bn = sqrt(bb);
+    int it = 0;
+    double pq_prev = 0.0;
+    if (bn > 0.0) {
+        for (it = 1; it <= max_iter + 1; ++it) {
+            for (int64_t v = 0; v < nc; ++v) rf[v] = (float)r[v];
+            orc_lp_forward(nx, ny, nz, type, rf, w, dil, round_bf16, zf, NULL);
+            double rzn = 0.0, zq = 0.0;
+            for (int64_t v = 0; v < nc; ++v) {
+                zd[v] = zf[v];
+                rzn += r[v] * zd[v];
+                zq += zd[v] * q[v];
+            }
+            if (rzn == 0.0 || !isfinite(rzn)) break;
+            /* FCG(1): p = z + beta p A-orthogonal to the previous p, beta = -z.q / p.q */
+            const double beta = it == 1 ? 0.0 : -zq / pq_prev;
+            for (int64_t v = 0; v < nc; ++v) p[v] = zd[v] + beta * p[v];
+            lp_apply_A(&D, type, p, q);
+            double pq = 0.0;
+            for (int64_t v = 0; v < nc; ++v) pq += p[v] * q[v];
+            if (!(pq > 0.0)) break;
+            const double alpha = rzn / pq; /* exact line search: r is orthogonal to the previous p */
+            pq_prev = pq;
+            double rr = 0.0;
+            for (int64_t v = 0; v < nc; ++v) {
+                x[v] += alpha * p[v];
+                r[v] -= alpha * q[v];
+                rr += r[v] * r[v];
+            }
+            if (sqrt(rr) <= tol * bn) break;
+        }
+    }
+    lp_apply_A(&D, type, x, q);
+    double rr = 0.0;
+    for (int64_t v = 0; v < nc; ++v)
+        if (type[v] == NAT_FLUID) { double d = b[v] - q[v]; rr += d * d; }
+    if (rel_res) *rel_res = bn > 0.0 ? sqrt(rr) / bn : 0.0;
+    free(r); free(p); free(q); free(zd); free(rf); free(zf);
+    return it;
+}

@@ -161,6 +161,16 @@ int orc_nat_pcg(const uint8_t* type, const double* b, double* x, const orc_nat_p
 /* Apply the 7-point operator (for residual checks). */
 void orc_nat_apply_A(const uint8_t* type, const double* x, double* y, const orc_nat_params* P);
 
+/* Learned pressure preconditioner (no reference counterpart): grids x
+ * fastest, weights [27 taps][Cin][Cout] per layer (3->16->16->16->1). */
+int orc_lp_num_weights(void);
+void orc_lp_forward(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                    int round_bf16, float* z, double* inv_s);
+double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                        int round_bf16, float* z, double* grad);
+int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
+                int round_bf16, double tol, int max_iter, double* x, double* rel_res);
+
 #ifdef __cplusplus
 }
 #endif

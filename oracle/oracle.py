@@ -17,6 +17,7 @@ f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
 u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
 class Grid(C.Structure):
@@ -77,6 +78,10 @@ def lib():
             "orc_nat_p2g": (None, [I64, f32p, f32p, C.POINTER(NatParams), f64p, f64p, f64p, u8p]),
             "orc_nat_pcg": (I, [u8p, f64p, f64p, C.POINTER(NatParams), C.POINTER(D)]),
             "orc_nat_apply_A": (None, [u8p, f64p, f64p, C.POINTER(NatParams)]),
+            "orc_lp_num_weights": (I, []),
+            "orc_lp_forward": (None, [I, I, I, u8p, f32p, f32p, i32p, I, f32p, C.POINTER(D)]),
+            "orc_lp_loss_grad": (D, [I, I, I, u8p, f32p, f32p, i32p, I, f32p, f64p]),
+            "orc_lp_fpcg": (I, [I, I, I, u8p, f64p, f32p, i32p, I, D, I, f64p, C.POINTER(D)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -253,3 +258,39 @@ def nat_apply_A(type_, x, P):
     y = np.empty(x.size, np.float64)
     lib().orc_nat_apply_A(np.ascontiguousarray(type_, np.uint8), np.ascontiguousarray(x, np.float64), y, C.byref(P))
     return y
+
+
+LP_DIL = (1, 2, 4, 1)
+
+
+def lp_forward(type_, r, w, shape, dil=LP_DIL, round_bf16=True):
+    """z = s N(r) of the learned preconditioner; shape (nx, ny, nz), arrays x fastest."""
+    nx, ny, nz = shape
+    z = np.empty(nx * ny * nz, np.float32)
+    inv_s = C.c_double(0.0)
+    lib().orc_lp_forward(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(), np.ascontiguousarray(r, np.float32).ravel(),
+                         np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16), z,
+                         C.byref(inv_s))
+    return z, inv_s.value
+
+
+def lp_loss_grad(type_, r, w, shape, dil=LP_DIL, round_bf16=True):
+    """(loss, z, dloss/dw) of the residual loss |A z - r|^2 / |r|^2."""
+    nx, ny, nz = shape
+    z = np.empty(nx * ny * nz, np.float32)
+    g = np.empty(lib().orc_lp_num_weights(), np.float64)
+    loss = lib().orc_lp_loss_grad(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(),
+                                  np.ascontiguousarray(r, np.float32).ravel(), np.ascontiguousarray(w, np.float32),
+                                  np.ascontiguousarray(dil, np.int32), int(round_bf16), z, g)
+    return loss, z, g
+
+
+def lp_fpcg(type_, b, w, shape, tol=1e-6, max_iter=1000, dil=LP_DIL, round_bf16=True):
+    """Flexible PCG with the network as preconditioner: (x, iterations, relative residual)."""
+    nx, ny, nz = shape
+    x = np.zeros(nx * ny * nz, np.float64)
+    rr = C.c_double(0.0)
+    it = lib().orc_lp_fpcg(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(), np.ascontiguousarray(b, np.float64).ravel(),
+                           np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16), tol,
+                           max_iter, x, C.byref(rr))
+    return x, it, rr.value
