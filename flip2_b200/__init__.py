@@ -55,7 +55,8 @@ class Params(C.Structure):
     _fields_ = [("mode", C.c_int32), ("flip_ratio", C.c_float), ("gravity_y", C.c_float), ("pcg_tol", C.c_double),
                 ("pcg_max_iter", C.c_int32), ("pcg_check_every", C.c_int32), ("true_residual_every", C.c_int32),
                 ("permute_velocities", C.c_int32), ("device", C.c_int32), ("pressure_method", C.c_int32),
-                ("max_substep_dt", C.c_double), ("learned_max_iter", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("max_substep_dt", C.c_double), ("learned_max_iter", C.c_int32), ("lp_cuda_cores", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class PoissonSpec(C.Structure):

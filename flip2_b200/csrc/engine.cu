@@ -190,6 +190,7 @@ static void free_lp_activations(flip_engine* e) {
     e->lp.gact = e->lp.gact2 = nullptr;
     e->pcg.z = nullptr;
     e->lp_scalar = nullptr;
+    e->lp.err = nullptr;
 }
 static void free_arena(flip_engine* e) {
     free_lp_activations(e);
@@ -671,6 +672,8 @@ static int lp_alloc_weights(flip_engine* e) {
     const int dil[kLpLayers] = {1, 2, 4, 1};
     for (int l = 0; l < kLpLayers; ++l) e->lp.dil[l] = dil[l];
     e->lp.adam_t = 0;
+    e->lp.tensor_cores = e->P.lp_cuda_cores ? 0 : 1;
+    e->lp.sms = e->sms;
     return FLIP_OK;
 }
 // activations for every slot of the grid: 3 x 16 BF16 + 2 x 16 FP32 + z
@@ -687,6 +690,7 @@ static int lp_alloc_activations(flip_engine* e) {
     e->lp.gact2 = (float*)(e->lp_aarena + 3 * ab + gb);
     e->pcg.z = (float*)(e->lp_aarena + 3 * ab + 2 * gb);
     e->lp_scalar = (double*)(e->lp_aarena + 3 * ab + 2 * gb + zb);
+    e->lp.err = (int*)(e->lp_aarena + 3 * ab + 2 * gb + zb + 16);
     return FLIP_OK;
 }
 // the network's view of the current problem: activations on the dilated
@@ -703,6 +707,15 @@ static LpGrid lp_grid(flip_engine* e, const int* halt) {
     G.halt = halt;
     G.D = e->D;
     return G;
+}
+// the tensor-core kernels' error word: a bounded wait that gave up
+static int lp_check_err(flip_engine* e) {
+    if (!e->lp.err) return FLIP_OK;
+    int w = 0;
+    E_CUDA(cudaMemcpyAsync(&w, e->lp.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    if (w) return e->fail(FLIP_ERR_TIMEOUT, "learned preconditioner: a tensor-core wait timed out");
+    return FLIP_OK;
 }
 static int lp_ready(flip_engine* e) {
     if (!e->lp_have_weights) return e->fail(FLIP_ERR_STATE, "learned preconditioner: no weights (flip_lp_init or flip_lp_set_weights)");
@@ -782,6 +795,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(e->mark(9));
         E_TRY(nat_fpcg_graph(e, chunk));
         E_TRY(run_chunks(e, e->fpcg_graph, chunk, 7u * (uint32_t)chunk + 1u, max_learned));
+        E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
         double rr = s.true_checks ? s.rr_true : s.rr;
@@ -1078,10 +1092,11 @@ extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
             out->pressure_iters = e->last_iters;
             out->converged = e->last_converged;
             out->residual = e->last_rel;
-            uint32_t ew[2] = {0, 0};
+            uint32_t ew[3] = {0, 0, 0};
             E_CUDA(cudaMemcpy(ew, e->sort_scratch, 4, cudaMemcpyDeviceToHost));
             E_CUDA(cudaMemcpy(ew + 1, e->scan_scratch, 4, cudaMemcpyDeviceToHost));
-            out->error_flags = ew[0] | ew[1];
+            if (e->lp.err) E_CUDA(cudaMemcpy(ew + 2, e->lp.err, 4, cudaMemcpyDeviceToHost));
+            out->error_flags = ew[0] | ew[1] | (ew[2] ? 0x4u : 0u);
         } else {
             out->nodes = e->nodes;
             out->voxels = e->voxels;
@@ -1343,7 +1358,8 @@ extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, float* z_lin, do
         E_CUDA(cudaMemcpyAsync(z_lin, e->pcg.p0, 4 * e->nslots, cudaMemcpyDeviceToHost, e->stream));
         e->launches += 1;
     }
-    return lp_read_loss(e, loss);
+    E_TRY(lp_read_loss(e, loss));
+    return lp_check_err(e);
 }
 
 extern "C" int flip_get_solve_info(flip_engine* e, flip_solve_info* out) {

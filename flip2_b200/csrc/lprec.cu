@@ -335,8 +335,14 @@ __global__ void lp_to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __
 // ------------------------------------------------------------ launchers
 int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* z, int grid, cudaStream_t st) {
     lp_in_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, net.act[0]);
-    lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.act[0], net.act[1]);
-    lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.act[1], net.act[2]);
+    if (net.tensor_cores) {
+        int rc = lp_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], net.act[0], net.act[1], net.err, net.sms, st);
+        if (rc == FLIP_OK) rc = lp_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], net.act[1], net.act[2], net.err, net.sms, st);
+        if (rc != FLIP_OK) return rc;
+    } else {
+        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.act[0], net.act[1]);
+        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.act[1], net.act[2]);
+    }
     lp_out_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], net.act[2], d_inv_s, z);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;

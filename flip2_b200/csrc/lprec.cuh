@@ -31,6 +31,9 @@ struct LpNet {
     float* gact;          // gradient of one activation layer: [slot][16]
     float* gact2;         // second gradient buffer: [slot][16]
     int adam_t;
+    int tensor_cores;     // 1: the 16 -> 16 layers of the forward pass run on tcgen05
+    int sms;              // SM count (persistent grid of the tensor-core kernels)
+    int* err;             // device error word of the tensor-core kernels (bit 0: a wait timed out)
 };
 
 // Inputs the network reads: residual r (FP32, read only at fluid cells),
@@ -49,6 +52,10 @@ struct LpGrid {
     NatDims D;
 };
 
+// one 16 -> 16 layer (ReLU) on the tensor cores: out = relu(conv(in)) on the
+// active tiles (lprec_tc.cu); dil in {1, 2, 4}
+int lp_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
+                      int* err, int sms, cudaStream_t st);
 // z = s * N([r/s, fluid, solid]) on fluid cells, 0 elsewhere; s = 1/(*d_inv_s)
 int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* z, int grid, cudaStream_t st);
 // gradient of the loss with respect to the weights given dL/dz (gz, FP32 on

@@ -1,0 +1,264 @@
+// lprec_tc.cu -- tensor-core forward of the learned preconditioner's
+// 16 -> 16 channel layers (dilated 3^3 convolutions, BF16 in, FP32
+// accumulation in tensor memory, ReLU, BF16 out) as an implicit GEMM on the
+// sm_100a UMMA unit (tcgen05.mma, kind::f16).
+//
+// One CTA works on one 8^3 tile of the active list at a time:
+//   1. stage the tile's input box (8 + 2 dil)^3 voxels x 16 channels in
+//      shared memory as two 8-channel planes, 16 B per voxel and plane, in
+//      x-fastest order; voxels outside the box or in inactive tiles read 0;
+//   2. one thread issues, for each z-slice of the tile and each of the 27
+//      taps, one M=64 x N=16 x K=16 MMA: A = the 64 voxels (8 x, 8 y) of the
+//      slice shifted by the tap, read straight from the box (rows 16 B apart,
+//      8-row groups one box row apart, the two channel planes one plane
+//      apart: the K-major no-swizzle canonical layout), B = the tap's 16 x 16
+//      weights; the 27 products accumulate into one TMEM accumulator per
+//      z-slice (8 slices x 16 columns);
+//   3. the MMAs commit to an mbarrier; every warp waits on it (bounded), reads
+//      its accumulators with tcgen05.ld, applies ReLU and stores BF16.
+// An M=64 accumulator keeps row m in TMEM lane (m % 16) + 32 (m / 16) and
+// column n at column n.  Waits are bounded: on a timeout the kernel sets an
+// error flag, waits (bounded) for its MMAs, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include "common.cuh"
+#include "lprec.cuh"
+
+namespace flip {
+
+namespace {
+constexpr int kTcThreads = 256;   // 8 warps: 2 warpgroups for the TMEM reads
+constexpr int kTcCols = 128;      // 8 z-slices x 16 FP32 columns
+constexpr uint32_t kTcSpinLimit = 1u << 24;
+constexpr uint32_t kInstrDesc = (1u << 4)           // D: FP32
+                                | (1u << 7)         // A: BF16
+                                | (1u << 10)        // B: BF16
+                                | ((16u >> 3) << 17)  // N = 16
+                                | ((64u >> 4) << 24);  // M = 64
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no swizzle: rows 16 B apart, 8-row groups sbo bytes apart, the two
+// 16-byte K halves lbo bytes apart; descriptor version 1 (sm100)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (uint32_t it = 0; it < kTcSpinLimit; ++it)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tile_origin_tc(uint32_t key, const NatDims& D, int& ox, int& oy, int& oz) {
+    ox = 8 * (int)(key % D.tx);
+    oy = 8 * (int)((key / D.tx) % D.ty);
+    oz = 8 * (int)(key / (D.tx * D.ty));
+}
+}  // namespace
+
+// shared-memory footprint of one CTA for dilation DIL
+template <int DIL>
+struct TcSmem {
+    static constexpr int B = 8 + 2 * DIL;                 // box edge
+    static constexpr int kPlane = B * B * B * 16;         // bytes of one 8-channel plane
+    static constexpr int kBox = 2 * kPlane;
+    static constexpr int kW = 27 * 512;                   // 27 taps x (16 co x 16 ci) BF16
+    static constexpr int kBytes = kBox + kW + 64;
+};
+
+template <int DIL>
+__global__ void __launch_bounds__(kTcThreads) lp_mid_tc_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb,
+                                                               const __nv_bfloat16* __restrict__ in,
+                                                               __nv_bfloat16* __restrict__ out, int* __restrict__ err) {
+    using S = TcSmem<DIL>;
+    constexpr int B = S::B;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* box = smem;
+    unsigned char* wsm = smem + S::kBox;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::kBox + S::kW);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kBox + S::kW + 16);
+    __shared__ int s_abort;
+    if (G.halt && *G.halt) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // weights: global [tap][ci][co] -> per tap [ci/8][co][ci%8] (K-major B: rows = co)
+    for (int e = tid; e < 27 * 256; e += kTcThreads) {
+        const int tap = e >> 8, ci = (e >> 4) & 15, co = e & 15;
+        const int off = tap * 512 + (ci >> 3) * 256 + co * 16 + (ci & 7) * 2;
+        *reinterpret_cast<__nv_bfloat16*>(wsm + off) = wb[e];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t box_s = smem_u32(box), w_s = smem_u32(wsm), mbar_s = smem_u32(mbar);
+    const uint32_t n = *G.d_nact;
+    uint32_t phase = 0;
+    bool pending_mma = false;
+    for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+        const uint32_t key = G.act_tiles[t];
+        int ox, oy, oz;
+        tile_origin_tc(key, G.D, ox, oy, oz);
+        // 1. input box, two 16-byte chunks per voxel
+        for (int e = tid; e < 2 * B * B * B; e += kTcThreads) {
+            const int c = e & 1, v = e >> 1;
+            const int bx = v % B, by = (v / B) % B, bz = v / (B * B);
+            const int gx = ox - DIL + bx, gy = oy - DIL + by, gz = oz - DIL + bz;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < G.D.nx && gy < G.D.ny && gz < G.D.nz) {
+                const uint32_t tt = (uint32_t)((gx >> 3) + G.D.tx * ((gy >> 3) + G.D.ty * (gz >> 3)));
+                if (G.tile_active[tt]) {
+                    const uint32_t sl = (tt << 9) | (uint32_t)((gx & 7) | ((gy & 7) << 3) | ((gz & 7) << 6));
+                    val = *reinterpret_cast<const uint4*>(in + (size_t)sl * 16 + c * 8);
+                }
+            }
+            *reinterpret_cast<uint4*>(box + c * S::kPlane + v * 16) = val;
+        }
+        // make the generic-proxy writes visible to the tensor core's async proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        // 2. 8 slices x 27 taps of M=64 N=16 K=16
+        if (tid == 0) {
+            for (int z = 0; z < 8; ++z) {
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                    const int bz = z + DIL + DIL * dz, by0 = DIL + DIL * dy, bx0 = DIL + DIL * dx;
+                    const uint32_t aoff = (uint32_t)(((bz * B + by0) * B + bx0) * 16);
+                    const uint64_t ad = umma_desc(box_s + aoff, S::kPlane, B * 16);
+                    const uint64_t bd = umma_desc(w_s + tap * 512, 256, 128);
+                    mma_f16(tmem + (uint32_t)(z * 16), ad, bd, kInstrDesc, tap > 0 ? 1u : 0u);
+                }
+            }
+            mma_commit(mbar_s);
+        }
+        pending_mma = true;
+        // 3. epilogue: warp w reads sub-partition w % 4 of slices w/4, w/4+2, w/4+4, w/4+6
+        const bool ok = mbar_wait(mbar_s, phase);
+        if (!ok) {
+            if (lane == 0) atomicExch(&s_abort, 1);
+        }
+        __syncthreads();
+        if (s_abort) break;
+        pending_mma = false;
+        phase ^= 1u;
+        tc_fence_after();
+        const int q = warp & 3;
+        for (int zz = warp >> 2; zz < 8; zz += 2) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(zz * 16), v);
+            if (lane < 16) {
+                const int m = lane + 16 * q;  // row of the slice: x = m % 8, y = m / 8
+                const uint32_t sl = (key << 9) | (uint32_t)((m & 7) | ((m >> 3) << 3) | (zz << 6));
+                uint4 o0, o1;
+                __nv_bfloat162* h0 = reinterpret_cast<__nv_bfloat162*>(&o0);
+                __nv_bfloat162* h1 = reinterpret_cast<__nv_bfloat162*>(&o1);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    h0[k] = __floats2bfloat162_rn(fmaxf(v[2 * k], 0.0f), fmaxf(v[2 * k + 1], 0.0f));
+                    h1[k] = __floats2bfloat162_rn(fmaxf(v[8 + 2 * k], 0.0f), fmaxf(v[8 + 2 * k + 1], 0.0f));
+                }
+                uint4* dst = reinterpret_cast<uint4*>(out + (size_t)sl * 16);
+                dst[0] = o0;
+                dst[1] = o1;
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM and the box are free for the next tile
+        tc_fence_after();
+    }
+    if (s_abort) {
+        if (tid == 0) atomicOr(err, 1);
+        // bounded wait for the MMAs of the abandoned tile before freeing TMEM
+        if (pending_mma) mbar_wait(mbar_s, phase);
+        __syncthreads();
+    }
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+}
+
+template <int DIL>
+static int launch_mid_tc(const LpGrid& G, const __nv_bfloat16* wb, const __nv_bfloat16* in, __nv_bfloat16* out, int* err,
+                         int sms, cudaStream_t st) {
+    using S = TcSmem<DIL>;
+    static bool attr_set = false;  // per process; the attribute is per function
+    if (!attr_set) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(lp_mid_tc_kernel<DIL>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    FLIP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lp_mid_tc_kernel<DIL>, kTcThreads, S::kBytes));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);  // at most 4 x 128 TMEM columns per SM
+    lp_mid_tc_kernel<DIL><<<sms * per_sm, kTcThreads, S::kBytes, st>>>(G, wb, in, out, err);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+int lp_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
+                      int* err, int sms, cudaStream_t st) {
+    switch (dil) {
+    case 1: return launch_mid_tc<1>(G, wb, in, out, err, sms, st);
+    case 2: return launch_mid_tc<2>(G, wb, in, out, err, sms, st);
+    case 4: return launch_mid_tc<4>(G, wb, in, out, err, sms, st);
+    default: return FLIP_ERR_ARG;
+    }
+}
+
+}  // namespace flip

@@ -164,7 +164,9 @@ typedef struct {
     int32_t pressure_method;     /* NATIVE: 0 Jacobi-PCG, 1 learned-preconditioned FPCG */
     double max_substep_dt;       /* NATIVE: largest sub-step of solveFrame (1/240)  */
     int32_t learned_max_iter;    /* NATIVE: FPCG cap before the Jacobi-PCG restart   */
-    int32_t reserved[3];
+    int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers on CUDA
+                                    cores instead of tcgen05 (for comparison)         */
+    int32_t reserved[2];
 } flip_params;
 
 /* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */
@@ -296,7 +298,9 @@ typedef struct {
     double residual;         /* last terminating residual (relative for NATIVE)  */
     double elapsed_time;
     uint64_t n;
-    uint32_t error_flags;    /* device error word (bit 0: look-back timeout)      */
+    uint32_t error_flags;    /* device error word (bit 0: look-back timeout;
+                                bit 2: a tensor-core wait of the learned
+                                preconditioner timed out)                        */
     uint32_t launches;       /* kernels this engine launched since creation      */
 } flip_info;
 int flip_get_info(flip_engine* e, flip_info* out);

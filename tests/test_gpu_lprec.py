@@ -102,6 +102,29 @@ def test_lp_forward_loss_grad_vs_oracle(torch, shape, seed):
     P.close()
 
 
+def test_lp_tensor_cores_match_cuda_cores(torch):
+    # the tcgen05 implicit-GEMM layers against the CUDA-core kernels on the
+    # same problem and weights: both accumulate BF16 products in FP32, in
+    # different orders, so the BF16 activations differ by at most a rare
+    # rounding step
+    shape = (64, 48, 40)
+    typ = random_types(shape, 5)
+    rng = np.random.default_rng(6)
+    r = (rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    w = (rng.standard_normal(F.lib().flip_lp_num_weights()) * 0.15).astype(np.float32)
+    zs = []
+    for cc in (0, 1):
+        P = engine(shape, lp_cuda_cores=cc)
+        P.poisson_set(typ, np.zeros(typ.size, np.float32))
+        P.lp_set_weights(w)
+        z, loss = P.lp_eval(r)
+        assert P.info().error_flags == 0
+        zs.append(z)
+        P.close()
+    assert np.linalg.norm(zs[0] - zs[1]) <= 1e-3 * np.linalg.norm(zs[1])
+    assert rel_err(zs[0], zs[1]) <= 1e-2
+
+
 # ------------------------------------------------------ pressure problems
 def test_generated_problem_pcg_vs_oracle(torch):
     shape = (64, 64, 64)
