@@ -141,7 +141,7 @@ def lib():
         "flip_poisson_solve": (i32, [vp, i32, d, i32, C.POINTER(SolveInfo)]),
         "flip_poisson_read_solution": (i32, [vp, vp]),
         "flip_lp_train_step": (i32, [vp, i32, C.c_float, C.POINTER(d)]),
-        "flip_lp_eval": (i32, [vp, vp, vp, C.POINTER(d), i32]),
+        "flip_lp_eval": (i32, [vp, vp, vp, vp, C.POINTER(d), i32]),
         "flip_set_timing": (i32, [vp, i32]),
         "flip_get_stage_ms": (i32, [vp, C.POINTER(C.c_double), i32, i32]),
         "flip_last_error": (C.c_char_p, [vp]),
@@ -498,17 +498,19 @@ class Particles:
         self._call("flip_poisson_read_solution", x.ctypes.data_as(C.c_void_p))
         return x
 
-    def lp_train_step(self, pcg_iters, lr):
+    def lp_train_step(self, sample, lr):
+        """sample >= 0: Jacobi-PCG iterate error; -1: white-noise error."""
         loss = C.c_double()
-        self._call("flip_lp_train_step", pcg_iters, lr, C.byref(loss))
+        self._call("flip_lp_train_step", sample, lr, C.byref(loss))
         return loss.value
 
-    def lp_eval(self, r_lin, want_grad=False):
+    def lp_eval(self, r_lin, e_lin, want_grad=False):
         r = np.ascontiguousarray(r_lin, np.float32)
+        ev = np.ascontiguousarray(e_lin, np.float32)
         z = np.empty_like(r)
         loss = C.c_double()
-        self._call("flip_lp_eval", r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p), C.byref(loss),
-                   1 if want_grad else 0)
+        self._call("flip_lp_eval", r.ctypes.data_as(C.c_void_p), ev.ctypes.data_as(C.c_void_p),
+                   z.ctypes.data_as(C.c_void_p), C.byref(loss), 1 if want_grad else 0)
         return z, loss.value
 
     def info(self):

@@ -79,8 +79,14 @@ struct flip_engine {
     // activation buffers are per domain and allocated on first use
     LpNet lp{};
     char* lp_warena = nullptr;   // w, g, m, v, wb
-    char* lp_aarena = nullptr;   // act[3], gact, gact2, z, scalars
-    double* lp_scalar = nullptr; // [0] loss sum, [1] r.r sum
+    char* lp_aarena = nullptr;   // act[3], actz[3], gact, gact2, z, f0, xs, ev, scalars
+    float* lp_f0 = nullptr;      // f(0) of the current problem's geometry
+    double* lp_scalar = nullptr; // [0..2] m.Am, m.r, e.r; [3] r.r sum
+    float* lp_xs = nullptr;      // reference solution of the current problem (training)
+    float* lp_ev = nullptr;      // error sample e with A e = r
+    bool xstar_ready = false;    // lp_xs holds the current problem's solution
+    bool solution_fresh = false; // pcg.x + pcg.xg is a converged solution of the current problem
+    uint64_t noise_counter = 0;
     bool lp_have_weights = false;
     cudaGraphExec_t fpcg_graph = nullptr;
     int fpcg_graph_iters = 0;
@@ -139,7 +145,7 @@ extern "C" void flip_default_params(int mode, flip_params* out) {
     out->device = 0;
     out->max_substep_dt = 1.0 / 240.0;
     out->pressure_method = 0;
-    out->learned_max_iter = 1000;
+    out->learned_max_iter = 100;
 }
 
 extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, flip_engine** out) {
@@ -187,10 +193,14 @@ static void free_lp_activations(flip_engine* e) {
     if (e->lp_aarena) cudaFree(e->lp_aarena);
     e->lp_aarena = nullptr;
     for (auto& a : e->lp.act) a = nullptr;
+    for (auto& a : e->lp.actz) a = nullptr;
+    e->lp_f0 = nullptr;
     e->lp.gact = e->lp.gact2 = nullptr;
     e->pcg.z = nullptr;
     e->lp_scalar = nullptr;
     e->lp.err = nullptr;
+    e->lp_xs = e->lp_ev = nullptr;
+    e->xstar_ready = false;
 }
 static void free_arena(flip_engine* e) {
     free_lp_activations(e);
@@ -682,15 +692,21 @@ static int lp_alloc_activations(flip_engine* e) {
     if (e->P.mode != FLIP_MODE_NATIVE) return e->fail(FLIP_ERR_STATE, "learned preconditioner: native mode only");
     const size_t ab = al(e->nslots * 16 * sizeof(__nv_bfloat16)), gb = al(e->nslots * 16 * sizeof(float)),
                  zb = al(e->nslots * sizeof(float));
-    const size_t total = 3 * ab + 2 * gb + zb + 256;
+    const size_t total = 6 * ab + 2 * gb + 4 * zb + 256;
     E_CUDA(cudaMalloc((void**)&e->lp_aarena, total));
     E_CUDA(cudaMemsetAsync(e->lp_aarena, 0, total, e->stream));
-    for (int l = 0; l < 3; ++l) e->lp.act[l] = (__nv_bfloat16*)(e->lp_aarena + l * ab);
-    e->lp.gact = (float*)(e->lp_aarena + 3 * ab);
-    e->lp.gact2 = (float*)(e->lp_aarena + 3 * ab + gb);
-    e->pcg.z = (float*)(e->lp_aarena + 3 * ab + 2 * gb);
-    e->lp_scalar = (double*)(e->lp_aarena + 3 * ab + 2 * gb + zb);
-    e->lp.err = (int*)(e->lp_aarena + 3 * ab + 2 * gb + zb + 16);
+    char* q = e->lp_aarena;
+    for (int l = 0; l < 3; ++l, q += ab) e->lp.act[l] = (__nv_bfloat16*)q;
+    for (int l = 0; l < 3; ++l, q += ab) e->lp.actz[l] = (__nv_bfloat16*)q;
+    e->lp.gact = (float*)q; q += gb;
+    e->lp.gact2 = (float*)q; q += gb;
+    e->pcg.z = (float*)q; q += zb;
+    e->lp_f0 = (float*)q; q += zb;
+    e->lp_xs = (float*)q; q += zb;
+    e->lp_ev = (float*)q; q += zb;
+    e->lp_scalar = (double*)q;
+    e->lp.err = (int*)(q + 64);
+    e->xstar_ready = false;
     return FLIP_OK;
 }
 // the network's view of the current problem: activations on the dilated
@@ -705,6 +721,7 @@ static LpGrid lp_grid(flip_engine* e, const int* halt) {
     G.out_tiles = e->node_keys;
     G.d_nout = e->d_counts;
     G.halt = halt;
+    G.cell = e->pcg.cell;
     G.D = e->D;
     return G;
 }
@@ -744,7 +761,7 @@ static int nat_fpcg_graph(flip_engine* e, int iters) {
     for (int k = 0; k < iters && rc == FLIP_OK; ++k) {
         rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
         if (rc == FLIP_OK && k == iters - 1) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-        if (rc == FLIP_OK) rc = lp_forward_dev(e->lp, G, inv_s, e->pcg.z, nat_grid(e, 2), e->stream);
+        if (rc == FLIP_OK) rc = lp_forward_dev(e->lp, G, inv_s, e->lp_f0, e->pcg.z, nat_grid(e, 2), e->stream);
         if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream);
     }
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
@@ -789,9 +806,10 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
         E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
         const LpGrid G = lp_grid(e, &e->pcg.st->halt);
-        E_TRY(lp_forward_dev(e->lp, G, &e->pcg.st->inv_s, e->pcg.z, nat_grid(e, 2), e->stream));
+        E_TRY(lp_bias_dev(e->lp, G, &e->pcg.st->inv_s, e->lp_f0, nat_grid(e, 2), e->stream));
+        E_TRY(lp_forward_dev(e->lp, G, &e->pcg.st->inv_s, e->lp_f0, e->pcg.z, nat_grid(e, 2), e->stream));
         E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream));
-        e->launches += 6;
+        e->launches += 10;
         E_TRY(e->mark(9));
         E_TRY(nat_fpcg_graph(e, chunk));
         E_TRY(run_chunks(e, e->fpcg_graph, chunk, 7u * (uint32_t)chunk + 1u, max_learned));
@@ -829,6 +847,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
     }
     e->last_iters = info.iters + info.plain_iters;
     e->last_converged = info.converged;
+    e->solution_fresh = info.converged != 0;
     e->last_rel = info.rel_residual;
     e->last_solve = info;
     if (out) *out = info;
@@ -840,6 +859,7 @@ static int nat_pressure(flip_engine* e) {
     E_TRY(nat_solve(e, (const float* const*)e->m, e->P.pressure_method, e->P.pcg_tol, e->P.pcg_max_iter, learned,
                     e->timing ? &e->last_solve : nullptr));
     e->poisson_ready = true;  // b, the cell types and the tile lists of this solve stay in place
+    e->xstar_ready = false;
     return FLIP_OK;
 }
 
@@ -1209,6 +1229,8 @@ static int poisson_tiles(flip_engine* e) {
     e->launches += 6;
     e->poisson_ready = true;
     e->have_voxels = false;
+    e->xstar_ready = false;
+    e->solution_fresh = false;
     return FLIP_OK;
 }
 
@@ -1293,66 +1315,105 @@ extern "C" int flip_poisson_read_solution(flip_engine* e, double* x_lin) {
     return rc;
 }
 
-// read back the loss sum and the state; loss = sum / n_fluid
+// loss = (m.Am - 2 m.r) / e.r + 1 from the device sums
 static int lp_read_loss(flip_engine* e, double* loss) {
-    double l2 = 0.0;
-    E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
-    E_CUDA(cudaMemcpyAsync(e->h_small, e->lp_scalar, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    double sums[3] = {0.0, 0.0, 0.0};
+    E_CUDA(cudaMemcpyAsync(e->h_small, e->lp_scalar, sizeof(sums), cudaMemcpyDeviceToHost, e->stream));
     E_CUDA(cudaStreamSynchronize(e->stream));
-    memcpy(&l2, e->h_small, sizeof(double));
-    if (loss) *loss = l2 / std::max(e->h_state->nfluid, 1.0);
+    memcpy(sums, e->h_small, sizeof(sums));
+    if (loss) *loss = sums[2] > 0.0 ? (sums[0] - 2.0 * sums[1]) / sums[2] + 1.0 : 0.0;
     return FLIP_OK;
 }
 
-extern "C" int flip_lp_train_step(flip_engine* e, int pcg_iters, float lr, double* loss) {
-    CHECK_NATIVE("flip_lp_train_step");
-    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_train_step: no problem (flip_poisson_generate/set)");
-    if (pcg_iters < 0 || pcg_iters > 100000 || !(lr >= 0.0f)) return e->fail(FLIP_ERR_ARG, "flip_lp_train_step: bad arguments");
-    E_TRY(lp_ready(e));
-    // the sample: the residual after pcg_iters Jacobi-PCG iterations from x = 0
-    pcg_state_host(e, 0.0, pcg_iters + 1, 0);
-    e->h_state->true_every = 0;
-    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
-    const float* const nullU[3] = {nullptr, nullptr, nullptr};
-    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));
-    for (int k = 0; k < pcg_iters; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+// the reference solution x* of the current problem, for error samples
+static int lp_reference_solution(flip_engine* e) {
+    if (e->xstar_ready) return FLIP_OK;
+    if (!e->solution_fresh) {
+        flip_solve_info info{};
+        E_TRY(nat_solve(e, nullptr, 0, e->P.pcg_tol, e->P.pcg_max_iter, e->P.pcg_max_iter, &info));
+        if (!info.converged) return e->fail(FLIP_ERR_NOT_CONVERGED, "flip_lp_train_step: the reference solve did not converge");
+    }
     const LpGrid G = lp_grid(e, nullptr);
-    const float* inv_s = &e->pcg.st->inv_s;
-    const int grid = nat_grid(e, 2);
-    E_TRY(lp_forward_dev(e->lp, G, inv_s, e->pcg.z, grid, e->stream));
-    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, sizeof(double), e->stream));
-    E_TRY(lp_loss_grad(G, inv_s, e->pcg.z, e->pcg.q, e->pcg.p1, e->lp_scalar, &e->pcg.st->nfluid, grid, e->stream));
-    E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
-    E_TRY(lp_backward_dev(e->lp, G, inv_s, e->pcg.p1, grid, e->stream));
-    E_TRY(lp_adam(e->lp, lr, e->stream));
-    e->launches += 1 + 2 * (uint32_t)pcg_iters + 4 + 2 + 7 + 1;
-    return lp_read_loss(e, loss);
+    E_TRY(lp_store_solution(G, e->pcg.x, e->pcg.xg, e->lp_xs, nat_grid(e, 2), e->stream));
+    e->launches += 1;
+    e->xstar_ready = true;
+    return FLIP_OK;
 }
 
-extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, float* z_lin, double* loss, int want_grad) {
+// loss, gradient and Adam for the sample in pcg.r / lp_ev (inv_s set)
+static int lp_loss_backward(flip_engine* e, const float* inv_s, bool want_grad, float lr, bool step) {
+    const LpGrid G = lp_grid(e, nullptr);
+    const int grid = nat_grid(e, 2);
+    E_TRY(lp_bias_dev(e->lp, G, inv_s, e->lp_f0, grid, e->stream));
+    E_TRY(lp_forward_dev(e->lp, G, inv_s, e->lp_f0, e->pcg.z, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, 3 * sizeof(double), e->stream));
+    E_TRY(lp_loss_grad(G, e->pcg.z, e->lp_ev, e->pcg.q, e->pcg.p1, e->lp_scalar, grid, e->stream));
+    e->launches += 8 + 2;
+    if (want_grad) {
+        E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
+        E_TRY(lp_backward_dev(e->lp, G, inv_s, e->pcg.p1, grid, e->stream));
+        e->launches += 14;
+    }
+    if (step) {
+        E_TRY(lp_adam(e->lp, lr, e->stream));
+        e->launches += 1;
+    }
+    return FLIP_OK;
+}
+
+extern "C" int flip_lp_train_step(flip_engine* e, int sample, float lr, double* loss) {
+    CHECK_NATIVE("flip_lp_train_step");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_train_step: no problem (flip_poisson_generate/set or a step)");
+    if (sample < -1 || sample > 100000 || !(lr >= 0.0f)) return e->fail(FLIP_ERR_ARG, "flip_lp_train_step: bad arguments");
+    E_TRY(lp_ready(e));
+    E_TRY(lp_reference_solution(e));
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    const LpGrid G = lp_grid(e, nullptr);
+    const int grid = nat_grid(e, 2);
+    // pcg_init sets the cell codes, n_fluid, r = b and inv_s = 1/rms(b)
+    pcg_state_host(e, 0.0, sample + 1, 0);
+    e->h_state->true_every = 0;
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));
+    e->launches += 1;
+    float* inv_s = &e->pcg.st->inv_s;
+    if (sample >= 0) {
+        // the residual of x_k after k Jacobi-PCG iterations from 0, and e = x* - x_k
+        for (int k = 0; k < sample; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_TRY(lp_error_from_solution(G, e->pcg.x, e->pcg.xg, e->lp_xs, e->lp_ev, grid, e->stream));
+        e->launches += 2 * (uint32_t)sample + 1;
+    } else {
+        // white noise e on the fluid cells and r = A e
+        E_TRY(lp_noise_sample(G, 0x5DEECE66Dull + e->noise_counter++, e->lp_ev, e->pcg.r, grid, e->stream));
+        E_TRY(lp_input_scale(G, e->lp_scalar + 3, &e->pcg.st->nfluid, inv_s, grid, e->stream));
+        e->launches += 4;
+    }
+    e->solution_fresh = false;  // pcg.x now holds x_k
+    E_TRY(lp_loss_backward(e, inv_s, true, lr, true));
+    E_TRY(lp_read_loss(e, loss));
+    return lp_check_err(e);
+}
+
+extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, const float* e_lin, float* z_lin, double* loss,
+                            int want_grad) {
     CHECK_NATIVE("flip_lp_eval");
-    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_eval: no problem (flip_poisson_generate/set)");
-    if (!r_lin) return e->fail(FLIP_ERR_ARG, "flip_lp_eval: null residual");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_lp_eval: no problem (flip_poisson_generate/set or a step)");
+    if (!r_lin || !e_lin) return e->fail(FLIP_ERR_ARG, "flip_lp_eval: null residual or error");
     E_TRY(lp_ready(e));
     pcg_state_host(e, 0.0, 0, 0);
     E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
     E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));  // cell codes, n_fluid
+    e->solution_fresh = false;
     E_CUDA(cudaMemcpyAsync(e->pcg.p0, r_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
     E_TRY(nat_launch_lin_tiles_f32(e->pcg.p0, e->pcg.r, e->D, 1, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->pcg.p0, e_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_lin_tiles_f32(e->pcg.p0, e->lp_ev, e->D, 1, e->stream));
     const LpGrid G = lp_grid(e, nullptr);
     float* inv_s = &e->pcg.st->inv_s;
-    const int grid = nat_grid(e, 2);
-    E_TRY(lp_input_scale(G, e->lp_scalar + 1, &e->pcg.st->nfluid, inv_s, grid, e->stream));
-    E_TRY(lp_forward_dev(e->lp, G, inv_s, e->pcg.z, grid, e->stream));
-    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, sizeof(double), e->stream));
-    E_TRY(lp_loss_grad(G, inv_s, e->pcg.z, e->pcg.q, e->pcg.p1, e->lp_scalar, &e->pcg.st->nfluid, grid, e->stream));
-    e->launches += 1 + 1 + 2 + 4 + 2;
-    if (want_grad) {
-        E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
-        E_TRY(lp_backward_dev(e->lp, G, inv_s, e->pcg.p1, grid, e->stream));
-        e->launches += 7;
-    }
+    E_TRY(lp_input_scale(G, e->lp_scalar + 3, &e->pcg.st->nfluid, inv_s, nat_grid(e, 2), e->stream));
+    e->launches += 1 + 2 + 2;
+    E_TRY(lp_loss_backward(e, inv_s, want_grad != 0, 0.0f, false));
     if (z_lin) {
         E_TRY(nat_launch_lin_tiles_f32(e->pcg.z, e->pcg.p0, e->D, 0, e->stream));
         E_CUDA(cudaMemcpyAsync(z_lin, e->pcg.p0, 4 * e->nslots, cudaMemcpyDeviceToHost, e->stream));

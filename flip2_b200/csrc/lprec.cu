@@ -36,7 +36,7 @@ __device__ __forceinline__ void tile_origin(uint32_t key, const NatDims& D, int&
 __device__ __forceinline__ void input_channels(const LpGrid& G, uint32_t u, float inv_s, float (&in)[3]) {
     const uint8_t t = G.type[u];
     const bool fl = t == kFluid;
-    in[0] = fl ? G.r[u] * inv_s : 0.0f;
+    in[0] = (fl && G.r) ? G.r[u] * inv_s : 0.0f;
     in[1] = fl ? 1.0f : 0.0f;
     in[2] = (t == kSolid) ? 1.0f : 0.0f;
 }
@@ -139,10 +139,11 @@ __global__ void __launch_bounds__(512) lp_mid_kernel(LpGrid G, const __nv_bfloat
     }
 }
 
-// layer 3: 16 -> 1, scaled back by s and masked to fluid cells
+// layer 3: 16 -> 1 on fluid cells.  raw: z = f (the zero-residual pass);
+// else z = s (f - f0[v]) with f0 optional
 __global__ void __launch_bounds__(512) lp_out_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
                                                      const __nv_bfloat16* __restrict__ in, const float* __restrict__ d_inv_s,
-                                                     float* __restrict__ z) {
+                                                     const float* __restrict__ f0, int raw, float* __restrict__ z) {
     if (G.halt && *G.halt) return;
     __shared__ float W[27 * 16];
     for (int i = threadIdx.x; i < 27 * 16; i += 512) W[i] = __bfloat162float(wb[i]);
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(512) lp_out_kernel(LpGrid G, const __nv_bfloat
 #pragma unroll
                 for (int ci = 0; ci < 16; ++ci) acc = fmaf(W[tap * 16 + ci], x[ci], acc);
             }
-            acc *= s;
+            if (!raw) acc = (acc - (f0 ? f0[v] : 0.0f)) * s;
         }
         z[v] = acc;
     }
@@ -179,11 +180,12 @@ __global__ void __launch_bounds__(512) lp_out_kernel(LpGrid G, const __nv_bfloat
 // sum_tap W3[tap][ci] * s * gz(u - dil*off); gz is zero off fluid cells
 __global__ void __launch_bounds__(512) lp_out_dgrad_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
                                                            const float* __restrict__ gz, const __nv_bfloat16* __restrict__ a2,
-                                                           const float* __restrict__ d_inv_s, float* __restrict__ g2) {
+                                                           const float* __restrict__ d_inv_s, float sign,
+                                                           float* __restrict__ g2) {
     __shared__ float W[27 * 16];
     for (int i = threadIdx.x; i < 27 * 16; i += 512) W[i] = __bfloat162float(wb[i]);
     __syncthreads();
-    const float s = 1.0f / *d_inv_s;
+    const float s = sign / *d_inv_s;
     const uint32_t n = *G.d_nact;
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
     for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
@@ -267,15 +269,15 @@ __global__ void __launch_bounds__(512) lp_mid_dgrad_kernel(LpGrid G, const __nv_
 template <int MODE, int CIN, int COUT>
 __global__ void __launch_bounds__(512) lp_wgrad_kernel(LpGrid G, int dil, const float* __restrict__ gout,
                                                        const __nv_bfloat16* __restrict__ ain, const float* __restrict__ d_inv_s,
-                                                       const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_n,
-                                                       float* __restrict__ dw) {
+                                                       float sign, const uint32_t* __restrict__ tiles,
+                                                       const uint32_t* __restrict__ d_n, float* __restrict__ dw) {
     constexpr int P = CIN * COUT;
     constexpr int S = 512 / P;  // voxel subsets per CTA
     const int pair = threadIdx.x % P, sub = threadIdx.x / P;
     if (sub >= S) return;
     const int ci = pair / COUT, co = pair % COUT;
     const float inv_s = *d_inv_s;
-    const float gscale = (MODE == 2) ? 1.0f / inv_s : 1.0f;
+    const float gscale = (MODE == 2) ? sign / inv_s : 1.0f;
     float acc[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q) acc[q] = 0.0f;
@@ -333,101 +335,217 @@ __global__ void lp_to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __
 }
 
 // ------------------------------------------------------------ launchers
-int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* z, int grid, cudaStream_t st) {
-    lp_in_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, net.act[0]);
+// the three hidden layers into acts[0..2]
+static int lp_hidden(const LpNet& net, const LpGrid& G, const float* d_inv_s, __nv_bfloat16* const* acts, int grid,
+                     cudaStream_t st) {
+    lp_in_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, acts[0]);
     if (net.tensor_cores) {
-        int rc = lp_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], net.act[0], net.act[1], net.err, net.sms, st);
-        if (rc == FLIP_OK) rc = lp_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], net.act[1], net.act[2], net.err, net.sms, st);
+        int rc = lp_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1], net.err, net.sms, st);
+        if (rc == FLIP_OK) rc = lp_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2], net.err, net.sms, st);
         if (rc != FLIP_OK) return rc;
     } else {
-        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.act[0], net.act[1]);
-        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.act[1], net.act[2]);
+        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1]);
+        lp_mid_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2]);
     }
-    lp_out_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], net.act[2], d_inv_s, z);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
-int lp_backward_dev(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz, int grid, cudaStream_t st) {
+int lp_bias_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* f0, int grid, cudaStream_t st) {
+    LpGrid G0 = G;
+    G0.r = nullptr;
+    int rc = lp_hidden(net, G0, d_inv_s, net.actz, grid, st);
+    if (rc != FLIP_OK) return rc;
+    lp_out_kernel<<<grid, 512, 0, st>>>(G0, net.wb + kLpWOff[3], net.dil[3], net.actz[2], d_inv_s, nullptr, 1, f0);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, const float* f0, float* z, int grid,
+                   cudaStream_t st) {
+    int rc = lp_hidden(net, G, d_inv_s, net.act, grid, st);
+    if (rc != FLIP_OK) return rc;
+    lp_out_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], net.act[2], d_inv_s, f0, 0, z);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+// one backward pass through the activations acts, dL/d(output) = sign * s * gz
+static int lp_backward_path(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz,
+                            __nv_bfloat16* const* acts, float sign, int grid, cudaStream_t st) {
     // layer 3 (16 -> 1)
-    lp_wgrad_kernel<2, 16, 1><<<grid, 512, 0, st>>>(G, net.dil[3], gz, net.act[2], d_inv_s, G.out_tiles, G.d_nout,
+    lp_wgrad_kernel<2, 16, 1><<<grid, 512, 0, st>>>(G, net.dil[3], gz, acts[2], d_inv_s, sign, G.out_tiles, G.d_nout,
                                                     net.g + kLpWOff[3]);
-    lp_out_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], gz, net.act[2], d_inv_s, net.gact);
+    lp_out_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], gz, acts[2], d_inv_s, sign, net.gact);
     // layer 2 (16 -> 16): Gout = gact (wrt act[2]), input act[1]
-    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[2], net.gact, net.act[1], d_inv_s, G.act_tiles, G.d_nact,
+    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[2], net.gact, acts[1], d_inv_s, 1.0f, G.act_tiles, G.d_nact,
                                                      net.g + kLpWOff[2]);
-    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.gact, net.act[1], net.gact2);
+    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.gact, acts[1], net.gact2);
     // layer 1: Gout = gact2 (wrt act[1]), input act[0]
-    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[1], net.gact2, net.act[0], d_inv_s, G.act_tiles, G.d_nact,
+    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[1], net.gact2, acts[0], d_inv_s, 1.0f, G.act_tiles, G.d_nact,
                                                      net.g + kLpWOff[1]);
-    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.gact2, net.act[0], net.gact);
+    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.gact2, acts[0], net.gact);
     // layer 0: Gout = gact (wrt act[0]), input = the three channels
-    lp_wgrad_kernel<0, 3, 16><<<grid, 512, 0, st>>>(G, net.dil[0], net.gact, nullptr, d_inv_s, G.act_tiles, G.d_nact,
+    lp_wgrad_kernel<0, 3, 16><<<grid, 512, 0, st>>>(G, net.dil[0], net.gact, nullptr, d_inv_s, 1.0f, G.act_tiles, G.d_nact,
                                                     net.g + kLpWOff[0]);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
-// 7-point operator on fluid cells from the cell types (the PCG matrix)
-__device__ __forceinline__ float lp_apply_A(const float* __restrict__ x, const LpGrid& G, int i, int j, int k, uint32_t v) {
-    const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-    float d = 0.0f, sum = 0.0f;
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        const int a = i + oi[m], b = j + oj[m], c = k + ok[m];
-        if (a < 0 || b < 0 || c < 0 || a >= G.D.nx || b >= G.D.ny || c >= G.D.nz) continue;
-        const uint32_t u = lslot(a, b, c, G.D);
-        const uint8_t t = G.type[u];
-        if (t == kSolid) continue;
-        d += 1.0f;
-        if (t == kFluid) sum += x[u];
-    }
-    return fmaf(d, x[v], -sum);
+int lp_backward_dev(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz, int grid, cudaStream_t st) {
+    int rc = lp_backward_path(net, G, d_inv_s, gz, net.act, 1.0f, grid, st);
+    if (rc != FLIP_OK) return rc;
+    LpGrid G0 = G;
+    G0.r = nullptr;  // the zero-residual pass enters with a minus sign
+    return lp_backward_path(net, G0, d_inv_s, gz, net.actz, -1.0f, grid, st);
 }
 
-__global__ void __launch_bounds__(512) lp_loss_res_kernel(LpGrid G, const float* __restrict__ d_inv_s,
-                                                          const float* __restrict__ z, float* __restrict__ e,
-                                                          double* __restrict__ d_loss2) {
+// m = N(r) + D^-1 r at a fluid cell from its slot
+__device__ __forceinline__ float lp_m(const float* __restrict__ z, const LpGrid& G, uint32_t u, uint8_t c) {
+    const float d = (float)(c & 7u);
+    return d > 0.0f ? z[u] + G.r[u] / d : z[u];
+}
+
+// A m - r on fluid cells; sums m.Am, m.r, e.r
+__global__ void __launch_bounds__(512) lp_anorm_kernel(LpGrid G, const float* __restrict__ z, const float* __restrict__ ev,
+                                                       float* __restrict__ wbuf, double* __restrict__ sums) {
     __shared__ double sh[32];
-    const float inv_s = *d_inv_s;
-    const uint32_t n = *G.d_nact;
+    const uint32_t n = *G.d_nout;
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
-    double acc = 0.0;
+    double mam = 0.0, mr = 0.0, er = 0.0;
     for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
-        const uint32_t key = G.act_tiles[t];
+        const uint32_t key = G.out_tiles[t];
         int ox, oy, oz;
         tile_origin(key, G.D, ox, oy, oz);
         const uint32_t v = (key << 9) | threadIdx.x;
-        float ev = 0.0f;
-        if (G.type[v] == kFluid) {
-            ev = (lp_apply_A(z, G, ox + li, oy + lj, oz + lk, v) - G.r[v]) * inv_s;
-            acc += (double)ev * (double)ev;
+        const uint8_t c = G.cell[v];
+        float wv = 0.0f;
+        if (c & 0x80u) {
+            const int i = ox + li, j = oy + lj, k = oz + lk;
+            const float m = lp_m(z, G, v, c);
+            const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+            float sum = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const int a = i + oi[q], b = j + oj[q], cc = k + ok[q];
+                if (a < 0 || b < 0 || cc < 0 || a >= G.D.nx || b >= G.D.ny || cc >= G.D.nz) continue;
+                const uint32_t u = lslot(a, b, cc, G.D);
+                const uint8_t cu = G.cell[u];
+                if (cu & 0x80u) sum += lp_m(z, G, u, cu);
+            }
+            const float am = fmaf((float)(c & 7u), m, -sum);
+            const float rv = G.r[v];
+            wv = am - rv;
+            mam += (double)m * (double)am;
+            mr += (double)m * (double)rv;
+            er += (double)ev[v] * (double)rv;
         }
-        e[v] = ev;
+        wbuf[v] = wv;
     }
-    double r = block_sum_f64<512>(acc, sh);
-    if (threadIdx.x == 0 && r != 0.0) atomicAdd(d_loss2, r);
+    const double a = block_sum_f64<512>(mam, sh);
+    const double b = block_sum_f64<512>(mr, sh);
+    const double e = block_sum_f64<512>(er, sh);
+    if (threadIdx.x == 0) {
+        if (a != 0.0) atomicAdd(sums, a);
+        if (b != 0.0) atomicAdd(sums + 1, b);
+        if (e != 0.0) atomicAdd(sums + 2, e);
+    }
 }
 
-__global__ void __launch_bounds__(512) lp_loss_gz_kernel(LpGrid G, const float* __restrict__ e,
-                                                         const double* __restrict__ d_nfluid,
-                                                         const float* __restrict__ d_inv_s, float* __restrict__ gz) {
-    const float scale = (float)(2.0 / fmax(*d_nfluid, 1.0)) * *d_inv_s;
+__global__ void __launch_bounds__(512) lp_anorm_gz_kernel(LpGrid G, const float* __restrict__ wbuf,
+                                                          const double* __restrict__ sums, float* __restrict__ gz) {
+    const double er = sums[2];
+    const float scale = er > 0.0 ? (float)(2.0 / er) : 0.0f;
     const uint32_t n = *G.d_nact;
+    for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+        const uint32_t v = (G.act_tiles[t] << 9) | threadIdx.x;
+        gz[v] = (G.cell[v] & 0x80u) ? scale * wbuf[v] : 0.0f;
+    }
+}
+
+int lp_loss_grad(const LpGrid& G, const float* z, const float* ev, float* wbuf, float* gz, double* d_sums, int grid,
+                 cudaStream_t st) {
+    lp_anorm_kernel<<<grid, 512, 0, st>>>(G, z, ev, wbuf, d_sums);
+    lp_anorm_gz_kernel<<<grid, 512, 0, st>>>(G, wbuf, d_sums, gz);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+// counter-based normal numbers: splitmix64 of (seed, slot), Box-Muller
+__device__ __forceinline__ uint64_t lp_mix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__global__ void __launch_bounds__(512) lp_noise_kernel(LpGrid G, uint64_t seed, float* __restrict__ ev) {
+    const uint32_t n = *G.d_nout;
+    for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+        const uint32_t v = (G.out_tiles[t] << 9) | threadIdx.x;
+        float e = 0.0f;
+        if (G.cell[v] & 0x80u) {
+            const uint64_t h = lp_mix(seed * 0x100000001B3ull + v);
+            const float u1 = ((float)(h >> 40) + 0.5f) * (1.0f / 16777216.0f);
+            const float u2 = (float)((h >> 16) & 0xFFFFFFull) * (1.0f / 16777216.0f);
+            e = sqrtf(-2.0f * logf(u1)) * cosf(6.283185307f * u2);
+        }
+        ev[v] = e;
+    }
+}
+__global__ void __launch_bounds__(512) lp_apply_A_kernel(LpGrid G, const float* __restrict__ x, float* __restrict__ y) {
+    const uint32_t n = *G.d_nout;
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
     for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
-        const uint32_t key = G.act_tiles[t];
+        const uint32_t key = G.out_tiles[t];
         int ox, oy, oz;
         tile_origin(key, G.D, ox, oy, oz);
         const uint32_t v = (key << 9) | threadIdx.x;
-        gz[v] = (G.type[v] == kFluid) ? scale * lp_apply_A(e, G, ox + li, oy + lj, oz + lk, v) : 0.0f;
+        const uint8_t c = G.cell[v];
+        float out = 0.0f;
+        if (c & 0x80u) {
+            const int i = ox + li, j = oy + lj, k = oz + lk;
+            const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
+            float sum = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const int a = i + oi[q], b = j + oj[q], cc = k + ok[q];
+                if (a < 0 || b < 0 || cc < 0 || a >= G.D.nx || b >= G.D.ny || cc >= G.D.nz) continue;
+                const uint32_t u = lslot(a, b, cc, G.D);
+                if (G.cell[u] & 0x80u) sum += x[u];
+            }
+            out = fmaf((float)(c & 7u), x[v], -sum);
+        }
+        y[v] = out;
     }
 }
+int lp_noise_sample(const LpGrid& G, uint64_t seed, float* ev, float* r, int grid, cudaStream_t st) {
+    lp_noise_kernel<<<grid, 512, 0, st>>>(G, seed, ev);
+    lp_apply_A_kernel<<<grid, 512, 0, st>>>(G, ev, r);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 
-int lp_loss_grad(const LpGrid& G, const float* d_inv_s, const float* z, float* e, float* gz, double* d_loss2,
-                 const double* d_nfluid, int grid, cudaStream_t st) {
-    lp_loss_res_kernel<<<grid, 512, 0, st>>>(G, d_inv_s, z, e, d_loss2);
-    lp_loss_gz_kernel<<<grid, 512, 0, st>>>(G, e, d_nfluid, d_inv_s, gz);
+__global__ void __launch_bounds__(512) lp_solution_kernel(LpGrid G, const double* __restrict__ x, const float* __restrict__ xg,
+                                                          const float* __restrict__ xs, float* __restrict__ out) {
+    const uint32_t n = *G.d_nout;
+    for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+        const uint32_t v = (G.out_tiles[t] << 9) | threadIdx.x;
+        float o = 0.0f;
+        if (G.cell[v] & 0x80u) {
+            const double xv = x[v] + (double)xg[v];
+            o = xs ? (float)((double)xs[v] - xv) : (float)xv;
+        }
+        out[v] = o;
+    }
+}
+int lp_store_solution(const LpGrid& G, const double* x, const float* xg, float* xs, int grid, cudaStream_t st) {
+    lp_solution_kernel<<<grid, 512, 0, st>>>(G, x, xg, nullptr, xs);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int lp_error_from_solution(const LpGrid& G, const double* x, const float* xg, const float* xs, float* ev, int grid,
+                           cudaStream_t st) {
+    lp_solution_kernel<<<grid, 512, 0, st>>>(G, x, xg, xs, ev);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

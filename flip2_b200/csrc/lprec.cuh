@@ -28,6 +28,7 @@ struct LpNet {
     float* v;             // Adam second moment
     __nv_bfloat16* wb;    // BF16 copy used by the kernels
     __nv_bfloat16* act[3];  // activations after layers 0..2: [slot][16]
+    __nv_bfloat16* actz[3]; // the same for the zero-residual pass f(0)
     float* gact;          // gradient of one activation layer: [slot][16]
     float* gact2;         // second gradient buffer: [slot][16]
     int adam_t;
@@ -49,6 +50,7 @@ struct LpGrid {
     const uint32_t* out_tiles;   // tiles with fluid cells (outputs)
     const uint32_t* d_nout;
     const int* halt;             // optional: nonzero stops the kernels (a converged FPCG)
+    const uint8_t* cell;         // PCG cell codes: fluid bit, Jacobi diagonal in bits 0-2
     NatDims D;
 };
 
@@ -56,17 +58,34 @@ struct LpGrid {
 // active tiles (lprec_tc.cu); dil in {1, 2, 4}
 int lp_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
                       int* err, int sms, cudaStream_t st);
-// z = s * N([r/s, fluid, solid]) on fluid cells, 0 elsewhere; s = 1/(*d_inv_s)
-int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* z, int grid, cudaStream_t st);
+// The network: N(r) = s (f(r/s) - f(0)) on fluid cells, 0 elsewhere, with
+// f = the convolutions on the channels [r/s, fluid, solid], s = 1/(*d_inv_s)
+// = rms(r) over the fluid cells.  f(0) depends on the geometry only; without
+// it the network can answer every residual with the same geometry-shaped
+// field (the hydrostatic part of the training solutions), which gives
+// flexible CG nothing new after its first step.
+// f0 = f(0) (once per problem; uses the actz buffers)
+int lp_bias_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* f0, int grid, cudaStream_t st);
+// z = N(r) given f0
+int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, const float* f0, float* z, int grid,
+                   cudaStream_t st);
 // gradient of the loss with respect to the weights given dL/dz (gz, FP32 on
-// the slots of the active tiles, zero off fluid cells); accumulates into
-// net.g (caller zeroes it)
+// the slots of the active tiles, zero off fluid cells), through both the
+// f(r/s) and the f(0) activations; accumulates into net.g (caller zeroes it)
 int lp_backward_dev(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz, int grid, cudaStream_t st);
-// training loss L = |A z - r|^2 / |r|^2 over the fluid cells, with
-// |r|^2 = s^2 n_fluid: e = (A z - r)/s, *d_loss2 += |e|^2 (caller zeroes it),
-// gz = dL/dz = 2 A e / (s n_fluid) (A is symmetric on the fluid cells)
-int lp_loss_grad(const LpGrid& G, const float* d_inv_s, const float* z, float* e, float* gz, double* d_loss2,
-                 const double* d_nfluid, int grid, cudaStream_t st);
+// training loss of the preconditioner M(r) = N(r) + D^-1 r for a sample
+// (r, e) with A e = r: L = |M(r) - e|_A^2 / |e|_A^2 = (m.Am - 2 m.r)/e.r + 1.
+// Accumulates m.Am, m.r, e.r into d_sums[0..2] (caller zeroes them), keeps
+// A m - r in wbuf and writes gz = dL/dN = 2 (A m - r) / e.r on the fluid
+// cells of the active tiles (0 elsewhere)
+int lp_loss_grad(const LpGrid& G, const float* z, const float* ev, float* wbuf, float* gz, double* d_sums, int grid,
+                 cudaStream_t st);
+// white-noise error sample: e ~ N(0,1) on fluid cells (hash of seed and slot), r = A e
+int lp_noise_sample(const LpGrid& G, uint64_t seed, float* ev, float* r, int grid, cudaStream_t st);
+// xs = x + xg (the reference solution) and e = xs - (x + xg) on the fluid cells
+int lp_store_solution(const LpGrid& G, const double* x, const float* xg, float* xs, int grid, cudaStream_t st);
+int lp_error_from_solution(const LpGrid& G, const double* x, const float* xg, const float* xs, float* ev, int grid,
+                           cudaStream_t st);
 // *d_inv_s = 1 / rms(r) over the fluid cells of the output tiles
 int lp_input_scale(const LpGrid& G, double* d_acc, const double* d_nfluid, float* d_inv_s, int grid, cudaStream_t st);
 // Adam step on the FP32 master weights, then the BF16 copy

@@ -726,16 +726,17 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
     }
 }
 
-// flexible CG (Notay's FCG(1), the same recurrence as Polak-Ribiere PCG):
-// after z = N(r), the new direction p' = z + beta p is A-orthogonal to p for
-// beta = -z.q / p.q (q = A p), and alpha = r.z / p'.q' is the exact line
-// search along p' (r is orthogonal to p).  A nonlinear N may give r.z < 0;
+// flexible CG (Notay's FCG(1), the same recurrence as Polak-Ribiere PCG)
+// with the preconditioner M(r) = N(r) + D^-1 r.  This kernel adds the Jacobi
+// term to the network output z in place.  The new direction p' = z + beta p
+// is A-orthogonal to p for beta = -z.q / p.q (q = A p), and alpha = r.z /
+// p'.q' is the exact line search along p' (r is orthogonal to p).  A nonlinear N may give r.z < 0;
 // alpha is then negative and the step still minimises the A-norm error along
 // p', so only r.z = 0 (no progress possible) or a non-finite value ends the
 // solve.  init: beta = 0.
 __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __restrict__ tiles,
                                                            const uint32_t* __restrict__ d_ntiles, const float* __restrict__ r,
-                                                           const float* __restrict__ z, const float* __restrict__ q,
+                                                           float* __restrict__ z, const float* __restrict__ q,
                                                            const uint8_t* __restrict__ cell, int init, PcgState* st,
                                                            double* partials) {
     if (st->halt) return;
@@ -747,17 +748,21 @@ __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __rest
         const uint32_t c4 = *reinterpret_cast<const uint32_t*>(cell + s);
         if (!c4) continue;
         const float4 r4 = *reinterpret_cast<const float4*>(r + s);
-        const float4 z4 = *reinterpret_cast<const float4*>(z + s);
+        float4 z4 = *reinterpret_cast<const float4*>(z + s);
         const float4 q4 = *reinterpret_cast<const float4*>(q + s);
         const float* rv = &r4.x;
-        const float* zv = &z4.x;
+        float* zv = &z4.x;
         const float* qv = &q4.x;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            if (!((c4 >> (8 * m)) & kCellFluid)) continue;
+            const uint8_t c = (uint8_t)(c4 >> (8 * m));
+            if (!(c & kCellFluid)) continue;
+            const float d = (float)(c & 7u);
+            zv[m] = d > 0.0f ? zv[m] + rv[m] / d : zv[m];  // M(r) = N(r) + D^-1 r
             rz += (double)rv[m] * (double)zv[m];
             zq += (double)zv[m] * (double)qv[m];
         }
+        *reinterpret_cast<float4*>(z + s) = z4;
     }
     double vals[2] = {rz, zq}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {

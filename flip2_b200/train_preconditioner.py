@@ -7,9 +7,12 @@ Training problems on a cells^3 grid: generated pressure problems (solid
 spheres of radius 4..16 voxels to 10% of the box, a fluid surface at 50-85%
 of the height, six Gaussian velocity impulses plus gravity) alternating with
 the pressure problems of a dam-break simulation that runs in the same engine
-(block 0.5 x 0.5 x 1 of the box, Jacobi-PCG, dt 1/480).  A sample is the
-residual after k Jacobi-PCG iterations from x = 0, k drawn from
-0, 2, 5, 10, 20, 40, 80; the loss is |A N(r) - r|^2 / |r|^2; Adam.
+(block 0.5 x 0.5 x 1 of the box, Jacobi-PCG, dt 1/480).  The solver applies
+M(r) = N(r) + D^-1 r.  A sample is (r, e) with A e = r: 70% the residual and
+error of x_k after k Jacobi-PCG iterations from x = 0 (k drawn from 0, 2, 5,
+10, 20, 40, 80; e = x* - x_k against the problem's converged solution), 30%
+white-noise errors e with r = A e.  The loss is the A-norm error of M(r) as
+an estimate of e, relative to |e|_A; Adam.
 
 Evaluation: Jacobi-PCG against learned FPCG (tol 1e-6) on held-out generated
 problems and on dam-break steps, iterations and device milliseconds, one
@@ -57,6 +60,7 @@ def main():
     ap.add_argument("--out", default="flip2_b200/data/lprec_weights.npy")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--eval-problems", type=int, default=8)
+    ap.add_argument("--noise", type=float, default=0.3, help="fraction of white-noise error samples")
     args = ap.parse_args()
 
     P, pos, vel = make_engine(args.cells)
@@ -82,7 +86,7 @@ def main():
         frac = min(1.0, (time.time() - t0) / budget)
         lr = args.lr * (args.lr_final / args.lr) ** frac
         for _ in range(args.steps_per_problem):
-            k = int(SAMPLE_ITERS[rng.integers(len(SAMPLE_ITERS))])
+            k = int(SAMPLE_ITERS[rng.integers(len(SAMPLE_ITERS))]) if rng.random() >= args.noise else -1
             losses.append(P.lp_train_step(k, lr))
             step += 1
         if prob % 50 == 0:

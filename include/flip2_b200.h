@@ -280,14 +280,19 @@ int flip_get_solve_info(flip_engine* e, flip_solve_info* out);
 int flip_poisson_solve(flip_engine* e, int method, double tol, int max_iter, flip_solve_info* info);
 /* solution (FP64) in x-fastest order */
 int flip_poisson_read_solution(flip_engine* e, double* x_lin);
-/* one training step on the current problem: Jacobi-PCG runs pcg_iters
- * iterations from b, its residual r is the sample, loss
- * |A N(r) - r|^2 / |r|^2, one Adam step at rate lr; *loss before the step */
-int flip_lp_train_step(flip_engine* e, int pcg_iters, float lr, double* loss);
-/* evaluate N on a given residual (x fastest) of the current problem: z out
- * (x fastest, may be NULL), the loss, and with want_grad the weight
+/* The solver applies M(r) = N(r) + D^-1 r (network plus Jacobi).  One
+ * training step on the current problem with a sample (r, e), A e = r:
+ *   sample >= 0: x_k after `sample` Jacobi-PCG iterations from 0, r its
+ *                residual and e = x* - x_k, x* the problem's converged
+ *                solution (solved once per problem, or the solve just done);
+ *   sample = -1: e white noise on the fluid cells and r = A e.
+ * Loss L = |M(r) - e|_A^2 / |e|_A^2, one Adam step at rate lr; *loss is the
+ * value before the step. */
+int flip_lp_train_step(flip_engine* e, int sample, float lr, double* loss);
+/* evaluate on a given r and e (x fastest) of the current problem: z = N(r)
+ * out (x fastest, may be NULL), the loss, and with want_grad the weight
  * gradient (flip_lp_get_grad) without updating the weights */
-int flip_lp_eval(flip_engine* e, const float* r_lin, float* z_lin, double* loss, int want_grad);
+int flip_lp_eval(flip_engine* e, const float* r_lin, const float* e_lin, float* z_lin, double* loss, int want_grad);
 
 typedef struct {
     uint32_t nodes;          /* occupied root cells (REFERENCE) / tiles (NATIVE)   */

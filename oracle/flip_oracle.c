@@ -900,12 +900,13 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
 /* ============================================ learned preconditioner (CPU)
  * The product's pressure-preconditioner network, restated for the parity
  * tests (it has no reference counterpart).  Grids are x fastest, nx*ny*nz.
- * Four 3^3 convolutions, channels 3 -> 16 -> 16 -> 16 -> 1, dilations dil[],
- * ReLU after the first three, zero padding outside the box.  Weights are
- * [27 taps][Cin][Cout] per layer with tap = 9 (dz+1) + 3 (dy+1) + (dx+1) and
- * the neighbour at (i + dil dx, j + dil dy, k + dil dz).  Inputs at a cell:
- * r/s (fluid only), fluid flag, solid flag with s = rms of r over the fluid
- * cells; the output is s * N and zero off fluid cells.
+ * f: four 3^3 convolutions, channels 3 -> 16 -> 16 -> 16 -> 1, dilations
+ * dil[], ReLU after the first three, zero padding outside the box.  Weights
+ * are [27 taps][Cin][Cout] per layer with tap = 9 (dz+1) + 3 (dy+1) + (dx+1)
+ * and the neighbour at (i + dil dx, j + dil dy, k + dil dz).  Inputs at a
+ * cell: r/s (fluid only), fluid flag, solid flag with s = rms of r over the
+ * fluid cells.  The network is N(r) = s (f(r/s) - f(0)) on fluid cells and 0
+ * elsewhere; f(0) sees the geometry channels alone.
  * round_bf16 = 1 rounds the weights and the three hidden activations to
  * BF16 (round to nearest even), as the CUDA kernels store them; sums are
  * FP64 here and FP32 on the GPU. */
@@ -981,9 +982,28 @@ static void lp_conv(const lp_dims* D, const float* in, int cin, const float* W, 
 typedef struct {
     float* in;      /* [nc][3]  */
     float* act[3];  /* [nc][16] */
+    float* in0;     /* the zero-residual pass f(0): inputs and activations */
+    float* act0[3];
     float* wr;      /* weights as used (rounded or not) */
     float inv_s, s;
 } lp_fwd;
+
+/* f on given input channels: hidden activations into act[], output into out[nc] (FP64 sums) */
+static void lp_f(const lp_dims* D, const float* in, const float* wr, const int* dil, int round_bf16, float** act,
+                 double* tmp, double* out) {
+    const int64_t nc = D->nc;
+    const float* cur = in;
+    for (int l = 0; l < 3; ++l) {
+        lp_conv(D, cur, LP_CIN[l], wr + LP_OFF[l], 16, dil[l], tmp);
+        act[l] = (float*)malloc(sizeof(float) * 16 * nc);
+        for (int64_t q = 0; q < 16 * nc; ++q) {
+            float a = (float)(tmp[q] > 0.0 ? tmp[q] : 0.0);
+            act[l][q] = round_bf16 ? bf16_round(a) : a;
+        }
+        cur = act[l];
+    }
+    lp_conv(D, cur, 16, wr + LP_OFF[3], 1, dil[3], out);
+}
 
 static void lp_forward_keep(const lp_dims* D, const uint8_t* type, const float* r, const float* w, const int* dil,
                             int round_bf16, float* z, lp_fwd* F) {
@@ -1002,25 +1022,32 @@ static void lp_forward_keep(const lp_dims* D, const uint8_t* type, const float* 
         F->in[3 * v + 1] = fl ? 1.0f : 0.0f;
         F->in[3 * v + 2] = type[v] == NAT_SOLID ? 1.0f : 0.0f;
     }
-    double* tmp = (double*)malloc(sizeof(double) * 16 * nc);
-    const float* cur = F->in;
-    for (int l = 0; l < 3; ++l) {
-        lp_conv(D, cur, LP_CIN[l], F->wr + LP_OFF[l], 16, dil[l], tmp);
-        F->act[l] = (float*)malloc(sizeof(float) * 16 * nc);
-        for (int64_t q = 0; q < 16 * nc; ++q) {
-            float a = (float)(tmp[q] > 0.0 ? tmp[q] : 0.0);
-            F->act[l][q] = round_bf16 ? bf16_round(a) : a;
-        }
-        cur = F->act[l];
+    F->in0 = (float*)malloc(sizeof(float) * 3 * nc);
+    for (int64_t v = 0; v < nc; ++v) {
+        F->in0[3 * v] = 0.0f;
+        F->in0[3 * v + 1] = F->in[3 * v + 1];
+        F->in0[3 * v + 2] = F->in[3 * v + 2];
     }
-    lp_conv(D, cur, 16, F->wr + LP_OFF[3], 1, dil[3], tmp);
-    for (int64_t v = 0; v < nc; ++v) z[v] = type[v] == NAT_FLUID ? (float)tmp[v] * F->s : 0.0f;
+    double* tmp = (double*)malloc(sizeof(double) * 16 * nc);
+    double* o = (double*)malloc(sizeof(double) * nc);
+    double* o0 = (double*)malloc(sizeof(double) * nc);
+    lp_f(D, F->in, F->wr, dil, round_bf16, F->act, tmp, o);
+    lp_f(D, F->in0, F->wr, dil, round_bf16, F->act0, tmp, o0);
+    /* the GPU rounds f(0) to FP32 before the subtraction */
+    for (int64_t v = 0; v < nc; ++v)
+        z[v] = type[v] == NAT_FLUID ? (float)((double)(float)o[v] - (double)(float)o0[v]) * F->s : 0.0f;
     free(tmp);
+    free(o);
+    free(o0);
 }
 
 static void lp_fwd_free(lp_fwd* F) {
     free(F->in);
-    for (int l = 0; l < 3; ++l) free(F->act[l]);
+    free(F->in0);
+    for (int l = 0; l < 3; ++l) {
+        free(F->act[l]);
+        free(F->act0[l]);
+    }
     free(F->wr);
 }
 
@@ -1086,55 +1113,86 @@ static void lp_dgrad(const lp_dims* D, const double* g, int cout, const float* W
             }
 }
 
-/* loss L = |A z - r|^2 / |r|^2 over the fluid cells and its gradient with
- * respect to the (unrounded) weights; the BF16 roundings pass the gradient
- * straight through.  Returns L; z and grad (orc_lp_num_weights()) out. */
-double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
-                        int round_bf16, float* z, double* grad) {
+/* Jacobi diagonal inverse 1/d on fluid cells (d = non-solid neighbours, walls solid), 0 elsewhere */
+static void lp_dinv(const lp_dims* D, const uint8_t* type, double* dinv) {
+    static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    for (int k = 0; k < D->nz; ++k)
+        for (int j = 0; j < D->ny; ++j)
+            for (int i = 0; i < D->nx; ++i) {
+                int64_t id = lp_at(D, i, j, k);
+                double d = 0.0;
+                if (type[id] == NAT_FLUID)
+                    for (int q = 0; q < 6; ++q) {
+                        int64_t n = lp_at(D, i + off[q][0], j + off[q][1], k + off[q][2]);
+                        if (n >= 0 && type[n] != NAT_SOLID) d += 1.0;
+                    }
+                dinv[id] = d > 0.0 ? 1.0 / d : 0.0;
+            }
+}
+
+/* Training loss of the learned preconditioner M(r) = N(r) + D^-1 r for a
+ * sample (r, e) with A e = r (e = x* - x_k from a solver run, or white
+ * noise): the A-norm error of M(r) as an approximation of e, relative to
+ * e's own,
+ *     L = |M(r) - e|_A^2 / |e|_A^2 = (m.Am - 2 m.r) / e.r + 1,
+ * evaluated with the given r and e (e.r normalises).  Returns L; z = N(r)
+ * (the network output alone) and the gradient with respect to the
+ * (unrounded) weights out; the BF16 roundings pass the gradient straight
+ * through.  dL/dN = 2 (A m - r) / e.r on the fluid cells. */
+double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* ev, const float* w,
+                        const int* dil, int round_bf16, float* z, double* grad) {
     lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
     const int64_t nc = D.nc;
     lp_fwd F;
     lp_forward_keep(&D, type, r, w, dil, round_bf16, z, &F);
-    double* zd = (double*)malloc(sizeof(double) * nc);
-    double* e = (double*)malloc(sizeof(double) * nc);
+    double* m = (double*)malloc(sizeof(double) * nc);
+    double* am = (double*)malloc(sizeof(double) * nc);
+    double* dinv = (double*)malloc(sizeof(double) * nc);
     double* gz = (double*)malloc(sizeof(double) * nc);
-    for (int64_t v = 0; v < nc; ++v) zd[v] = z[v];
-    lp_apply_A(&D, type, zd, e);
-    double l2 = 0.0, nf = 0.0;
+    lp_dinv(&D, type, dinv);
+    for (int64_t v = 0; v < nc; ++v) m[v] = type[v] == NAT_FLUID ? (double)z[v] + dinv[v] * (double)r[v] : 0.0;
+    lp_apply_A(&D, type, m, am);
+    double mam = 0.0, mr = 0.0, er = 0.0;
     for (int64_t v = 0; v < nc; ++v) {
-        if (type[v] != NAT_FLUID) { e[v] = 0.0; continue; }
-        e[v] = (e[v] - (double)r[v]) * (double)F.inv_s;
-        l2 += e[v] * e[v];
-        nf += 1.0;
+        if (type[v] != NAT_FLUID) continue;
+        mam += m[v] * am[v];
+        mr += m[v] * (double)r[v];
+        er += (double)ev[v] * (double)r[v];
     }
-    if (nf < 1.0) nf = 1.0;
-    const double loss = l2 / nf;
+    const double loss = (mam - 2.0 * mr) / er + 1.0;
     if (grad) {
         memset(grad, 0, sizeof(double) * LP_OFF[4]);
-        lp_apply_A(&D, type, e, gz);
-        /* dL/d(out of layer 3) = s * dL/dz, dL/dz = 2 A e inv_s / nf on fluid cells */
+        /* dL/d(out of layer 3) = s dL/dN */
         for (int64_t v = 0; v < nc; ++v)
-            gz[v] = type[v] == NAT_FLUID ? gz[v] * 2.0 * (double)F.inv_s / nf * (double)F.s : 0.0;
+            gz[v] = type[v] == NAT_FLUID ? 2.0 * (am[v] - (double)r[v]) / er * (double)F.s : 0.0;
         double* g = (double*)malloc(sizeof(double) * 16 * nc);
         double* g2 = (double*)malloc(sizeof(double) * 16 * nc);
-        lp_wgrad(&D, gz, 1, F.act[2], 16, dil[3], grad + LP_OFF[3]);
-        lp_dgrad(&D, gz, 1, F.wr + LP_OFF[3], 16, dil[3], F.act[2], g);
-        lp_wgrad(&D, g, 16, F.act[1], 16, dil[2], grad + LP_OFF[2]);
-        lp_dgrad(&D, g, 16, F.wr + LP_OFF[2], 16, dil[2], F.act[1], g2);
-        lp_wgrad(&D, g2, 16, F.act[0], 16, dil[1], grad + LP_OFF[1]);
-        lp_dgrad(&D, g2, 16, F.wr + LP_OFF[1], 16, dil[1], F.act[0], g);
-        lp_wgrad(&D, g, 16, F.in, 3, dil[0], grad + LP_OFF[0]);
+        /* through f(r/s) with +gz, then through f(0) with -gz */
+        for (int path = 0; path < 2; ++path) {
+            float** act = path ? F.act0 : F.act;
+            const float* in = path ? F.in0 : F.in;
+            if (path)
+                for (int64_t v = 0; v < nc; ++v) gz[v] = -gz[v];
+            lp_wgrad(&D, gz, 1, act[2], 16, dil[3], grad + LP_OFF[3]);
+            lp_dgrad(&D, gz, 1, F.wr + LP_OFF[3], 16, dil[3], act[2], g);
+            lp_wgrad(&D, g, 16, act[1], 16, dil[2], grad + LP_OFF[2]);
+            lp_dgrad(&D, g, 16, F.wr + LP_OFF[2], 16, dil[2], act[1], g2);
+            lp_wgrad(&D, g2, 16, act[0], 16, dil[1], grad + LP_OFF[1]);
+            lp_dgrad(&D, g2, 16, F.wr + LP_OFF[1], 16, dil[1], act[0], g);
+            lp_wgrad(&D, g, 16, in, 3, dil[0], grad + LP_OFF[0]);
+        }
         free(g);
         free(g2);
     }
-    free(zd);
-    free(e);
+    free(m);
+    free(am);
+    free(dinv);
     free(gz);
     lp_fwd_free(&F);
     return loss;
 }
 
-/* flexible CG (FCG(1)) with the network as preconditioner, in
+/* flexible CG (FCG(1)) with M(r) = N(r) + D^-1 r as preconditioner, in
  * FP64 apart from the network; returns iterations (max_iter + 1 if not
  * converged), x out, *rel_res = |b - A x| / |b| */
 int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
@@ -1144,6 +1202,8 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
     double *r = (double*)calloc((size_t)nc, 8), *p = (double*)calloc((size_t)nc, 8), *q = (double*)calloc((size_t)nc, 8),
            *zd = (double*)calloc((size_t)nc, 8);
     float *rf = (float*)calloc((size_t)nc, 4), *zf = (float*)calloc((size_t)nc, 4);
+    double* dinv = (double*)malloc(sizeof(double) * nc);
+    lp_dinv(&D, type, dinv);
     double bb = 0.0;
     for (int64_t v = 0; v < nc; ++v) {
         x[v] = 0.0;
@@ -1159,7 +1219,7 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
             orc_lp_forward(nx, ny, nz, type, rf, w, dil, round_bf16, zf, NULL);
             double rzn = 0.0, zq = 0.0;
             for (int64_t v = 0; v < nc; ++v) {
-                zd[v] = zf[v];
+                zd[v] = (double)zf[v] + dinv[v] * r[v]; /* M(r) = N(r) + D^-1 r */
                 rzn += r[v] * zd[v];
                 zq += zd[v] * q[v];
             }
@@ -1187,6 +1247,6 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
     for (int64_t v = 0; v < nc; ++v)
         if (type[v] == NAT_FLUID) { double d = b[v] - q[v]; rr += d * d; }
     if (rel_res) *rel_res = bn > 0.0 ? sqrt(rr) / bn : 0.0;
-    free(r); free(p); free(q); free(zd); free(rf); free(zf);
+    free(r); free(p); free(q); free(zd); free(rf); free(zf); free(dinv);
     return it;
 }

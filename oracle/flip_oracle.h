@@ -166,8 +166,8 @@ void orc_nat_apply_A(const uint8_t* type, const double* x, double* y, const orc_
 int orc_lp_num_weights(void);
 void orc_lp_forward(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
                     int round_bf16, float* z, double* inv_s);
-double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
-                        int round_bf16, float* z, double* grad);
+double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* e, const float* w,
+                        const int* dil, int round_bf16, float* z, double* grad);
 int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
                 int round_bf16, double tol, int max_iter, double* x, double* rel_res);
 

@@ -80,7 +80,7 @@ def lib():
             "orc_nat_apply_A": (None, [u8p, f64p, f64p, C.POINTER(NatParams)]),
             "orc_lp_num_weights": (I, []),
             "orc_lp_forward": (None, [I, I, I, u8p, f32p, f32p, i32p, I, f32p, C.POINTER(D)]),
-            "orc_lp_loss_grad": (D, [I, I, I, u8p, f32p, f32p, i32p, I, f32p, f64p]),
+            "orc_lp_loss_grad": (D, [I, I, I, u8p, f32p, f32p, f32p, i32p, I, f32p, f64p]),
             "orc_lp_fpcg": (I, [I, I, I, u8p, f64p, f32p, i32p, I, D, I, f64p, C.POINTER(D)]),
         }
         for name, (res, args) in sig.items():
@@ -274,14 +274,16 @@ def lp_forward(type_, r, w, shape, dil=LP_DIL, round_bf16=True):
     return z, inv_s.value
 
 
-def lp_loss_grad(type_, r, w, shape, dil=LP_DIL, round_bf16=True):
-    """(loss, z, dloss/dw) of the residual loss |A z - r|^2 / |r|^2."""
+def lp_loss_grad(type_, r, e, w, shape, dil=LP_DIL, round_bf16=True):
+    """(loss, z = N(r), dloss/dw) of the A-norm loss of M(r) = N(r) + D^-1 r
+    against the error e (A e = r): (m.Am - 2 m.r) / e.r + 1."""
     nx, ny, nz = shape
     z = np.empty(nx * ny * nz, np.float32)
     g = np.empty(lib().orc_lp_num_weights(), np.float64)
     loss = lib().orc_lp_loss_grad(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(),
-                                  np.ascontiguousarray(r, np.float32).ravel(), np.ascontiguousarray(w, np.float32),
-                                  np.ascontiguousarray(dil, np.int32), int(round_bf16), z, g)
+                                  np.ascontiguousarray(r, np.float32).ravel(), np.ascontiguousarray(e, np.float32).ravel(),
+                                  np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16),
+                                  z, g)
     return loss, z, g
 
 

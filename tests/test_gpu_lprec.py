@@ -69,7 +69,7 @@ def test_lp_centre_chain_exact(torch, a, expect):
     P.poisson_set(typ, np.zeros(typ.size, np.float32))
     P.lp_set_weights(centre_chain_weights(a))
     r = np.where(typ == 1, 1.0, 0.0).astype(np.float32)
-    z, loss = P.lp_eval(r)
+    z, loss = P.lp_eval(r, r)
     assert np.all(z[typ == 1] == np.float32(expect))
     assert np.all(z[typ != 1] == 0.0)
     P.close()
@@ -81,17 +81,19 @@ def test_lp_forward_loss_grad_vs_oracle(torch, shape, seed):
     typ = random_types(shape, seed)
     rng = np.random.default_rng(seed + 10)
     r = (rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    ev = (r + 0.5 * rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
     w = (rng.standard_normal(F.lib().flip_lp_num_weights()) * 0.15).astype(np.float32)
     P.poisson_set(typ, np.zeros(typ.size, np.float32))
     P.lp_set_weights(w)
-    z, loss = P.lp_eval(r, want_grad=True)
+    z, loss = P.lp_eval(r, ev, want_grad=True)
     g = P.lp_grad()
-    lo, zo, go = O.lp_loss_grad(typ.reshape(shape[::-1]), r, w, shape, round_bf16=True)
+    lo, zo, go = O.lp_loss_grad(typ.reshape(shape[::-1]), r, ev, w, shape, round_bf16=True)
     # FP32 sums on the GPU vs FP64 here, and the rare activation whose BF16
     # rounding flips with that: 2e-3 in L2 and 2e-2 of the largest value
     assert np.linalg.norm(z - zo) <= 2e-3 * np.linalg.norm(zo)
     assert rel_err(z, zo) <= 2e-2
-    assert abs(loss - lo) <= 2e-3 * lo
+    # the loss is (m.Am - 2 m.r)/e.r + 1: compare the A-norm terms, 2e-3 of their size
+    assert abs(loss - lo) <= 2e-3 * max(1.0, abs(lo))
     # the gradient sums millions of products through FP32 atomics: 5e-3 in L2
     # over all weights and per layer
     assert np.linalg.norm(g - go) <= 5e-3 * np.linalg.norm(go)
@@ -117,7 +119,7 @@ def test_lp_tensor_cores_match_cuda_cores(torch):
         P = engine(shape, lp_cuda_cores=cc)
         P.poisson_set(typ, np.zeros(typ.size, np.float32))
         P.lp_set_weights(w)
-        z, loss = P.lp_eval(r)
+        z, loss = P.lp_eval(r, r)
         assert P.info().error_flags == 0
         zs.append(z)
         P.close()
@@ -170,7 +172,7 @@ def trained(torch):
     P = engine(shape)
     P.lp_init(seed=0)
     losses = []
-    iters = [0, 2, 5, 10, 20, 40]
+    iters = [0, 2, 5, 10, 20, 40, -1]
     for step in range(240):
         if step % 4 == 0:
             P.poisson_generate(seed=1000 + step, radius=(2.0, 5.0))

@@ -1,15 +1,15 @@
 """The oracle's restatement of the learned pressure preconditioner, pinned
 against PyTorch autograd (an independent implementation of the same dilated
-3^3 convolutions, run here in FP64 on the CPU): forward output, residual loss
-and the weight gradient.  The network has no reference counterpart, so torch
-is its pin."""
+3^3 convolutions, run here in FP64 on the CPU): forward output, the A-norm
+training loss of M(r) = N(r) + D^-1 r and the weight gradient.  The network
+has no reference counterpart, so torch is its pin."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 
 
-def _torch_net(T, typ, r, w, dil):
+def _torch_net(T, typ, r, ev, w, dil):
     import torch
     nw = w.size
     offs = [0, 27 * 3 * 16, 27 * 3 * 16 + 27 * 256, 27 * 3 * 16 + 2 * 27 * 256, nw]
@@ -23,19 +23,24 @@ def _torch_net(T, typ, r, w, dil):
     fl, so = (t == 1).double(), (t == 2).double()
     rt = torch.tensor(r, dtype=torch.float64) * fl
     s = torch.sqrt(torch.sum(rt ** 2) / fl.sum())
-    h = torch.stack([rt / s, fl, so])[None]
-    for l in range(4):
-        h = torch.nn.functional.conv3d(h, tw(l), padding=dil[l], dilation=dil[l])
-        if l < 3:
-            h = torch.relu(h)
-    z = h[0, 0] * s * fl
+    def f(x):
+        h = torch.stack([x, fl, so])[None]
+        for l in range(4):
+            h = torch.nn.functional.conv3d(h, tw(l), padding=dil[l], dilation=dil[l])
+            if l < 3:
+                h = torch.relu(h)
+        return h[0, 0]
+
+    z = (f(rt / s) - f(torch.zeros_like(rt))) * s * fl
     k = torch.zeros(1, 1, 3, 3, 3, dtype=torch.float64)
     for (a, b, c) in ((0, 1, 1), (2, 1, 1), (1, 0, 1), (1, 2, 1), (1, 1, 0), (1, 1, 2)):
         k[0, 0, a, b, c] = 1.0
     d = torch.nn.functional.conv3d((t != 2).double()[None, None], k, padding=1)[0, 0]
-    zf = z * fl
-    Az = (d * zf - torch.nn.functional.conv3d(zf[None, None], k, padding=1)[0, 0]) * fl
-    loss = torch.sum((Az - rt) ** 2) / torch.sum(rt ** 2)
+    dinv = torch.where(fl > 0, 1.0 / d.clamp(min=1.0), torch.zeros_like(d))
+    m = (z + dinv * rt) * fl
+    Am = (d * m - torch.nn.functional.conv3d(m[None, None], k, padding=1)[0, 0]) * fl
+    et = torch.tensor(ev, dtype=torch.float64) * fl
+    loss = (torch.sum(m * Am) - 2.0 * torch.sum(m * rt)) / torch.sum(et * rt) + 1.0
     loss.backward()
     return z.detach().numpy().ravel(), float(loss.detach()), W.grad.numpy()
 
@@ -47,9 +52,10 @@ def test_lp_oracle_vs_torch_autograd(shape, dil):
     rng = np.random.default_rng(3)
     typ = rng.choice([0, 1, 1, 1, 2], size=(nz, ny, nx)).astype(np.uint8)
     r = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    ev = (r + 0.5 * rng.standard_normal((nz, ny, nx))).astype(np.float32)  # any e with e.r > 0 normalises
     w = (rng.standard_normal(O.lib().orc_lp_num_weights()) * 0.2).astype(np.float32)
-    loss, z, g = O.lp_loss_grad(typ, r, w, shape, dil=dil, round_bf16=False)
-    zt, lt, gt = _torch_net(torch, typ, r, w, dil)
+    loss, z, g = O.lp_loss_grad(typ, r, ev, w, shape, dil=dil, round_bf16=False)
+    zt, lt, gt = _torch_net(torch, typ, r, ev, w, dil)
     # the oracle keeps FP32 inputs and activations, torch FP64: 1e-6 bounds that
     assert np.max(np.abs(z - zt)) <= 1e-6 * np.max(np.abs(zt))
     assert abs(loss - lt) <= 1e-6 * abs(lt)
