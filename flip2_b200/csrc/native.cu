@@ -348,13 +348,13 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
 // neighbour (air neighbours are Dirichlet zero, solid ones Neumann).
 
 // last CTA to finish sums the per-CTA partials (fixed order: deterministic)
-template <int NV>
-__device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
-                                                  double (&out)[NV]) {
+template <int NV, int NT>
+__device__ __forceinline__ bool last_block_reduce_n(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
+                                                    double (&out)[NV]) {
     __shared__ bool s_last;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
-        double r = block_sum_f64<512>(v[q], sh);
+        double r = block_sum_f64<NT>(v[q], sh);
         if (threadIdx.x == 0) partials[q * kPcgBlocks + blockIdx.x] = r;
     }
     __threadfence();
@@ -366,11 +366,16 @@ __device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* parti
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         double a = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += 512) a += ((volatile double*)partials)[q * kPcgBlocks + b];
-        out[q] = block_sum_f64<512>(a, sh);
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) a += ((volatile double*)partials)[q * kPcgBlocks + b];
+        out[q] = block_sum_f64<NT>(a, sh);
     }
     if (threadIdx.x == 0) *ticket = 0u;
     return true;  // out[] valid in thread 0
+}
+template <int NV>
+__device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
+                                                  double (&out)[NV]) {
+    return last_block_reduce_n<NV, 512>(v, partials, ticket, sh, out);
 }
 
 #define NAT_TILE_LOOP_BEGIN                                                                   \
@@ -476,10 +481,46 @@ struct DirLoads {
     uint8_t c, hc;
 };
 
+// The halo cell a thread loads, as constants of the thread: face f = tid/64
+// (0..5: -x, +x, -y, +y, -z, +z; 6, 7: none), the neighbour tile's key
+// offset, the cell's slot inside that tile, and the tile-coordinate test for
+// the neighbour to exist (packed coordinates: 10 bits per axis).
+struct HaloSlot {
+    int face;
+    int delta;     // neighbour key = key + delta
+    uint32_t hl;   // slot within the neighbour tile
+    int shift;     // bit offset of the face's axis in the packed coordinates
+    int lim;       // -1: need coordinate > 0; else need coordinate < lim
+    int hx, hy, hz;  // offsets from the tile origin, -1..8 (shared-memory box)
+};
+__device__ __forceinline__ HaloSlot halo_slot(int tid, const NatDims& D) {
+    HaloSlot h;
+    h.face = tid >> 6;
+    const int e0 = tid & 7, e1 = (tid >> 3) & 7;
+    h.delta = 0; h.hl = 0; h.shift = 0; h.lim = -1; h.hx = h.hy = h.hz = 0;
+    switch (h.face) {
+    case 0: h.delta = -1; h.hl = 7 + 8 * e0 + 64 * e1; h.shift = 0; h.lim = -1; h.hx = -1; h.hy = e0; h.hz = e1; break;
+    case 1: h.delta = 1; h.hl = 8 * e0 + 64 * e1; h.shift = 0; h.lim = D.tx - 1; h.hx = 8; h.hy = e0; h.hz = e1; break;
+    case 2: h.delta = -D.tx; h.hl = e0 + 56 + 64 * e1; h.shift = 10; h.lim = -1; h.hx = e0; h.hy = -1; h.hz = e1; break;
+    case 3: h.delta = D.tx; h.hl = e0 + 64 * e1; h.shift = 10; h.lim = D.ty - 1; h.hx = e0; h.hy = 8; h.hz = e1; break;
+    case 4: h.delta = -D.tx * D.ty; h.hl = e0 + 8 * e1 + 448; h.shift = 20; h.lim = -1; h.hx = e0; h.hy = e1; h.hz = -1; break;
+    case 5: h.delta = D.tx * D.ty; h.hl = e0 + 8 * e1; h.shift = 20; h.lim = D.tz - 1; h.hx = e0; h.hy = e1; h.hz = 8; break;
+    default: break;
+    }
+    return h;
+}
+// slot of the thread's halo cell for the tile (key, packed coordinates tc), or -1
+__device__ __forceinline__ int64_t halo_at(const HaloSlot& h, uint32_t key, uint32_t tc) {
+    if (h.face >= 6) return -1;
+    const int c = (int)((tc >> h.shift) & 1023u);
+    const bool ok = h.lim < 0 ? c > 0 : c < h.lim;
+    if (!ok) return -1;
+    return (int64_t)((((uint32_t)((int)key + h.delta)) << 9) | h.hl);
+}
+
 __device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ tcoord,
-                                         uint32_t t, const NatDims& D, const float* __restrict__ r,
-                                         const float* __restrict__ p, const uint8_t* __restrict__ cell, int face, int hx,
-                                         int hy, int hz) {
+                                         uint32_t t, const HaloSlot& H, const float* __restrict__ r,
+                                         const float* __restrict__ p, const uint8_t* __restrict__ cell) {
     const uint32_t key = tiles[t];
     L.key = key;
     const uint32_t s = (key << 9) | threadIdx.x;
@@ -489,11 +530,9 @@ __device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict
     L.hc = 0;
     L.hr = 0.0f;
     L.hp = 0.0f;
-    if (face < 6) {
-        const uint32_t tc = tcoord[t];
-        const int i = 8 * (int)(tc & 1023u) + hx, j = 8 * (int)((tc >> 10) & 1023u) + hy, k = 8 * (int)(tc >> 20) + hz;
-        if (i >= 0 && j >= 0 && k >= 0 && i < D.nx && j < D.ny && k < D.nz) {
-            const uint32_t sn = nslot(i, j, k, D);
+    if (H.face < 6) {
+        const int64_t sn = halo_at(H, key, tcoord[t]);
+        if (sn >= 0) {
             L.hc = cell[sn];
             L.hr = r[sn];
             L.hp = p[sn];
@@ -524,19 +563,13 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
     const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
     const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
     // halo cell handled by this thread (384 of them: 6 faces x 64)
-    const int face = tid >> 6, e0 = tid & 7, e1 = (tid >> 3) & 7;
-    int hx = 0, hy = 0, hz = 0;  // offsets from the tile origin, -1..8
-    if (face == 0) { hx = -1; hy = e0; hz = e1; }
-    else if (face == 1) { hx = 8; hy = e0; hz = e1; }
-    else if (face == 2) { hx = e0; hy = -1; hz = e1; }
-    else if (face == 3) { hx = e0; hy = 8; hz = e1; }
-    else if (face == 4) { hx = e0; hy = e1; hz = -1; }
-    else if (face == 5) { hx = e0; hy = e1; hz = 8; }
-    const int bh = (hx + 1) + 10 * ((hy + 1) + 10 * (hz + 1));
+    const HaloSlot H = halo_slot(tid, D);
+    const int face = H.face;
+    const int bh = (H.hx + 1) + 10 * ((H.hy + 1) + 10 * (H.hz + 1));
     double pq = 0.0;
     DirLoads cur;
     uint32_t t = blockIdx.x;
-    if (t < ntiles) dir_load(cur, tiles, tcoord, t, D, r, p, cell, face, hx, hy, hz);
+    if (t < ntiles) dir_load(cur, tiles, tcoord, t, H, r, p, cell);
     for (; t < ntiles; t += gridDim.x) {
         const uint32_t s = (cur.key << 9) | tid;
         const uint8_t c = cur.c;
@@ -550,7 +583,7 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
         }
         DirLoads nxt;
         const uint32_t tn = t + gridDim.x;
-        if (tn < ntiles) dir_load(nxt, tiles, tcoord, tn, D, r, p, cell, face, hx, hy, hz);
+        if (tn < ntiles) dir_load(nxt, tiles, tcoord, tn, H, r, p, cell);
         __syncthreads();
         float qc = 0.0f;
         if (c & kCellFluid) {
@@ -592,46 +625,56 @@ __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const fl
     }
 }
 
-__global__ void __launch_bounds__(512, 3) pcg_update_kernel(const uint32_t* __restrict__ tiles,
-                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
-                                                             float* __restrict__ xg, float* __restrict__ r,
-                                                             const float* p0, const float* p1, const float* __restrict__ q,
-                                                             const uint8_t* __restrict__ cell, PcgState* st,
-                                                             double* partials) {
+// One warp per tile: the warp's 32 lanes hold the tile's 128 quads, four
+// each, and issue all 20 loads of a tile before using any of them; the next
+// tile's key is loaded one tile ahead.
+constexpr int kUpdThreads = 256;
+__global__ void __launch_bounds__(kUpdThreads, 2) pcg_update_kernel(const uint32_t* __restrict__ tiles,
+                                                                     const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                                     float* __restrict__ xg, float* __restrict__ r,
+                                                                     const float* p0, const float* p1,
+                                                                     const float* __restrict__ q,
+                                                                     const uint8_t* __restrict__ cell, PcgState* st,
+                                                                     double* partials) {
     if (st->done || st->pending) return;
     const float* __restrict__ p = st->pcur ? p0 : p1;  // the direction the matvec just wrote
     __shared__ double sh[32];
     __shared__ float tab[8];
     if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
     __syncthreads();
-    const uint32_t nquads = *d_ntiles * 128u;
+    const uint32_t ntiles = *d_ntiles;
     const float a = (float)st->alpha;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = gridDim.x * (kUpdThreads / 32);
+    uint32_t t = blockIdx.x * (kUpdThreads / 32) + (threadIdx.x >> 5);
     double rr = 0.0, rz = 0.0;
-    const uint32_t stride = gridDim.x * 512u;
-    for (uint32_t qd = blockIdx.x * 512u + threadIdx.x; qd < nquads; qd += 2u * stride) {
-        const uint32_t qe = qd + stride;
-        const bool two = qe < nquads;
-        const uint32_t s0 = (tiles[qd >> 7] << 9) | ((qd & 127u) << 2);
-        const uint32_t s1 = two ? ((tiles[qe >> 7] << 9) | ((qe & 127u) << 2)) : s0;
-        const uint32_t c0 = *reinterpret_cast<const uint32_t*>(cell + s0);
-        const uint32_t c1 = two ? *reinterpret_cast<const uint32_t*>(cell + s1) : 0u;
-        const float4 pa = *reinterpret_cast<const float4*>(p + s0), pb = *reinterpret_cast<const float4*>(p + s1);
-        const float4 qa = *reinterpret_cast<const float4*>(q + s0), qb = *reinterpret_cast<const float4*>(q + s1);
-        float4 ra = *reinterpret_cast<const float4*>(r + s0), rb = *reinterpret_cast<const float4*>(r + s1);
-        float4 ga = *reinterpret_cast<const float4*>(xg + s0), gb = *reinterpret_cast<const float4*>(xg + s1);
-        if (c0) {
-            upd_quad(tab, c0, pa, qa, ra, ga, a, rr, rz);
-            *reinterpret_cast<float4*>(r + s0) = ra;
-            *reinterpret_cast<float4*>(xg + s0) = ga;
+    uint32_t key = t < ntiles ? tiles[t] : 0u;
+    for (; t < ntiles; t += nwarps) {
+        const uint32_t tn = t + nwarps;
+        const uint32_t key_next = tn < ntiles ? tiles[tn] : 0u;
+        uint32_t c[4];
+        float4 pv[4], qv[4], rv[4], gv[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const uint32_t s = (key << 9) | (uint32_t)((lane + 32 * m) << 2);
+            c[m] = *reinterpret_cast<const uint32_t*>(cell + s);
+            pv[m] = *reinterpret_cast<const float4*>(p + s);
+            qv[m] = *reinterpret_cast<const float4*>(q + s);
+            rv[m] = *reinterpret_cast<const float4*>(r + s);
+            gv[m] = *reinterpret_cast<const float4*>(xg + s);
         }
-        if (c1) {
-            upd_quad(tab, c1, pb, qb, rb, gb, a, rr, rz);
-            *reinterpret_cast<float4*>(r + s1) = rb;
-            *reinterpret_cast<float4*>(xg + s1) = gb;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (!c[m]) continue;
+            const uint32_t s = (key << 9) | (uint32_t)((lane + 32 * m) << 2);
+            upd_quad(tab, c[m], pv[m], qv[m], rv[m], gv[m], a, rr, rz);
+            *reinterpret_cast<float4*>(r + s) = rv[m];
+            *reinterpret_cast<float4*>(xg + s) = gv[m];
         }
+        key = key_next;
     }
     double vals[2] = {rr, rz}, out[2];
-    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+    if (last_block_reduce_n<2, kUpdThreads>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
         st->iter += 1;
         st->pcur ^= 1;
         st->rr = out[0];
@@ -667,15 +710,8 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
     const int tid = threadIdx.x;
     const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
     const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
-    const int face = tid >> 6, e0 = tid & 7, e1 = (tid >> 3) & 7;
-    int hx = 0, hy = 0, hz = 0;
-    if (face == 0) { hx = -1; hy = e0; hz = e1; }
-    else if (face == 1) { hx = 8; hy = e0; hz = e1; }
-    else if (face == 2) { hx = e0; hy = -1; hz = e1; }
-    else if (face == 3) { hx = e0; hy = 8; hz = e1; }
-    else if (face == 4) { hx = e0; hy = e1; hz = -1; }
-    else if (face == 5) { hx = e0; hy = e1; hz = 8; }
-    const int bh = (hx + 1) + 10 * ((hy + 1) + 10 * (hz + 1));
+    const HaloSlot H = halo_slot(tid, D);
+    const int bh = (H.hx + 1) + 10 * ((H.hy + 1) + 10 * (H.hz + 1));
     double rr = 0.0, rz = 0.0;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const uint32_t key = tiles[t];
@@ -683,14 +719,10 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
         const uint8_t c = cell[s];
         const double xs = (c & kCellFluid) ? x[s] + (double)xg[s] : 0.0;
         X[bc] = xs;
-        if (face < 6) {
-            const uint32_t tc = tcoord[t];
-            const int i = 8 * (int)(tc & 1023u) + hx, j = 8 * (int)((tc >> 10) & 1023u) + hy, k = 8 * (int)(tc >> 20) + hz;
+        if (H.face < 6) {
+            const int64_t sn = halo_at(H, key, tcoord[t]);
             double v = 0.0;
-            if (i >= 0 && j >= 0 && k >= 0 && i < D.nx && j < D.ny && k < D.nz) {
-                const uint32_t sn = nslot(i, j, k, D);
-                if (cell[sn] & kCellFluid) v = x[sn] + (double)xg[sn];
-            }
+            if (sn >= 0 && (cell[sn] & kCellFluid)) v = x[sn] + (double)xg[sn];
             X[bh] = v;
         }
         __syncthreads();
@@ -931,8 +963,8 @@ int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_nt
                                      cudaStream_t s) {
     pcg_dirmatvec_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell, B.q, B.x,
                                                           B.xg, B.st, B.partials);
-    pcg_update_kernel<<<kPcgUpdateBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell, B.st,
-                                                       B.partials);
+    pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
+                                                               B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -945,8 +977,8 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
                              cudaStream_t s) {
     pcg_dirmatvec_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
                                                     B.st, B.partials);
-    pcg_update_kernel<<<kPcgUpdateBlocks, 512, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell, B.st,
-                                                       B.partials);
+    pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
+                                                               B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
