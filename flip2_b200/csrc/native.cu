@@ -551,7 +551,11 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
     if (st->done || st->pending) return;
     const float* __restrict__ p = st->pcur ? p1 : p0;
     float* __restrict__ pn = st->pcur ? p0 : p1;
-    __shared__ float P[1000];  // 10^3 box: tile + halo, index (x+1) + 10 (y+1) + 100 (z+1)
+    // 10^3 box: tile + halo, index (x+1) + 10 (y+1) + 100 (z+1); two of them,
+    // alternating per tile, so one barrier per tile suffices: a thread writes
+    // a box again only after the next tile's barrier, which every thread
+    // reaches after its reads of this box
+    __shared__ float Pbox[2][1000];
     __shared__ double sh[32];
     __shared__ float tab[8];
     if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
@@ -570,7 +574,8 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
     DirLoads cur;
     uint32_t t = blockIdx.x;
     if (t < ntiles) dir_load(cur, tiles, tcoord, t, H, r, p, cell);
-    for (; t < ntiles; t += gridDim.x) {
+    for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+        float* P = Pbox[it & 1];
         const uint32_t s = (cur.key << 9) | tid;
         const uint8_t c = cur.c;
         const float pc = kFlex ? dir_value_z(c, cur.r, cur.p, beta) : dir_value(tab, c, cur.r, cur.p, beta);
@@ -592,7 +597,6 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
         }
         q[s] = qc;
         pq += (double)pc * (double)qc;
-        __syncthreads();
         cur = nxt;
     }
     double vals[1] = {pq}, out[1];
