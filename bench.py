@@ -47,12 +47,56 @@ def parse_args():
     ap.add_argument("--impl", default="flip2_b200", choices=["flip2_b200", "reference"])
     ap.add_argument("--cells", type=int, default=N_CELLS, help="voxels per axis (default 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the learned-vs-plain pressure comparison")
+    ap.add_argument("--config", default="c2", choices=["c2", "c5"],
+                    help="c2: the 256^3 dam-break (default); c5: dam-break + sphere with the learned pressure solve")
     return ap.parse_args()
 
 
-def scene(cells):
+C5_SPHERE = (0.5, 0.75, 0.5, 0.15)  # centre-top sphere of radius 0.15 above the block
+
+
+def scene(cells, config="c2"):
     from flip2_b200 import scenes
-    return scenes.dam_break(cells, block=BLOCK, seed=0)
+    return scenes.dam_break(cells, block=BLOCK, seed=0, sphere=C5_SPHERE if config == "c5" else None)
+
+
+# ---------------------------------------------- learned vs plain pressure
+C4_CELLS = 128
+C4_PROBLEMS = 4
+C4_SEED0 = 900_000
+
+
+def c4_pressure(F, device):
+    """128^3 pressure problems (solid spheres of radius 4..16 voxels to 10% of
+    the box, fluid surface at 50-85% height, Gaussian impulses plus gravity),
+    solved to 1e-6 by Jacobi-PCG and by learned FCG with the committed weights
+    (Jacobi-PCG restart after 100 FCG iterations).  Device ms from CUDA events
+    inside the engine; the relative residuals are FP64 true residuals."""
+    wpath = os.path.join(ROOT, "flip2_b200", "data", "lprec_weights.npy")
+    if not os.path.exists(wpath):
+        return None
+    P = F.Particles(1, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE, device=device))
+    R = C4_CELLS // 4
+    P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
+    P.lp_set_weights(np.load(wpath))
+    P.poisson_generate(seed=C4_SEED0)
+    P.poisson_solve(0, 1e-6, 20000)  # warm-up: graphs and the network's buffers
+    P.poisson_solve(1, 1e-6, 4)
+    rows = []
+    for k in range(C4_PROBLEMS):
+        P.poisson_generate(seed=C4_SEED0 + k)
+        a = P.poisson_solve(0, 1e-6, 20000)
+        b = P.poisson_solve(1, 1e-6, 100)
+        rows.append({"plain_ms": a.ms, "plain_iters": a.iters, "plain_rel_residual": a.rel_residual,
+                     "learned_ms": b.ms, "learned_fcg_iters": b.iters, "fell_back": b.fell_back,
+                     "restart_iters": b.plain_iters, "learned_rel_residual": b.rel_residual})
+    P.close()
+    plain = sum(r["plain_ms"] for r in rows) / len(rows)
+    learned = sum(r["learned_ms"] for r in rows) / len(rows)
+    return {"workload": "128^3 generated pressure problems (seeds %d..%d), tol 1e-6" % (C4_SEED0, C4_SEED0 + C4_PROBLEMS - 1),
+            "plain_ms_mean": plain, "learned_ms_mean": learned, "speedup_learned_over_plain": plain / learned,
+            "fallback_rate": sum(r["fell_back"] for r in rows) / len(rows), "problems": rows}
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -187,13 +231,16 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    pos, vel = scene(args.cells)
+    pos, vel = scene(args.cells, args.config)
     n = pos.shape[0]
     stream = torch.cuda.Stream(device=dev)
-    params = F.default_params(F.MODE_NATIVE, device=local)
+    c5 = args.config == "c5"
+    params = F.default_params(F.MODE_NATIVE, device=local, pressure_method=1 if c5 else 0)
     P = F.Particles(n, mode=F.MODE_NATIVE, params=params, stream=stream.cuda_stream)
     R = args.cells // 4
     P.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / args.cells)
+    if c5:
+        P.lp_set_weights(np.load(os.path.join(ROOT, "flip2_b200", "data", "lprec_weights.npy")))
     # pinned host state for the end-to-end leg
     host = [torch.from_numpy(np.ascontiguousarray(pos[:, k])).pin_memory() for k in range(3)]
     host += [torch.from_numpy(np.ascontiguousarray(vel[:, k])).pin_memory() for k in range(3)]
@@ -225,8 +272,11 @@ def main():
     barrier()
     torch.cuda.synchronize(dev)
     ev0.record(stream)
+    fell_back = 0
     for _ in range(args.steps):
         P.step(DT)
+        if c5:
+            fell_back += P.solve_info().fell_back
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -288,20 +338,36 @@ def main():
                 "algorithmic_bytes": "49 B per active voxel per iteration x %d voxels" % voxels,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
 
+    # the north-star particle metric: binning, P2G and G2P/advection only
+    part_keys = ["keys", "sort", "gather", "segment_heads", "grid_clear", "p2g", "g2p_advect"]
+    part_ms = sum(stages[k] for k in part_keys)
+    particle_stages = {"value": n / (part_ms / 1e3), "unit": METRIC, "ms_per_step": part_ms, "stages": part_keys,
+                       "note": "stage times from CUDA events of the profiled steps; excludes pressure and projection"}
+
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not c5:
         cpu = cpu_baseline(args.cells)
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_c4 and not c5:
+        c4 = c4_pressure(F, local)
     if rank == 0:
+        workload = WORKLOAD
+        if c5:
+            workload = WORKLOAD.replace("block 0.5x0.5x1", "block 0.5x0.5x1 + sphere r=0.15 at (0.5,0.75,0.5)").replace(
+                "Jacobi-PCG to 1e-6", "learned FCG (100-iteration cap, Jacobi-PCG restart) to 1e-6")
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "particles": n, "grid": "%d^3" % args.cells, "dt": DT,
+                "config": {"workload": workload, "particles": n, "grid": "%d^3" % args.cells, "dt": DT,
                            "parallelism": "replicas x%d" % world,
                            "l2": "inputs larger than L2: %.0f MB particle state per replica" % (24 * n / 1e6)},
+                "particle_stages": particle_stages, "c4_pressure": c4,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
                 "pcg_iters_per_step": iters, "pressure_solve_ms": stages["pcg_setup"] + stages["pcg_iterations"],
                 "stages_ms": stages, "fluid_tiles": fluid_tiles,
                 "pcg_rel_residual": info.residual, "error_flags": info.error_flags}
+        if c5:
+            line["fallback_rate"] = fell_back / args.steps
         print(json.dumps(line), flush=True)
     P.close()
     if dist is not None:

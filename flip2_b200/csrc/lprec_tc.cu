@@ -241,6 +241,8 @@ static int launch_mid_tc(const LpGrid& G, const __nv_bfloat16* wb, const __nv_bf
     static bool attr_set = false;  // per process; the attribute is per function
     if (!attr_set) {
         FLIP_CUDA_TRY(cudaFuncSetAttribute(lp_mid_tc_kernel<DIL>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
+        // all of the unified L1 as shared memory, so several CTAs fit per SM
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(lp_mid_tc_kernel<DIL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         attr_set = true;
     }
     int per_sm = 0;
