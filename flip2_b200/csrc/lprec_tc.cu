@@ -245,9 +245,13 @@ static int launch_mid_tc(const LpGrid& G, const __nv_bfloat16* wb, const __nv_bf
         FLIP_CUDA_TRY(cudaFuncSetAttribute(lp_mid_tc_kernel<DIL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         attr_set = true;
     }
-    int per_sm = 0;
-    FLIP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lp_mid_tc_kernel<DIL>, kTcThreads, S::kBytes));
-    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);  // at most 4 x 128 TMEM columns per SM
+    // CTAs per SM from the shared-memory budget (each CTA also holds 1 KB of
+    // static and 1 KB of reserved shared memory); at most 4 x 128 TMEM columns
+    int dev = 0, smem_sm = 0;
+    FLIP_CUDA_TRY(cudaGetDevice(&dev));
+    FLIP_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    int per_sm = smem_sm / (S::kBytes + 2048);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
     lp_mid_tc_kernel<DIL><<<sms * per_sm, kTcThreads, S::kBytes, st>>>(G, wb, in, out, err);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;

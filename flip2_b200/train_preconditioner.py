@@ -38,7 +38,7 @@ def make_engine(cells, pressure_method=0):
     return P, pos, vel
 
 
-def evaluate(P, cells, seeds, tol=1e-6, max_iter=1000):
+def evaluate(P, cells, seeds, tol=1e-6, max_iter=100):
     rows = []
     for s in seeds:
         P.poisson_generate(seed=s)
@@ -61,6 +61,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--eval-problems", type=int, default=8)
     ap.add_argument("--noise", type=float, default=0.3, help="fraction of white-noise error samples")
+    ap.add_argument("--eval-max-iter", type=int, default=100, help="learned FCG cap in the evaluation")
+    ap.add_argument("--eval-dam-steps", type=int, default=40, help="dam-break steps per method in the evaluation")
     args = ap.parse_args()
 
     P, pos, vel = make_engine(args.cells)
@@ -98,20 +100,20 @@ def main():
     print(json.dumps({"trained_steps": step, "problems": prob, "seconds": round(train_s, 1),
                       "final_loss": float(np.mean(losses[-100:])), "out": args.out}), flush=True)
 
-    rows = evaluate(P, args.cells, range(900_000, 900_000 + args.eval_problems))
+    rows = evaluate(P, args.cells, range(900_000, 900_000 + args.eval_problems), max_iter=args.eval_max_iter)
     a = np.array(rows)
     print(json.dumps({"eval": "generated", "cells": args.cells, "jacobi_iters": a[:, 0].tolist(),
                       "jacobi_ms": np.round(a[:, 1], 2).tolist(), "learned_iters": a[:, 2].tolist(),
                       "learned_ms": np.round(a[:, 3], 2).tolist(), "fell_back": int(a[:, 4].sum())}), flush=True)
     P.close()
     # dam-break steps with each method
-    for method in (0, 1):
+    for method in ((0, 1) if args.eval_dam_steps > 0 else ()):
         Q, _, _ = make_engine(args.cells, pressure_method=method)
         if method:
             Q.lp_set_weights(w)
         Q.set_timing(True)
         its, ms, fb = [], [], 0
-        for k in range(40):
+        for k in range(args.eval_dam_steps):
             Q.step(1.0 / 480.0)
             si = Q.solve_info()
             its.append(si.iters + si.plain_iters)
