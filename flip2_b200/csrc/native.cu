@@ -608,6 +608,177 @@ __global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Vectorised direction update + matvec.  A CTA of 512 threads runs four
+// independent groups of 128; each group walks its own tiles and syncs on its
+// own named barrier.  A thread owns four consecutive x-cells of one (y, z) row
+// (float4 loads and stores) and three of the tile's 384 halo cells.  The
+// tile's p' goes to a 10 x 10 x 16-float shared box (rows padded so that
+// x = 0 and x = 4 start on 16 bytes; x = -1 .. 8 at row offsets 3 .. 12),
+// two boxes per group alternating per tile, and the stencil reads its y and
+// z neighbours as 16-byte rows.  Loads of the group's next tile are issued
+// before the current tile's barrier.
+constexpr int kDm4Groups = 4;
+constexpr int kDm4Blocks = 296;  // 148 SMs x 2 CTAs
+constexpr int kBoxRow = 16;
+constexpr int kBoxFloats = 10 * 10 * kBoxRow;
+__device__ __forceinline__ int box_at(int x, int y, int z) { return ((z + 1) * 10 + (y + 1)) * kBoxRow + x + 4; }
+
+struct Dm4Loads {
+    uint32_t key;
+    float4 r, p;
+    uint32_t c;
+    float hr[3], hp[3];
+    uint32_t hc;  // the three halo codes, a byte each
+};
+
+template <bool kFlex>
+__device__ __forceinline__ float4 dir4(const float* tab, uint32_t c4, float4 r, float4 p, float beta) {
+    float4 o;
+    o.x = kFlex ? dir_value_z((uint8_t)c4, r.x, p.x, beta) : dir_value(tab, (uint8_t)c4, r.x, p.x, beta);
+    o.y = kFlex ? dir_value_z((uint8_t)(c4 >> 8), r.y, p.y, beta) : dir_value(tab, (uint8_t)(c4 >> 8), r.y, p.y, beta);
+    o.z = kFlex ? dir_value_z((uint8_t)(c4 >> 16), r.z, p.z, beta) : dir_value(tab, (uint8_t)(c4 >> 16), r.z, p.z, beta);
+    o.w = kFlex ? dir_value_z((uint8_t)(c4 >> 24), r.w, p.w, beta) : dir_value(tab, (uint8_t)(c4 >> 24), r.w, p.w, beta);
+    return o;
+}
+
+constexpr int kDm4Smem = kDm4Groups * 2 * kBoxFloats * (int)sizeof(float);
+template <bool kFlex>
+__global__ void __launch_bounds__(512, 2) pcg_dirmatvec4_kernel(const uint32_t* __restrict__ tiles,
+                                                                 const uint32_t* __restrict__ tcoord,
+                                                                 const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                                 const float* __restrict__ r, float* p0, float* p1,
+                                                                 const uint8_t* __restrict__ cell, float* __restrict__ q,
+                                                                 double* __restrict__ x, float* __restrict__ xg,
+                                                                 PcgState* st, double* partials) {
+    if (st->done || st->pending) return;
+    const float* __restrict__ p = st->pcur ? p1 : p0;
+    float* __restrict__ pn = st->pcur ? p0 : p1;
+    extern __shared__ __align__(16) float dm4_box[];  // [groups][2][kBoxFloats], dynamic (51 KB)
+    __shared__ double sh[32];
+    __shared__ float tab[8];
+    __shared__ int fdelta[6], flim[6];
+    if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
+    if (threadIdx.x < 6) {
+        const int f = threadIdx.x;
+        const int d = f < 2 ? 1 : (f < 4 ? D.tx : D.tx * D.ty);
+        const int T = f < 2 ? D.tx : (f < 4 ? D.ty : D.tz);
+        fdelta[f] = (f & 1) ? d : -d;
+        flim[f] = (f & 1) ? T - 1 : -1;
+    }
+    __syncthreads();
+    const uint32_t ntiles = *d_ntiles;
+    const float beta = (float)st->beta;
+    const bool flush = st->flush != 0;
+    const int g = threadIdx.x >> 7, u = threadIdx.x & 127;
+    const int row = u >> 1, half = u & 1;
+    const int cy = row & 7, cz = row >> 3, cx = 4 * half;
+    const uint32_t lo = (uint32_t)(cx + 8 * cy + 64 * cz);
+    const int bo = box_at(cx, cy, cz);
+    // halo cells u, u+128, u+256: face h/64, (e0, e1) = in-face position
+    uint32_t hA[3];  // face | slot-in-neighbour << 3 | box index << 12
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int h = u + 128 * k, f = h >> 6, e0 = h & 7, e1 = (h >> 3) & 7;
+        int hl = 0, bxi = 0;
+        switch (f) {
+        case 0: hl = 7 + 8 * e0 + 64 * e1; bxi = box_at(-1, e0, e1); break;
+        case 1: hl = 8 * e0 + 64 * e1; bxi = box_at(8, e0, e1); break;
+        case 2: hl = e0 + 56 + 64 * e1; bxi = box_at(e0, -1, e1); break;
+        case 3: hl = e0 + 64 * e1; bxi = box_at(e0, 8, e1); break;
+        case 4: hl = e0 + 8 * e1 + 448; bxi = box_at(e0, e1, -1); break;
+        default: hl = e0 + 8 * e1; bxi = box_at(e0, e1, 8); break;
+        }
+        hA[k] = (uint32_t)f | ((uint32_t)hl << 3) | ((uint32_t)bxi << 12);
+    }
+    const uint32_t stride = gridDim.x * kDm4Groups;
+    auto load = [&](Dm4Loads& L, uint32_t t) {
+        const uint32_t key = tiles[t];
+        const uint32_t tc = tcoord[t];
+        L.key = key;
+        const uint32_t s = (key << 9) | lo;
+        L.r = *reinterpret_cast<const float4*>(r + s);
+        L.p = *reinterpret_cast<const float4*>(p + s);
+        L.c = *reinterpret_cast<const uint32_t*>(cell + s);
+        L.hc = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int f = (int)(hA[k] & 7u);
+            const int cc = (int)((tc >> (10 * (f >> 1))) & 1023u);
+            const int lim = flim[f];
+            const bool ok = lim < 0 ? cc > 0 : cc < lim;
+            L.hr[k] = 0.0f;
+            L.hp[k] = 0.0f;
+            if (ok) {
+                const uint32_t sn = (((uint32_t)((int)key + fdelta[f])) << 9) | ((hA[k] >> 3) & 511u);
+                L.hr[k] = r[sn];
+                L.hp[k] = p[sn];
+                L.hc |= (uint32_t)cell[sn] << (8 * k);
+            }
+        }
+    };
+    double pq = 0.0;
+    Dm4Loads cur;
+    uint32_t t = (uint32_t)(blockIdx.x * kDm4Groups + g);
+    if (t < ntiles) load(cur, t);
+    for (int it = 0; t < ntiles; t += stride, ++it) {
+        float* Bx = dm4_box + (2 * g + (it & 1)) * kBoxFloats;
+        const uint32_t s = (cur.key << 9) | lo;
+        const float4 pc = dir4<kFlex>(tab, cur.c, cur.r, cur.p, beta);
+        *reinterpret_cast<float4*>(Bx + bo) = pc;
+        *reinterpret_cast<float4*>(pn + s) = pc;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const uint8_t hc = (uint8_t)(cur.hc >> (8 * k));
+            Bx[hA[k] >> 12] = kFlex ? dir_value_z(hc, cur.hr[k], cur.hp[k], beta)
+                                    : dir_value(tab, hc, cur.hr[k], cur.hp[k], beta);
+        }
+        if (flush && cur.c) {
+            const float* gv = xg + s;
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                if ((cur.c >> (8 * m)) & kCellFluid) {
+                    x[s + m] += (double)gv[m];
+                    xg[s + m] = 0.0f;
+                }
+        }
+        Dm4Loads nxt;
+        const uint32_t tn = t + stride;
+        if (tn < ntiles) load(nxt, tn);
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(128) : "memory");
+        const float left = Bx[bo - 1], right = Bx[bo + 4];
+        const float4 ym = *reinterpret_cast<const float4*>(Bx + bo - kBoxRow);
+        const float4 yp = *reinterpret_cast<const float4*>(Bx + bo + kBoxRow);
+        const float4 zm = *reinterpret_cast<const float4*>(Bx + bo - 10 * kBoxRow);
+        const float4 zp = *reinterpret_cast<const float4*>(Bx + bo + 10 * kBoxRow);
+        const float xl[4] = {left, pc.x, pc.y, pc.z}, xr[4] = {pc.y, pc.z, pc.w, right};
+        const float yl[4] = {ym.x, ym.y, ym.z, ym.w}, yr[4] = {yp.x, yp.y, yp.z, yp.w};
+        const float zl[4] = {zm.x, zm.y, zm.z, zm.w}, zr[4] = {zp.x, zp.y, zp.z, zp.w};
+        const float pv[4] = {pc.x, pc.y, pc.z, pc.w};
+        float qv[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const uint8_t c = (uint8_t)(cur.c >> (8 * m));
+            float qc = 0.0f;
+            if (c & kCellFluid) {
+                const float sum = ((xl[m] + xr[m]) + (yl[m] + yr[m])) + (zl[m] + zr[m]);
+                qc = fmaf((float)(c & 7u), pv[m], -sum);
+            }
+            qv[m] = qc;
+            pq += (double)pv[m] * (double)qc;
+        }
+        *reinterpret_cast<float4*>(q + s) = make_float4(qv[0], qv[1], qv[2], qv[3]);
+        cur = nxt;
+    }
+    double vals[1] = {pq}, out[1];
+    if (last_block_reduce<1>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->pq = out[0];
+        st->flush = 0;
+        if (out[0] > 0.0) st->alpha = st->rz / out[0];
+        else { st->alpha = 0.0; st->done = 3; }  // breakdown
+    }
+}
+
 // xg += alpha p, r -= alpha q, partial r.r and r.z; eight cells per thread
 // per round (two 16-byte quads per array, all loads issued before use)
 __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const float4& p4, const float4& q4, float4& r4,
@@ -963,9 +1134,19 @@ int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const N
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+// the matvec's 51 KB of shared boxes exceed the default 48 KB: raise the limit once per process
+static int dm4_prepare() {
+    static bool done = false;
+    if (done) return FLIP_OK;
+    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
+    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
+    done = true;
+    return FLIP_OK;
+}
 int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                                      cudaStream_t s) {
-    pcg_dirmatvec_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell, B.q, B.x,
+    if (int rc = dm4_prepare()) return rc;
+    pcg_dirmatvec4_kernel<true><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell, B.q, B.x,
                                                           B.xg, B.st, B.partials);
     pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
                                                                B.st, B.partials);
@@ -979,7 +1160,8 @@ int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuff
 }
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                              cudaStream_t s) {
-    pcg_dirmatvec_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
+    if (int rc = dm4_prepare()) return rc;
+    pcg_dirmatvec4_kernel<false><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
                                                     B.st, B.partials);
     pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
                                                                B.st, B.partials);
