@@ -540,74 +540,6 @@ __device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict
     }
 }
 
-template <bool kFlex>
-__global__ void __launch_bounds__(512, 4) pcg_dirmatvec_kernel(const uint32_t* __restrict__ tiles,
-                                                                const uint32_t* __restrict__ tcoord,
-                                                                const uint32_t* __restrict__ d_ntiles, NatDims D,
-                                                                const float* __restrict__ r, float* p0, float* p1,
-                                                                const uint8_t* __restrict__ cell, float* __restrict__ q,
-                                                                double* __restrict__ x, float* __restrict__ xg,
-                                                                PcgState* st, double* partials) {
-    if (st->done || st->pending) return;
-    const float* __restrict__ p = st->pcur ? p1 : p0;
-    float* __restrict__ pn = st->pcur ? p0 : p1;
-    // 10^3 box: tile + halo, index (x+1) + 10 (y+1) + 100 (z+1); two of them,
-    // alternating per tile, so one barrier per tile suffices: a thread writes
-    // a box again only after the next tile's barrier, which every thread
-    // reaches after its reads of this box
-    __shared__ float Pbox[2][1000];
-    __shared__ double sh[32];
-    __shared__ float tab[8];
-    if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
-    __syncthreads();
-    const uint32_t ntiles = *d_ntiles;
-    const float beta = (float)st->beta;
-    const bool flush = st->flush != 0;
-    const int tid = threadIdx.x;
-    const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
-    const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
-    // halo cell handled by this thread (384 of them: 6 faces x 64)
-    const HaloSlot H = halo_slot(tid, D);
-    const int face = H.face;
-    const int bh = (H.hx + 1) + 10 * ((H.hy + 1) + 10 * (H.hz + 1));
-    double pq = 0.0;
-    DirLoads cur;
-    uint32_t t = blockIdx.x;
-    if (t < ntiles) dir_load(cur, tiles, tcoord, t, H, r, p, cell);
-    for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
-        float* P = Pbox[it & 1];
-        const uint32_t s = (cur.key << 9) | tid;
-        const uint8_t c = cur.c;
-        const float pc = kFlex ? dir_value_z(c, cur.r, cur.p, beta) : dir_value(tab, c, cur.r, cur.p, beta);
-        P[bc] = pc;
-        pn[s] = pc;
-        if (face < 6) P[bh] = kFlex ? dir_value_z(cur.hc, cur.hr, cur.hp, beta) : dir_value(tab, cur.hc, cur.hr, cur.hp, beta);
-        if (flush && (c & kCellFluid)) {
-            x[s] += (double)xg[s];
-            xg[s] = 0.0f;
-        }
-        DirLoads nxt;
-        const uint32_t tn = t + gridDim.x;
-        if (tn < ntiles) dir_load(nxt, tiles, tcoord, tn, H, r, p, cell);
-        __syncthreads();
-        float qc = 0.0f;
-        if (c & kCellFluid) {
-            const float sum = ((P[bc - 1] + P[bc + 1]) + (P[bc - 10] + P[bc + 10])) + (P[bc - 100] + P[bc + 100]);
-            qc = fmaf((float)(c & 7u), pc, -sum);
-        }
-        q[s] = qc;
-        pq += (double)pc * (double)qc;
-        cur = nxt;
-    }
-    double vals[1] = {pq}, out[1];
-    if (last_block_reduce<1>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
-        st->pq = out[0];
-        st->flush = 0;
-        if (out[0] > 0.0) st->alpha = st->rz / out[0];
-        else { st->alpha = 0.0; st->done = 3; }  // breakdown
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Vectorised direction update + matvec.  A CTA of 512 threads runs four
 // independent groups of 128; each group walks its own tiles and syncs on its
