@@ -459,14 +459,7 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     }
 }
 
-// fused direction update + matvec, one 8^3 tile at a time: p' = D^-1 r +
-// beta p is computed for the tile and its one-cell halo into shared memory
-// (the halo cells belong to neighbouring tiles, which compute the same values
-// for themselves), then q = A p' is read from shared memory.  p' goes to the
-// other p buffer because neighbouring tiles still read p.  The loads of the
-// next tile (centre and halo, all independent) are issued before the current
-// tile's stencil, so their latency overlaps it.  After a true-residual check
-// this kernel also folds xg into x (no neighbour reads of x happen here).
+// p' of one cell: D^-1 r + beta p (Jacobi PCG) on fluid cells, 0 elsewhere
 __device__ __forceinline__ float dir_value(const float* tab, uint8_t c, float r, float p, float beta) {
     return (c & kCellFluid) ? fmaf(beta, p, r * jacobi_inv_s(tab, c)) : 0.0f;
 }
@@ -474,12 +467,6 @@ __device__ __forceinline__ float dir_value(const float* tab, uint8_t c, float r,
 __device__ __forceinline__ float dir_value_z(uint8_t c, float z, float p, float beta) {
     return (c & kCellFluid) ? fmaf(beta, p, z) : 0.0f;
 }
-
-struct DirLoads {
-    uint32_t key;
-    float r, p, hr, hp;
-    uint8_t c, hc;
-};
 
 // The halo cell a thread loads, as constants of the thread: face f = tid/64
 // (0..5: -x, +x, -y, +y, -z, +z; 6, 7: none), the neighbour tile's key
@@ -518,30 +505,14 @@ __device__ __forceinline__ int64_t halo_at(const HaloSlot& h, uint32_t key, uint
     return (int64_t)((((uint32_t)((int)key + h.delta)) << 9) | h.hl);
 }
 
-__device__ __forceinline__ void dir_load(DirLoads& L, const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ tcoord,
-                                         uint32_t t, const HaloSlot& H, const float* __restrict__ r,
-                                         const float* __restrict__ p, const uint8_t* __restrict__ cell) {
-    const uint32_t key = tiles[t];
-    L.key = key;
-    const uint32_t s = (key << 9) | threadIdx.x;
-    L.c = cell[s];
-    L.r = r[s];
-    L.p = p[s];
-    L.hc = 0;
-    L.hr = 0.0f;
-    L.hp = 0.0f;
-    if (H.face < 6) {
-        const int64_t sn = halo_at(H, key, tcoord[t]);
-        if (sn >= 0) {
-            L.hc = cell[sn];
-            L.hr = r[sn];
-            L.hp = p[sn];
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
-// Vectorised direction update + matvec.  A CTA of 512 threads runs four
+// Fused direction update + matvec: p' = D^-1 r + beta p (or z + beta p for
+// flexible CG) for a tile and its one-cell halo into shared memory (the halo
+// cells belong to neighbouring tiles, which compute the same values for
+// themselves), then q = A p' from shared memory, and p'.q.  p' goes to the
+// other p buffer because neighbouring tiles still read p.  After a
+// true-residual check this kernel also folds xg into x.
+// Vectorised: a CTA of 512 threads runs four
 // independent groups of 128; each group walks its own tiles and syncs on its
 // own named barrier.  A thread owns four consecutive x-cells of one (y, z) row
 // (float4 loads and stores) and three of the tile's 384 halo cells.  The
