@@ -703,11 +703,13 @@ __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const fl
     }
 }
 
-// One warp per tile: the warp's 32 lanes hold the tile's 128 quads, four
-// each, and issue all 20 loads of a tile before using any of them; the next
-// tile's key is loaded one tile ahead.
+// A warp takes a unit of kUpdQuads x 32 quads (half a tile): each lane
+// issues all 5 x kUpdQuads loads of its quads before using any of them, and
+// the next unit's tile key is loaded one unit ahead.
 constexpr int kUpdThreads = 256;
-__global__ void __launch_bounds__(kUpdThreads, 2) pcg_update_kernel(const uint32_t* __restrict__ tiles,
+constexpr int kUpdQuads = 2;                    // quads per lane and unit
+constexpr int kUpdUnits = 128 / (32 * kUpdQuads);  // units per tile
+__global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32_t* __restrict__ tiles,
                                                                      const uint32_t* __restrict__ d_ntiles, NatDims D,
                                                                      float* __restrict__ xg, float* __restrict__ r,
                                                                      const float* p0, const float* p1,
@@ -720,21 +722,22 @@ __global__ void __launch_bounds__(kUpdThreads, 2) pcg_update_kernel(const uint32
     __shared__ float tab[8];
     if (threadIdx.x < 8) tab[threadIdx.x] = kJacobiInv[threadIdx.x];
     __syncthreads();
-    const uint32_t ntiles = *d_ntiles;
+    const uint32_t nunits = *d_ntiles * kUpdUnits;
     const float a = (float)st->alpha;
     const int lane = threadIdx.x & 31;
     const uint32_t nwarps = gridDim.x * (kUpdThreads / 32);
-    uint32_t t = blockIdx.x * (kUpdThreads / 32) + (threadIdx.x >> 5);
+    uint32_t w = blockIdx.x * (kUpdThreads / 32) + (threadIdx.x >> 5);
     double rr = 0.0, rz = 0.0;
-    uint32_t key = t < ntiles ? tiles[t] : 0u;
-    for (; t < ntiles; t += nwarps) {
-        const uint32_t tn = t + nwarps;
-        const uint32_t key_next = tn < ntiles ? tiles[tn] : 0u;
-        uint32_t c[4];
-        float4 pv[4], qv[4], rv[4], gv[4];
+    uint32_t key = w < nunits ? tiles[w / kUpdUnits] : 0u;
+    for (; w < nunits; w += nwarps) {
+        const uint32_t wn = w + nwarps;
+        const uint32_t key_next = wn < nunits ? tiles[wn / kUpdUnits] : 0u;
+        const uint32_t qbase = (w % kUpdUnits) * (32 * kUpdQuads) + lane;
+        uint32_t c[kUpdQuads];
+        float4 pv[kUpdQuads], qv[kUpdQuads], rv[kUpdQuads], gv[kUpdQuads];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const uint32_t s = (key << 9) | (uint32_t)((lane + 32 * m) << 2);
+        for (int m = 0; m < kUpdQuads; ++m) {
+            const uint32_t s = (key << 9) | ((qbase + 32 * m) << 2);
             c[m] = *reinterpret_cast<const uint32_t*>(cell + s);
             pv[m] = *reinterpret_cast<const float4*>(p + s);
             qv[m] = *reinterpret_cast<const float4*>(q + s);
@@ -742,9 +745,9 @@ __global__ void __launch_bounds__(kUpdThreads, 2) pcg_update_kernel(const uint32
             gv[m] = *reinterpret_cast<const float4*>(xg + s);
         }
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
+        for (int m = 0; m < kUpdQuads; ++m) {
             if (!c[m]) continue;
-            const uint32_t s = (key << 9) | (uint32_t)((lane + 32 * m) << 2);
+            const uint32_t s = (key << 9) | ((qbase + 32 * m) << 2);
             upd_quad(tab, c[m], pv[m], qv[m], rv[m], gv[m], a, rr, rz);
             *reinterpret_cast<float4*>(r + s) = rv[m];
             *reinterpret_cast<float4*>(xg + s) = gv[m];

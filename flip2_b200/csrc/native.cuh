@@ -30,7 +30,7 @@ struct PcgState {
 };
 
 constexpr int kPcgBlocks = 592;        // 148 SMs x 4 CTAs of 512 threads
-constexpr int kPcgUpdateBlocks = 296;  // 148 SMs x 2 CTAs of 256 threads (one warp per tile, 20 loads in flight a lane)
+constexpr int kPcgUpdateBlocks = 592;  // 148 SMs x 4 CTAs of 256 threads (a warp per half tile, 10 loads in flight a lane)
 
 // PCG vectors on the tile-blocked slots.  The solution is x + xg: x in FP64
 // holds everything up to the last true-residual check, xg (FP32) the
