@@ -56,7 +56,7 @@ class Params(C.Structure):
                 ("pcg_max_iter", C.c_int32), ("pcg_check_every", C.c_int32), ("true_residual_every", C.c_int32),
                 ("permute_velocities", C.c_int32), ("device", C.c_int32), ("pressure_method", C.c_int32),
                 ("max_substep_dt", C.c_double), ("learned_max_iter", C.c_int32), ("lp_cuda_cores", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("pcg_warm_start", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class PoissonSpec(C.Structure):

@@ -68,6 +68,8 @@ struct flip_engine {
     bool has_solid = false;
     uint32_t* grid_tiles = nullptr;
     PcgBuffers pcg{};
+    uint8_t* cell_prev = nullptr;  // cell codes of the previous step's solve (warm start)
+    bool warm_ok = false;          // pcg.x holds the previous step's converged pressure
     PcgState* h_state = nullptr;
     cudaGraphExec_t pcg_graph = nullptr;
     int pcg_graph_iters = 0;
@@ -146,6 +148,7 @@ extern "C" void flip_default_params(int mode, flip_params* out) {
     out->max_substep_dt = 1.0 / 240.0;
     out->pressure_method = 0;
     out->learned_max_iter = 100;
+    out->pcg_warm_start = 1;
 }
 
 extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, flip_engine** out) {
@@ -232,6 +235,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
     E_CUDA(cudaStreamSynchronize(e->stream));
     free_arena(e);
     free_ref_voxels(e);
+    e->warm_ok = false;
     e->grid.negX = (float)nx; e->grid.negY = (float)ny; e->grid.negZ = (float)nz;  // Grid narrows to float (grid.hpp:118-129)
     e->grid.sizeX = x; e->grid.sizeY = y; e->grid.sizeZ = z;
     e->grid.cellSize = (float)cellSize;
@@ -289,6 +293,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         for (float** q : pv) add((void**)q, 4 * e->nslots);
         add((void**)&e->pcg.x, 8 * e->nslots);
         add((void**)&e->pcg.cell, e->nslots);
+        add((void**)&e->cell_prev, e->nslots);
         add((void**)&e->pcg.tcoord, 4 * e->ntiles_total);
         add((void**)&e->pcg.st, sizeof(PcgState));
         add((void**)&e->pcg.partials, sizeof(double) * 4 * kPcgBlocks);
@@ -630,6 +635,10 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
         E_CUDA(cudaMemsetAsync(e->w[c], 0, fb, e->stream));
     }
     E_CUDA(cudaMemsetAsync(e->type, 0, e->nslots, e->stream));
+    // keep the last solve's cell codes for the warm start (a copy: the PCG
+    // graphs hold the pcg.cell pointer)
+    if (e->P.pcg_warm_start && e->warm_ok)
+        E_CUDA(cudaMemcpyAsync(e->cell_prev, e->pcg.cell, e->nslots, cudaMemcpyDeviceToDevice, e->stream));
     E_CUDA(cudaMemsetAsync(e->pcg.cell, 0, e->nslots, e->stream));
     E_CUDA(cudaMemsetAsync(e->tile_flags, 0, e->ntiles_total, e->stream));
     E_TRY(e->mark(5));
@@ -794,7 +803,7 @@ static int run_chunks(flip_engine* e, cudaGraphExec_t g, int chunk, uint32_t lau
 // if it stops without meeting tol (iteration cap or a non-positive r.z),
 // restarts Jacobi-PCG from x = 0.
 static int nat_solve(flip_engine* e, const float* const* U, int method, double tol, int max_plain, int max_learned,
-                     flip_solve_info* out) {
+                     flip_solve_info* out, bool warm = false) {
     flip_solve_info info{};
     const int chunk = e->P.pcg_check_every;
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
@@ -825,8 +834,10 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
     if (need_plain) {
         pcg_state_host(e, tol, max_plain, 0);
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
-        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
-        e->launches += 1;
+        const bool w = warm && method != 1;
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
+                                  w ? e->cell_prev : nullptr));
+        e->launches += w ? 2 : 1;
         if (method != 1) E_TRY(e->mark(9));
         E_TRY(nat_pcg_graph(e, chunk));
         E_TRY(run_chunks(e, e->pcg_graph, chunk, 2u * (uint32_t)chunk + 1u, max_plain));
@@ -856,8 +867,10 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
 
 static int nat_pressure(flip_engine* e) {
     const int learned = e->P.learned_max_iter > 0 ? e->P.learned_max_iter : e->P.pcg_max_iter;
+    const bool warm = e->P.pcg_warm_start && e->warm_ok;
     E_TRY(nat_solve(e, (const float* const*)e->m, e->P.pressure_method, e->P.pcg_tol, e->P.pcg_max_iter, learned,
-                    e->timing ? &e->last_solve : nullptr));
+                    e->timing ? &e->last_solve : nullptr, warm));
+    e->warm_ok = e->last_converged != 0;
     e->poisson_ready = true;  // b, the cell types and the tile lists of this solve stay in place
     e->xstar_ready = false;
     return FLIP_OK;
@@ -1219,6 +1232,7 @@ extern "C" int flip_lp_get_grad(flip_engine* e, float* g, uint64_t n) {
 
 // fluid tiles -> node_keys, their dilation -> tile_flags / grid_tiles, cell codes cleared
 static int poisson_tiles(flip_engine* e) {
+    e->warm_ok = false;
     E_CUDA(cudaMemsetAsync(e->pcg.cell, 0, e->nslots, e->stream));
     E_TRY(nat_launch_fluid_tiles(e->type, e->tile_flags, (uint32_t)e->ntiles_total, e->node_keys, e->d_counts, e->nslots,
                                  e->stream));
@@ -1296,6 +1310,7 @@ extern "C" int flip_poisson_solve(flip_engine* e, int method, double tol, int ma
     if ((method != 0 && method != 1) || !(tol > 0.0) || max_iter <= 0)
         return e->fail(FLIP_ERR_ARG, "flip_poisson_solve: method 0/1, tol > 0, max_iter > 0");
     flip_solve_info local{};
+    e->warm_ok = false;  // pcg.x will hold this problem's solution
     const int plain = method == 1 ? e->P.pcg_max_iter : max_iter;
     E_TRY(nat_solve(e, nullptr, method, tol, plain, max_iter, &local));
     if (info) *info = local;
@@ -1389,6 +1404,7 @@ extern "C" int flip_lp_train_step(flip_engine* e, int sample, float lr, double* 
         e->launches += 4;
     }
     e->solution_fresh = false;  // pcg.x now holds x_k
+    e->warm_ok = false;
     E_TRY(lp_loss_backward(e, inv_s, true, lr, true));
     E_TRY(lp_read_loss(e, loss));
     return lp_check_err(e);
@@ -1405,6 +1421,7 @@ extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, const float* e_l
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
     E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));  // cell codes, n_fluid
     e->solution_fresh = false;
+    e->warm_ok = false;
     E_CUDA(cudaMemcpyAsync(e->pcg.p0, r_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
     E_TRY(nat_launch_lin_tiles_f32(e->pcg.p0, e->pcg.r, e->D, 1, e->stream));
     E_CUDA(cudaMemcpyAsync(e->pcg.p0, e_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));

@@ -399,10 +399,13 @@ __device__ __forceinline__ float jacobi_inv_s(const float* tab, uint8_t c) { ret
 
 // divergence -> b = -div; cell codes; x = 0, r = b, p = 0 (the first
 // direction update turns p into D^-1 r)
+// cell_prev (warm start): the previous solve's cell codes; x starts from the
+// previous solution (x + xg) on cells that are fluid in both solves, 0
+// elsewhere, and pcg_warm_kernel then replaces r = b by b - A x
 __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
-                                                        PcgBuffers B) {
+                                                        const uint8_t* __restrict__ cell_prev, PcgBuffers B) {
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
     double bb = 0.0, rz = 0.0, nf = 0.0;
@@ -431,7 +434,9 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     }
     B.cell[s] = code;
     B.b[s] = b;
-    B.x[s] = 0.0;
+    double x0 = 0.0;
+    if (cell_prev && (code & kCellFluid) && (cell_prev[s] & kCellFluid)) x0 = B.x[s] + (double)B.xg[s];
+    B.x[s] = x0;
     B.xg[s] = 0.0f;
     B.r[s] = b;
     B.p0[s] = 0.0f;
@@ -839,6 +844,65 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
     }
 }
 
+// warm start: r = b - A x in FP64 for the initial guess, r.r and r.z, and
+// the state for the first iteration (converged already if |r| <= tol |b|;
+// b = 0 gives x = 0)
+__global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __restrict__ tiles,
+                                                           const uint32_t* __restrict__ tcoord,
+                                                           const uint32_t* __restrict__ d_ntiles, NatDims D,
+                                                           double* __restrict__ x, const float* __restrict__ bv,
+                                                           float* __restrict__ r, const uint8_t* __restrict__ cell,
+                                                           PcgState* st, double* partials) {
+    __shared__ double X[1000];
+    __shared__ double sh[32];
+    const uint32_t ntiles = *d_ntiles;
+    const bool zero = !(st->bb > 0.0);
+    const int tid = threadIdx.x;
+    const int li = tid & 7, lj = (tid >> 3) & 7, lk = tid >> 6;
+    const int bc = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
+    const HaloSlot H = halo_slot(tid, D);
+    const int bh = (H.hx + 1) + 10 * ((H.hy + 1) + 10 * (H.hz + 1));
+    double rr = 0.0, rz = 0.0;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t key = tiles[t];
+        const uint32_t s = (key << 9) | tid;
+        const uint8_t c = cell[s];
+        double xs = (c & kCellFluid) ? x[s] : 0.0;
+        if (zero && xs != 0.0) {
+            x[s] = 0.0;
+            xs = 0.0;
+        }
+        X[bc] = xs;
+        if (H.face < 6) {
+            const int64_t sn = halo_at(H, key, tcoord[t]);
+            double v = 0.0;
+            if (!zero && sn >= 0 && (cell[sn] & kCellFluid)) v = x[sn];
+            X[bh] = v;
+        }
+        __syncthreads();
+        if (c & kCellFluid) {
+            const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
+            const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
+            const float rs = (float)res;
+            r[s] = rs;
+            rr += res * res;
+            rz += (double)rs * (double)(rs * jacobi_inv(c));
+        }
+        __syncthreads();
+    }
+    double vals[2] = {rr, rz}, out[2];
+    if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
+        st->rr = out[0];
+        st->rr_true = out[0];
+        st->rz = out[1];
+        st->rz_prev = out[1];
+        st->beta = 0.0;
+        st->inv_s = out[0] > 0.0 ? (float)(1.0 / sqrt(out[0] / fmax(st->nfluid, 1.0))) : 1.0f;
+        st->done = (zero || out[0] <= st->tol2 * st->bb) ? 1 : 0;
+        st->halt = st->done;
+    }
+}
+
 // flexible CG (Notay's FCG(1), the same recurrence as Polak-Ribiere PCG)
 // with the preconditioner M(r) = N(r) + D^-1 r.  This kernel adds the Jacobi
 // term to the network output z in place.  The new direction p' = z + beta p
@@ -1035,8 +1099,10 @@ int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const N
     return FLIP_OK;
 }
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
-                        const uint8_t* type, PcgBuffers& B, cudaStream_t s) {
-    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, B);
+                        const uint8_t* type, PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
+    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
+    if (cell_prev)
+        pcg_warm_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -73,9 +73,11 @@ int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots
 int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s);
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
                          const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s);
-// U == nullptr: the right-hand side is already in B.b (standalone Poisson problems)
+// U == nullptr: the right-hand side is already in B.b (standalone Poisson problems).
+// cell_prev != nullptr: warm start from the previous solution (x + xg) on the
+// cells that were fluid in the previous solve (cell_prev: its cell codes)
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
-                        const uint8_t* type, PcgBuffers& B, cudaStream_t s);
+                        const uint8_t* type, PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev = nullptr);
 // flexible PCG: direction from z (B.z), and the r.z / z.q reduction giving beta
 int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                                      cudaStream_t s);

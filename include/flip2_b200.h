@@ -166,7 +166,10 @@ typedef struct {
     int32_t learned_max_iter;    /* NATIVE: FPCG cap before the Jacobi-PCG restart   */
     int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers on CUDA
                                     cores instead of tcgen05 (for comparison)         */
-    int32_t reserved[2];
+    int32_t pcg_warm_start;      /* NATIVE: 1 (default) starts each step's Jacobi-PCG
+                                    from the previous step's pressure on the cells
+                                    fluid in both; the stop test stays |r| <= tol |b| */
+    int32_t reserved[1];
 } flip_params;
 
 /* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */

@@ -83,6 +83,32 @@ def test_native_twenty_steps(torch):
     P.close()
 
 
+def test_native_warm_start(torch):
+    # twenty steps from the previous step's pressure and twenty from zero:
+    # every solve meets 1e-6 either way, the warm runs take fewer iterations,
+    # and the particles end up where the cold run puts them
+    nc, dt = 32, 1.0 / 240
+    pos, vel = scenes.dam_break(nc, seed=0)
+    out = {}
+    for warm in (0, 1):
+        P = native(pos.shape[0], nc, pcg_warm_start=warm)
+        P.upload(pos, vel)
+        iters = 0
+        for _ in range(20):
+            P.step(dt)
+            info = P.info()
+            assert info.converged == 1 and info.residual <= 1e-6
+            iters += info.pressure_iters
+        out[warm] = (iters, P.download())
+        P.close()
+    (ic, (pc, _)), (iw, (pw, _)) = out[0], out[1]
+    assert iw < ic
+    # the particle order differs between the runs (each step re-sorts), so
+    # compare each coordinate's sorted values: the two fluids agree to 5% of a cell
+    for k in range(3):
+        assert np.max(np.abs(np.sort(pc[:, k]) - np.sort(pw[:, k]))) < 0.05 / nc
+
+
 def test_native_solid_sphere(torch):
     """Interior solid cells (the learned-preconditioner problems carry solid
     spheres): faces touching solid cells stay zero, the solve converges, and
