@@ -125,6 +125,7 @@ def lib():
         "flip_solve_frame": (i32, [vp, d]),
         "flip_get_courant_dt": (d, [vp]),
         "flip_write_positions_csv": (i32, [vp, C.c_char_p]),
+        "flip_write_positions_bin": (i32, [vp, C.c_char_p]),
         "flip_step": (i32, [vp, d]),
         "flip_sync": (i32, [vp]),
         "flip_get_buffer": (i32, [vp, i32, C.POINTER(vp), C.POINTER(u64), C.POINTER(u32)]),
@@ -381,6 +382,9 @@ class Particles:
     def writePositionsToFile(self, fileName):
         self._call("flip_write_positions_csv", str(fileName).encode())
 
+    def write_positions_bin(self, fileName):
+        self._call("flip_write_positions_bin", str(fileName).encode())
+
     # extensions
     def step(self, dt):
         self._call("flip_step", dt)
@@ -517,3 +521,16 @@ class Particles:
         i = Info()
         self._call("flip_get_info", C.byref(i))
         return i
+
+
+def read_positions_bin(path):
+    """(n, 3) float32 positions of a frame written by flip_write_positions_bin."""
+    with open(path, "rb") as f:
+        head = f.read(16)
+        if len(head) != 16 or head[:8] != b"FLIP2POS":
+            raise ValueError("%s: not a FLIP2POS frame" % path)
+        n = int(np.frombuffer(head[8:], np.uint64)[0])
+        data = np.frombuffer(f.read(12 * n), np.float32)
+    if data.size != 3 * n:
+        raise ValueError("%s: truncated frame" % path)
+    return data.reshape(n, 3)

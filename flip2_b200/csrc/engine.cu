@@ -1054,6 +1054,29 @@ extern "C" int flip_write_positions_csv(flip_engine* e, const char* path) {
     return FLIP_OK;
 }
 
+// binary frame: 16-byte header {"FLIP2POS", uint32 count low, uint32 count
+// high} then count x 3 float32 (x, y, z interleaved), little endian
+extern "C" int flip_write_positions_bin(flip_engine* e, const char* path) {
+    if (!e || !path) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain");
+    std::vector<float> x(e->n), y(e->n), z(e->n), xyz(3 * e->n);
+    E_TRY(flip_download_particles_f32(e, x.data(), y.data(), z.data(), nullptr, nullptr, nullptr, e->n));
+    for (uint64_t i = 0; i < e->n; ++i) {
+        xyz[3 * i] = x[i];
+        xyz[3 * i + 1] = y[i];
+        xyz[3 * i + 2] = z[i];
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return e->fail(FLIP_ERR_ARG, std::string("cannot open ") + path);
+    const char magic[8] = {'F', 'L', 'I', 'P', '2', 'P', 'O', 'S'};
+    const uint32_t cnt[2] = {(uint32_t)(e->n & 0xFFFFFFFFu), (uint32_t)(e->n >> 32)};
+    bool ok = fwrite(magic, 1, 8, f) == 8 && fwrite(cnt, 4, 2, f) == 2 &&
+              fwrite(xyz.data(), sizeof(float), xyz.size(), f) == xyz.size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return e->fail(FLIP_ERR_ARG, std::string("cannot write ") + path);
+    return FLIP_OK;
+}
+
 extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, uint32_t* elem_size) {
     if (!e || !dev_ptr || !count || !elem_size) return FLIP_ERR_ARG;
     const bool ref = e->P.mode == FLIP_MODE_REFERENCE;

@@ -163,6 +163,9 @@ public:
     void initialize() { check(flip_initialize(e), "initialize", e); }
     void voxelVelsToParticles() { check(flip_voxel_vels_to_particles(e), "voxelVelsToParticles", e); }
     void moveSolidParticles() { check(flip_move_solid_particles(e), "moveSolidParticles", e); }
+    void writePositionsToBinaryFile(const std::string& fileName) {
+        check(flip_write_positions_bin(e, fileName.c_str()), "writePositionsToBinaryFile", e);
+    }
     void writePositionsToFile(const std::string& fileName) {
         check(flip_write_positions_csv(e, fileName.c_str()), "writePositionsToFile", e);
     }

@@ -210,6 +210,11 @@ int flip_solve_frame(flip_engine* e, double fps);   /* solveFrame, particles.cu:
 double flip_get_courant_dt(flip_engine* e);         /* getCourantDt, particles.cu:493-498          */
 /* writePositionsToFile (particles.cu:817-828): "x, y, z" per line. */
 int flip_write_positions_csv(flip_engine* e, const char* path);
+/* Binary variant of the same frame (no reference counterpart): a 16-byte
+ * header "FLIP2POS" + uint64 count (little endian), then count x 3 float32
+ * (x, y, z interleaved).  FP32 positions at 12 B a particle instead of about
+ * 30 B of text. */
+int flip_write_positions_bin(flip_engine* e, const char* path);
 
 /* One fixed-dt step of the whole path (bin, P2G, pressure, projection,
  * G2P + advection), asynchronous on the engine stream except for the

@@ -148,3 +148,23 @@ def test_native_engine_errors(torch):
         P.setDomain(0, 0, 0, 3, 4, 4, 0.25)  # 12 voxels: not a multiple of 8
     assert ei.value.status == 1
     P.close()
+
+
+def test_position_frames(torch, tmp_path):
+    # writePositionsToFile's "x, y, z" text (particles.cu:817-828, read by
+    # visualizeSavedPoints.py) and the binary variant hold the same frame
+    nc = 16
+    pos, vel = scenes.dam_break(nc, seed=1)
+    P = native(pos.shape[0], nc)
+    P.upload(pos, vel)
+    P.step(1.0 / 240)
+    pg, _ = P.download()
+    P.writePositionsToFile(tmp_path / "frame.csv")
+    P.write_positions_bin(tmp_path / "frame.bin")
+    P.close()
+    txt = np.loadtxt(tmp_path / "frame.csv", delimiter=",")
+    binf = F.read_positions_bin(tmp_path / "frame.bin")
+    assert binf.shape == pg.shape and np.array_equal(binf, pg)
+    assert txt.shape == pg.shape and np.max(np.abs(txt - pg)) <= 5e-6 * np.max(np.abs(pg))
+    with open(tmp_path / "frame.bin", "rb") as f:
+        assert f.read(8) == b"FLIP2POS"

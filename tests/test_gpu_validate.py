@@ -1,0 +1,103 @@
+"""Each benchmark configuration against an FP64 oracle run of the same input:
+pressure, velocity and particle-position errors of one native step (C1 at
+32^3; C2 and C5 at 256^3), and the learned and plain pressure solves of a
+C4 problem at 128^3 against an FP64 CG solution.  The errors are printed
+(pytest -s) as one JSON line per configuration and checked against the
+tolerances of the parity tests.
+
+The 256^3 cases run the FP64 oracle on the host for a few minutes, so they
+run only with FLIP2_VALIDATE_FULL=1."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import flip2_b200 as F
+from flip2_b200 import scenes
+from oracle import oracle as O
+from tests.util import rel_err, tiled_to_linear
+
+pytestmark = pytest.mark.gpu
+FULL = os.environ.get("FLIP2_VALIDATE_FULL") == "1"
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as T
+    assert T.cuda.is_available()
+    F.lib()
+    return T
+
+
+def step_errors(name, nc, block, dt, sphere=None, learned=False):
+    pos, vel = scenes.dam_break(nc, block=block, seed=0, sphere=sphere)
+    params = F.default_params(F.MODE_NATIVE, pressure_method=1 if learned else 0)
+    P = F.Particles(pos.shape[0], mode=F.MODE_NATIVE, params=params)
+    P.setDomain(0.0, 0.0, 0.0, nc // 4, nc // 4, nc // 4, 4.0 / nc)
+    if learned:
+        P.lp_set_weights(np.load(os.path.join(os.path.dirname(F.__file__), "data", "lprec_weights.npy")))
+    P.upload(pos, vel)
+    P.step(dt)
+    info = P.info()
+    perm = P.read(F.BUF_PERM)
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE), nc, nc, nc).astype(np.float64)
+    pg, vg = P.download()
+    P.close()
+    ref = O.nat_step(pos, vel, O.nat_params(nc, nc, nc, 1.0 / nc, dt=dt))
+    po, vo = ref["pos"][perm], ref["vel"][perm]
+    h = 1.0 / nc
+    fl = np.abs(ref["phi"]) > 0
+    out = {"config": name, "grid": "%d^3" % nc, "particles": int(pos.shape[0]),
+           "pressure_rel_err_max": rel_err(phi, ref["phi"]),
+           "pressure_rel_err_l2": float(np.linalg.norm(phi[fl] - ref["phi"][fl]) / np.linalg.norm(ref["phi"][fl])),
+           "velocity_rel_err_max": rel_err(vg, vo, floor=1.0),
+           "position_err_max_in_h": float(np.max(np.abs(pg - po)) / h),
+           "iters_gpu": int(info.pressure_iters), "iters_fp64": int(ref["iters"]),
+           "rel_residual_gpu": float(info.residual)}
+    print(json.dumps(out))
+    assert info.converged == 1 and info.residual <= 1e-6
+    assert out["pressure_rel_err_max"] < 2e-3
+    assert out["velocity_rel_err_max"] < 2e-3
+    assert out["position_err_max_in_h"] < 1e-3
+    return out
+
+
+def test_c1_errors(torch):
+    step_errors("C1", 32, (0.4, 0.6, 1.0), 1.0 / 240)
+
+
+@pytest.mark.skipif(not FULL, reason="FP64 oracle at 256^3 takes minutes (FLIP2_VALIDATE_FULL=1)")
+def test_c2_errors(torch):
+    step_errors("C2", 256, (0.5, 0.5, 1.0), 1.0 / 480)
+
+
+@pytest.mark.skipif(not FULL, reason="FP64 oracle at 256^3 takes minutes (FLIP2_VALIDATE_FULL=1)")
+def test_c5_errors(torch):
+    step_errors("C5", 256, (0.5, 0.5, 1.0), 1.0 / 480, sphere=(0.5, 0.75, 0.5, 0.15), learned=True)
+
+
+def test_c4_errors(torch):
+    # one C4 problem: both solves against the FP64 CG solution of the same system
+    nc = 128 if FULL else 64
+    P = F.Particles(1, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE))
+    P.setDomain(0.0, 0.0, 0.0, nc // 4, nc // 4, nc // 4, 1.0)
+    P.lp_set_weights(np.load(os.path.join(os.path.dirname(F.__file__), "data", "lprec_weights.npy")))
+    P.poisson_generate(seed=900_000)
+    typ = tiled_to_linear(P.read(F.BUF_CELL_TYPE, np.uint8), nc, nc, nc)
+    b = tiled_to_linear(P.read(F.BUF_DIVU, np.float32), nc, nc, nc).astype(np.float64)
+    res = {}
+    for method in (0, 1):
+        i = P.poisson_solve(method, 1e-6, 20000 if method == 0 else 100)
+        res[method] = (i, P.poisson_solution())
+    P.close()
+    xo, it, rr = O.nat_pcg(typ, b, O.nat_params(nc, nc, nc, 1.0, tol=1e-10, max_iter=100000))
+    out = {"config": "C4", "grid": "%d^3" % nc, "fp64_cg_iters_to_1e-10": int(it)}
+    for method, tag in ((0, "plain"), (1, "learned")):
+        i, x = res[method]
+        out[tag + "_rel_err_vs_fp64_cg"] = rel_err(x, xo)
+        out[tag + "_rel_residual"] = float(i.rel_residual)
+        out[tag + "_fell_back"] = int(i.fell_back)
+        assert i.converged == 1 and i.rel_residual <= 1e-6
+        assert rel_err(x, xo) < 2e-3
+    print(json.dumps(out))
