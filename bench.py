@@ -210,6 +210,45 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------ replicas and ranks
+class Ranks:
+    """One process per GPU under torchrun: the replicas share nothing but a
+    barrier around the timed region and the maximum of the ranks' times.
+    backend "nccl" on GPUs, "gloo" for the host-only tests."""
+
+    def __init__(self, backend="nccl", device=None, timeout_s=120):
+        import datetime
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            kw = {"timeout": datetime.timedelta(seconds=timeout_s)}
+            if backend == "nccl":
+                kw["device_id"] = device
+            dist.init_process_group(backend, **kw)
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ------------------------------------------------------------ own arm
 def main():
     args = parse_args()
@@ -221,15 +260,9 @@ def main():
         return
     import torch
     import flip2_b200 as F
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    ranks = Ranks("nccl", dev)
 
     pos, vel = scene(args.cells, args.config)
     n = pos.shape[0]
@@ -248,16 +281,7 @@ def main():
     P.upload_ptrs(ptrs)
     del pos, vel
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     for _ in range(max(3, args.warmup)):
         P.step(DT)
@@ -370,8 +394,7 @@ def main():
             line["fallback_rate"] = fell_back / args.steps
         print(json.dumps(line), flush=True)
     P.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
