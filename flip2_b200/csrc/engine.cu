@@ -72,7 +72,7 @@ struct flip_engine {
     bool warm_ok = false;          // pcg.x holds the previous step's converged pressure
     PcgState* h_state = nullptr;
     cudaGraphExec_t pcg_graph = nullptr;
-    int pcg_graph_iters = 0;
+    int pcg_graph_iters = 0, pcg_graph_limit = 0;
     int sms = 148;
     int last_iters = 0, last_converged = 0;
     double last_rel = 0.0;
@@ -91,7 +91,7 @@ struct flip_engine {
     uint64_t noise_counter = 0;
     bool lp_have_weights = false;
     cudaGraphExec_t fpcg_graph = nullptr;
-    int fpcg_graph_iters = 0;
+    int fpcg_graph_iters = 0, fpcg_graph_limit = 0;
     bool poisson_ready = false;  // a standalone pressure problem is in place
     float4* gen_sph = nullptr;   // generator inputs (device)
     float* gen_imp = nullptr;
@@ -658,22 +658,62 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
     return FLIP_OK;
 }
 
-static int nat_pcg_graph(flip_engine* e, int iters) {
-    if (e->pcg_graph && e->pcg_graph_iters == iters) return FLIP_OK;
-    if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
+// A whole solve as one graph: a conditional WHILE node whose body is
+// `body` (a chunk of iterations and the true-residual check, captured from
+// the engine stream) followed by the loop control kernel, which stops the
+// loop when the device state says done or after `limit` chunks.  The host
+// launches it once per solve and reads the state once at the end.
+template <class Body>
+static int build_loop_graph(flip_engine* e, Body body, int limit, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
-    E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = FLIP_OK;
-    for (int k = 0; k < iters && rc == FLIP_OK; ++k)
-        rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-    if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    E_CUDA(ce);
-    ce = cudaGraphInstantiate(&e->pcg_graph, g, 0);
+    E_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t ce = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node = nullptr;
+    if (ce == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ce = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    }
+    if (ce == cudaSuccess)
+        ce = cudaStreamBeginCaptureToGraph(e->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e->cuda(ce, "conditional loop graph");
+    }
+    int rc = body();
+    if (rc == FLIP_OK) rc = nat_launch_loop_ctl(h, e->pcg.st, limit, e->stream);
+    cudaGraph_t captured = nullptr;
+    ce = cudaStreamEndCapture(e->stream, &captured);
+    if (rc != FLIP_OK || ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return rc != FLIP_OK ? rc : e->cuda(ce, "cudaStreamEndCapture");
+    }
+    ce = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     E_CUDA(ce);
+    return FLIP_OK;
+}
+
+static int loop_limit(int max_iter, int chunk) { return (max_iter + chunk - 1) / chunk + 3; }
+
+static int nat_pcg_graph(flip_engine* e, int iters, int max_iter) {
+    const int limit = loop_limit(max_iter, iters);
+    if (e->pcg_graph && e->pcg_graph_iters == iters && e->pcg_graph_limit == limit) return FLIP_OK;
+    if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
+    E_TRY(build_loop_graph(e, [&]() {
+        int rc = FLIP_OK;
+        for (int k = 0; k < iters && rc == FLIP_OK; ++k)
+            rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        return rc;
+    }, limit, &e->pcg_graph));
     e->pcg_graph_iters = iters;
+    e->pcg_graph_limit = limit;
     return FLIP_OK;
 }
 
@@ -759,42 +799,34 @@ static void pcg_state_host(flip_engine* e, double tol, int max_iter, int flexibl
     *e->h_state = init;
 }
 
-static int nat_fpcg_graph(flip_engine* e, int iters) {
-    if (e->fpcg_graph && e->fpcg_graph_iters == iters) return FLIP_OK;
+static int nat_fpcg_graph(flip_engine* e, int iters, int max_iter) {
+    const int limit = loop_limit(max_iter, iters);
+    if (e->fpcg_graph && e->fpcg_graph_iters == iters && e->fpcg_graph_limit == limit) return FLIP_OK;
     if (e->fpcg_graph) { cudaGraphExecDestroy(e->fpcg_graph); e->fpcg_graph = nullptr; }
-    cudaGraph_t g = nullptr;
-    E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     const LpGrid G = lp_grid(e, &e->pcg.st->halt);
     const float* inv_s = &e->pcg.st->inv_s;
-    int rc = FLIP_OK;
-    for (int k = 0; k < iters && rc == FLIP_OK; ++k) {
-        rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-        if (rc == FLIP_OK && k == iters - 1) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-        if (rc == FLIP_OK) rc = lp_forward_dev(e->lp, G, inv_s, e->lp_f0, e->pcg.z, nat_grid(e, 2), e->stream);
-        if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream);
-    }
-    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    E_CUDA(ce);
-    ce = cudaGraphInstantiate(&e->fpcg_graph, g, 0);
-    cudaGraphDestroy(g);
-    E_CUDA(ce);
+    E_TRY(build_loop_graph(e, [&]() {
+        int rc = FLIP_OK;
+        for (int k = 0; k < iters && rc == FLIP_OK; ++k) {
+            rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            if (rc == FLIP_OK && k == iters - 1)
+                rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            if (rc == FLIP_OK) rc = lp_forward_dev(e->lp, G, inv_s, e->lp_f0, e->pcg.z, nat_grid(e, 2), e->stream);
+            if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream);
+        }
+        return rc;
+    }, limit, &e->fpcg_graph));
     e->fpcg_graph_iters = iters;
+    e->fpcg_graph_limit = limit;
     return FLIP_OK;
 }
 
-// launch a chunk graph until the device state says done; bounded on the host
-static int run_chunks(flip_engine* e, cudaGraphExec_t g, int chunk, uint32_t launches_per_chunk, int max_iter) {
-    int launched = 0;
-    for (;;) {
-        E_CUDA(cudaGraphLaunch(g, e->stream));
-        e->launches += launches_per_chunk;
-        launched += chunk;
-        E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
-        E_CUDA(cudaStreamSynchronize(e->stream));
-        if (e->h_state->done) break;
-        if (launched > max_iter + 2 * chunk) break;  // host-side bound as well
-    }
+// one launch of a solve's loop graph; the state comes back once at the end
+static int run_loop(flip_engine* e, cudaGraphExec_t g, uint32_t launches_per_chunk) {
+    E_CUDA(cudaGraphLaunch(g, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->launches += (launches_per_chunk + 1u) * (uint32_t)e->h_state->chunks;
     return FLIP_OK;
 }
 
@@ -820,8 +852,8 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream));
         e->launches += 10;
         E_TRY(e->mark(9));
-        E_TRY(nat_fpcg_graph(e, chunk));
-        E_TRY(run_chunks(e, e->fpcg_graph, chunk, 7u * (uint32_t)chunk + 1u, max_learned));
+        E_TRY(nat_fpcg_graph(e, chunk, max_learned));
+        E_TRY(run_loop(e, e->fpcg_graph, 7u * (uint32_t)chunk + 1u));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
@@ -839,8 +871,8 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
                                   w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
         if (method != 1) E_TRY(e->mark(9));
-        E_TRY(nat_pcg_graph(e, chunk));
-        E_TRY(run_chunks(e, e->pcg_graph, chunk, 2u * (uint32_t)chunk + 1u, max_plain));
+        E_TRY(nat_pcg_graph(e, chunk, max_plain));
+        E_TRY(run_loop(e, e->pcg_graph, 2u * (uint32_t)chunk + 1u));
         const PcgState& s = *e->h_state;
         if (method == 1) info.plain_iters = s.iter;
         else info.iters = s.iter;

@@ -1146,6 +1146,15 @@ int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const 
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+__global__ void pcg_loop_ctl_kernel(cudaGraphConditionalHandle h, PcgState* st, int limit) {
+    const int c = ++st->chunks;
+    cudaGraphSetConditional(h, (st->done || c >= limit) ? 0u : 1u);
+}
+int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, cudaStream_t s) {
+    pcg_loop_ctl_kernel<<<1, 1, 0, s>>>(h, st, limit);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
     nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, phig, type, U[0], U[1], U[2]);

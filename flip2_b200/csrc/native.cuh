@@ -27,6 +27,7 @@ struct PcgState {
     float inv_s;  // 1 / rms(r) over fluid cells: input scale of the learned preconditioner
     int flexible; // 1: FPCG (z = N(r) given), 0: Jacobi PCG
     double zq, nfluid;
+    int chunks;   // chunks the device-side loop has run
 };
 
 constexpr int kPcgBlocks = 592;        // 148 SMs x 4 CTAs of 512 threads
@@ -90,6 +91,9 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
 // true_every iterations; decides convergence
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s);
+// end of a loop chunk inside a conditional WHILE graph node: continue while
+// the solve is not done and fewer than limit chunks have run
+int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, cudaStream_t s);
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s);
 int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
