@@ -1002,10 +1002,28 @@ extern "C" int flip_initialize(flip_engine* e) {
     }
     return nat_bin(e);
 }
+// native Courant limit: 0.7 voxel sizes per sub-step for the fastest velocity
+// component, the reference's rule (particles.cu:493-498) on the native voxel;
+// 0 when every particle is at rest
+static int nat_courant_dt(flip_engine* e, double* dt) {
+    E_TRY(nat_launch_vmax(e->n, (const float* const*)(e->fp + 3), e->d_counts + 2, nat_grid(e, 4), e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_small + 2, e->d_counts + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->launches += 1;
+    float vmax = 0.0f;
+    memcpy(&vmax, e->h_small + 2, sizeof(float));
+    *dt = vmax > 0.0f ? 0.7 * (double)e->D.h / (double)vmax : 0.0;
+    return FLIP_OK;
+}
+
 extern "C" double flip_get_courant_dt(flip_engine* e) {
-    if (!e || !e->have_domain || e->P.mode != FLIP_MODE_REFERENCE) return 0.0;
+    if (!e || !e->have_domain) return 0.0;
     double dt = 0.0;
-    if (ref_courant_dt(e, &dt)) return 0.0;
+    if (e->P.mode == FLIP_MODE_REFERENCE) {
+        if (ref_courant_dt(e, &dt)) return 0.0;
+    } else {
+        if (cudaSetDevice(e->P.device) != cudaSuccess || nat_courant_dt(e, &dt)) return 0.0;
+    }
     return dt;
 }
 
@@ -1034,9 +1052,18 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
         E_CUDA(cudaStreamSynchronize(e->stream));
         return FLIP_OK;
     }
+    // sub-steps of min(max_substep_dt, the Courant limit, what is left of the frame)
     const double frameDt = 1.0 / fps;
-    const int nsub = std::max(1, (int)std::ceil(frameDt / e->P.max_substep_dt - 1e-9));
-    for (int k = 0; k < nsub; ++k) E_TRY(nat_step(e, frameDt / nsub));
+    double t = 0.0;
+    int guard = 0;
+    while (frameDt - t > 1e-12 * frameDt) {
+        double dt = std::min(e->P.max_substep_dt, frameDt - t), cfl = 0.0;
+        E_TRY(nat_courant_dt(e, &cfl));
+        if (cfl > 0.0) dt = std::min(dt, cfl);
+        if (!(dt > 1e-9 * frameDt) || ++guard > 100000) return e->fail(FLIP_ERR_STATE, "solveFrame: dt collapsed");
+        E_TRY(nat_step(e, dt));
+        t += dt;
+    }
     E_CUDA(cudaStreamSynchronize(e->stream));
     return FLIP_OK;
 }

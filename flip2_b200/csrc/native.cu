@@ -1155,6 +1155,24 @@ int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, c
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+// largest |velocity component| over the particles, as the bits of a
+// non-negative float (their unsigned order is the float order); *out must be 0
+__global__ void __launch_bounds__(256) nat_vmax_kernel(uint64_t n, const float* __restrict__ vx,
+                                                       const float* __restrict__ vy, const float* __restrict__ vz,
+                                                       uint32_t* __restrict__ out) {
+    float m = 0.0f;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fmaxf(fabsf(vx[i]), fmaxf(fabsf(vy[i]), fabsf(vz[i]))));
+    uint32_t b = __float_as_uint(m);
+    b = __reduce_max_sync(0xFFFFFFFFu, b);
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(out, b);
+}
+int nat_launch_vmax(uint64_t n, const float* const* V, uint32_t* d_out, int grid, cudaStream_t s) {
+    FLIP_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(uint32_t), s));
+    nat_vmax_kernel<<<grid, 256, 0, s>>>(n, V[0], V[1], V[2], d_out);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
     nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, phig, type, U[0], U[1], U[2]);

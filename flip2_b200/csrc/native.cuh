@@ -94,6 +94,8 @@ int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const 
 // end of a loop chunk inside a conditional WHILE graph node: continue while
 // the solve is not done and fewer than limit chunks have run
 int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, cudaStream_t s);
+// *d_out = bits of max over particles of max(|vx|, |vy|, |vz|) (the Courant limit's speed)
+int nat_launch_vmax(uint64_t n, const float* const* V, uint32_t* d_out, int grid, cudaStream_t s);
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
                        const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s);
 int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,

@@ -208,6 +208,10 @@ int flip_move_solid_particles(flip_engine* e);      /* moveSolidParticles, parti
 int flip_initialize(flip_engine* e);                /* initialize, particles.cu:805-812            */
 int flip_solve_frame(flip_engine* e, double fps);   /* solveFrame, particles.cu:784-803            */
 double flip_get_courant_dt(flip_engine* e);         /* getCourantDt, particles.cu:493-498          */
+/* In native mode solveFrame takes sub-steps of min(max_substep_dt, the
+ * Courant limit 0.7 h / max |v component|, the rest of the frame), with the
+ * speed reduced on the device; flip_get_courant_dt returns that limit (0 at
+ * rest). */
 /* writePositionsToFile (particles.cu:817-828): "x, y, z" per line. */
 int flip_write_positions_csv(flip_engine* e, const char* path);
 /* Binary variant of the same frame (no reference counterpart): a 16-byte

@@ -168,3 +168,31 @@ def test_position_frames(torch, tmp_path):
     assert txt.shape == pg.shape and np.max(np.abs(txt - pg)) <= 5e-6 * np.max(np.abs(pg))
     with open(tmp_path / "frame.bin", "rb") as f:
         assert f.read(8) == b"FLIP2POS"
+
+
+def test_native_solve_frame_courant(torch):
+    # solveFrame sub-steps: min(max_substep_dt, 0.7 h / max |v component|, the
+    # rest of the frame); the limit comes from a device-side max over particles
+    nc = 32
+    pos, _ = scenes.dam_break(nc, seed=0)
+    vel = scenes.random_velocities(pos.shape[0], seed=3, scale=8.0)  # Courant limit below max_substep_dt
+    P = native(pos.shape[0], nc)
+    P.upload(pos, vel)
+    h = 1.0 / nc
+    expect = 0.7 * h / float(np.max(np.abs(vel.astype(np.float32))))
+    got = P.getCourantDt()
+    assert abs(got - expect) <= 1e-6 * expect
+    t0 = P.info().elapsed_time
+    P.solveFrame(24.0)
+    info = P.info()
+    assert abs(info.elapsed_time - t0 - 1.0 / 24.0) < 1e-12
+    assert 0.0 < info.dt <= F.default_params(F.MODE_NATIVE).max_substep_dt + 1e-15
+    assert info.converged == 1
+    pg, vg = P.download()
+    assert np.all(np.isfinite(pg)) and pg.min() > 0.0 and pg.max() < 1.0
+    # at rest the limit is 0 (no Courant bound)
+    Q = native(pos.shape[0], nc)
+    Q.upload(pos, np.zeros_like(vel))
+    assert Q.getCourantDt() == 0.0
+    Q.close()
+    P.close()
