@@ -317,9 +317,10 @@ def main():
     torch.cuda.synchronize(dev)
     e0.record(stream)
     for _ in range(args.steps):
-        P.upload_ptrs(ptrs)
-        P.step(DT)
-        P.download_ptrs(ptrs)
+        # upload the state from pinned host memory, step, download the new
+        # state; each call's download overlaps the next call's upload
+        P.step_streamed(ptrs, DT)
+    P.sync()  # orders the engine stream after the last download
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()

@@ -126,6 +126,7 @@ def lib():
         "flip_get_courant_dt": (d, [vp]),
         "flip_write_positions_csv": (i32, [vp, C.c_char_p]),
         "flip_write_positions_bin": (i32, [vp, C.c_char_p]),
+        "flip_step_streamed_f32": (i32, [vp] * 7 + [u64, d]),
         "flip_step": (i32, [vp, d]),
         "flip_sync": (i32, [vp]),
         "flip_get_buffer": (i32, [vp, i32, C.POINTER(vp), C.POINTER(u64), C.POINTER(u32)]),
@@ -416,6 +417,11 @@ class Particles:
         """Upload from six host pointers (pinned or pageable), no copies in Python."""
         fn = "flip_upload_particles_f64" if f64 else "flip_upload_particles_f32"
         self._call(fn, *[C.c_void_p(p) if p else None for p in ptrs], self.size)
+
+    def step_streamed(self, ptrs, dt):
+        """Upload from six host float32 arrays (pointers), one step, download into
+        them; returns before the download ends (sync() waits for it)."""
+        self._call("flip_step_streamed_f32", *[C.c_void_p(p) for p in ptrs], self.size, dt)
 
     def download_ptrs(self, ptrs, f64=False):
         fn = "flip_download_particles_f64" if f64 else "flip_download_particles_f32"

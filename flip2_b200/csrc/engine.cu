@@ -96,6 +96,12 @@ struct flip_engine {
     float4* gen_sph = nullptr;   // generator inputs (device)
     float* gen_imp = nullptr;
     cudaEvent_t solve_ev[2] = {};
+    // streamed round trips (flip_step_streamed_f32): copy streams and the
+    // events that order each chunk's upload after the previous download
+    static constexpr int kRtChunks = 8;
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    cudaEvent_t ev_down[kRtChunks] = {}, ev_start = nullptr, ev_up = nullptr, ev_step = nullptr;
+    bool rt_down_pending = false;
     uint32_t launches = 0;
     // stage timing
     bool timing = false;
@@ -132,6 +138,16 @@ struct flip_engine {
 static size_t al(size_t v) { return (v + 255) / 256 * 256; }
 constexpr int kGenMaxSpheres = 4096;
 constexpr int kGenMaxImpulses = 64;
+
+// Work on the engine stream that follows a streamed round trip must not
+// touch the particle buffers while that call's download still reads them:
+// order the engine stream after the download (a device-side wait).
+static int rt_join(flip_engine* e) {
+    if (!e->rt_down_pending) return FLIP_OK;
+    E_CUDA(cudaStreamWaitEvent(e->stream, e->ev_down[flip_engine::kRtChunks - 1], 0));
+    e->rt_down_pending = false;
+    return FLIP_OK;
+}
 
 extern "C" void flip_default_params(int mode, flip_params* out) {
     if (!out) return;
@@ -232,6 +248,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
     if (!e) return FLIP_ERR_ARG;
     if (x == 0 || y == 0 || z == 0 || !(cellSize > 0.0)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: empty domain");
     E_CUDA(cudaSetDevice(e->P.device));
+    E_TRY(rt_join(e));
     E_CUDA(cudaStreamSynchronize(e->stream));
     free_arena(e);
     free_ref_voxels(e);
@@ -316,6 +333,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
 extern "C" int flip_upload_particles_f64(flip_engine* e, const double* px, const double* py, const double* pz,
                                          const double* vx, const double* vy, const double* vz, uint64_t n) {
     if (!e || !px || !py || !pz) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "upload before setDomain");
     if (n != e->n) return e->fail(FLIP_ERR_ARG, "upload size differs from the engine size");  // cudaVec.cu:90-93 exits here
     const double* src[6] = {px, py, pz, vx, vy, vz};
@@ -343,6 +361,7 @@ extern "C" int flip_upload_particles_f64(flip_engine* e, const double* px, const
 extern "C" int flip_upload_particles_f32(flip_engine* e, const float* px, const float* py, const float* pz,
                                          const float* vx, const float* vy, const float* vz, uint64_t n) {
     if (!e || !px || !py || !pz) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "upload before setDomain");
     if (n != e->n) return e->fail(FLIP_ERR_ARG, "upload size differs from the engine size");
     const float* src[6] = {px, py, pz, vx, vy, vz};
@@ -370,6 +389,7 @@ extern "C" int flip_upload_particles_f32(flip_engine* e, const float* px, const 
 extern "C" int flip_download_particles_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy,
                                            float* vz, uint64_t n) {
     if (!e) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "download before setDomain");
     if (n != e->n) return e->fail(FLIP_ERR_ARG, "download size differs from the engine size");
     float* dst[6] = {px, py, pz, vx, vy, vz};
@@ -392,6 +412,7 @@ extern "C" int flip_download_particles_f32(flip_engine* e, float* px, float* py,
 extern "C" int flip_download_particles_f64(flip_engine* e, double* px, double* py, double* pz, double* vx, double* vy,
                                            double* vz, uint64_t n) {
     if (!e) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "download before setDomain");
     if (n != e->n) return e->fail(FLIP_ERR_ARG, "download size differs from the engine size");
     double* dst[6] = {px, py, pz, vx, vy, vz};
@@ -413,6 +434,7 @@ extern "C" int flip_download_particles_f64(flip_engine* e, double* px, double* p
 
 extern "C" int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uint64_t n_voxels) {
     if (!e) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     if (e->P.mode != FLIP_MODE_NATIVE || !e->have_domain) return e->fail(FLIP_ERR_STATE, "solid mask needs a native-mode domain");
     const NatDims& D = e->D;
     if (n_voxels != (uint64_t)D.nx * D.ny * D.nz) return e->fail(FLIP_ERR_ARG, "solid mask size != voxel count");
@@ -939,6 +961,7 @@ static int nat_step(flip_engine* e, double dt) {
         if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain"); \
         e->err.clear();                                                       \
         E_CUDA(cudaSetDevice(e->P.device));                                   \
+        E_TRY(rt_join(e));                                                    \
     } while (0)
 
 extern "C" int flip_align_particles_to_grid(flip_engine* e) {
@@ -1096,7 +1119,66 @@ extern "C" int flip_step(flip_engine* e, double dt) {
 
 extern "C" int flip_sync(flip_engine* e) {
     if (!e) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));  // the last streamed download, in the engine stream's order
     E_CUDA(cudaStreamSynchronize(e->stream));
+    return FLIP_OK;
+}
+
+static int rt_setup(flip_engine* e) {
+    if (e->up_stream) return FLIP_OK;
+    E_CUDA(cudaStreamCreateWithFlags(&e->up_stream, cudaStreamNonBlocking));
+    E_CUDA(cudaStreamCreateWithFlags(&e->down_stream, cudaStreamNonBlocking));
+    for (auto& v : e->ev_down) E_CUDA(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+    E_CUDA(cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming));
+    E_CUDA(cudaEventCreateWithFlags(&e->ev_up, cudaEventDisableTiming));
+    E_CUDA(cudaEventCreateWithFlags(&e->ev_step, cudaEventDisableTiming));
+    return FLIP_OK;
+}
+
+// Upload the particle state from host arrays, one native step, and download
+// the new state into the same arrays.  The copies run in kRtChunks ranges on
+// two copy streams: a range's upload waits only for the previous call's
+// download of that range, so one call's download and the next call's upload
+// overlap (the host link is full duplex).  Returns before the download ends.
+extern "C" int flip_step_streamed_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy, float* vz,
+                                      uint64_t n, double dt) {
+    if (!e) return FLIP_ERR_ARG;
+    if (!e->have_domain) return e->fail(FLIP_ERR_STATE, "call before setDomain");
+    e->err.clear();
+    E_CUDA(cudaSetDevice(e->P.device));
+    if (e->P.mode != FLIP_MODE_NATIVE) return e->fail(FLIP_ERR_STATE, "flip_step_streamed_f32: native mode only");
+    if (!px || !py || !pz || !vx || !vy || !vz) return e->fail(FLIP_ERR_ARG, "flip_step_streamed_f32: null array");
+    if (n != e->n) return e->fail(FLIP_ERR_ARG, "flip_step_streamed_f32: size differs from the engine size");
+    if (!(dt > 0.0)) return e->fail(FLIP_ERR_ARG, "dt must be positive");
+    E_TRY(rt_setup(e));
+    float* host[6] = {px, py, pz, vx, vy, vz};
+    const int C = flip_engine::kRtChunks;
+    const uint64_t per = (n + C - 1) / C;
+    // uploads: after everything already on the engine stream, and range by
+    // range after the previous call's download of that range
+    E_CUDA(cudaEventRecord(e->ev_start, e->stream));
+    E_CUDA(cudaStreamWaitEvent(e->up_stream, e->ev_start, 0));
+    for (int c = 0; c < C; ++c) {
+        const uint64_t b = std::min<uint64_t>(n, c * per), m = std::min<uint64_t>(n, b + per) - b;
+        if (e->rt_down_pending) E_CUDA(cudaStreamWaitEvent(e->up_stream, e->ev_down[c], 0));
+        for (int a = 0; a < 6 && m; ++a)
+            E_CUDA(cudaMemcpyAsync(e->fp[a] + b, host[a] + b, 4 * m, cudaMemcpyHostToDevice, e->up_stream));
+    }
+    E_CUDA(cudaEventRecord(e->ev_up, e->up_stream));
+    E_CUDA(cudaStreamWaitEvent(e->stream, e->ev_up, 0));
+    e->rt_down_pending = false;
+    e->binned = e->have_voxels = false;
+    E_TRY(nat_step(e, dt));
+    // downloads of the new state (the step leaves it in fp)
+    E_CUDA(cudaEventRecord(e->ev_step, e->stream));
+    E_CUDA(cudaStreamWaitEvent(e->down_stream, e->ev_step, 0));
+    for (int c = 0; c < C; ++c) {
+        const uint64_t b = std::min<uint64_t>(n, c * per), m = std::min<uint64_t>(n, b + per) - b;
+        for (int a = 0; a < 6 && m; ++a)
+            E_CUDA(cudaMemcpyAsync(host[a] + b, e->fp[a] + b, 4 * m, cudaMemcpyDeviceToHost, e->down_stream));
+        E_CUDA(cudaEventRecord(e->ev_down[c], e->down_stream));
+    }
+    e->rt_down_pending = true;
     return FLIP_OK;
 }
 
@@ -1138,6 +1220,7 @@ extern "C" int flip_write_positions_bin(flip_engine* e, const char* path) {
 
 extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, uint32_t* elem_size) {
     if (!e || !dev_ptr || !count || !elem_size) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     const bool ref = e->P.mode == FLIP_MODE_REFERENCE;
     if (!ref && e->have_domain) {  // refresh the device-side tile count
         E_CUDA(cudaMemcpyAsync(e->h_small, e->d_counts, 8, cudaMemcpyDeviceToHost, e->stream));
@@ -1184,6 +1267,7 @@ extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64
 
 extern "C" int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint64_t bytes) {
     if (!e || !host_dst) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     void* p = nullptr;
     uint64_t c = 0;
     uint32_t es = 0;
@@ -1196,6 +1280,7 @@ extern "C" int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint6
 
 extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
     if (!e || !out) return FLIP_ERR_ARG;
+    E_TRY(rt_join(e));
     memset(out, 0, sizeof(*out));
     if (e->have_domain) {
         E_CUDA(cudaStreamSynchronize(e->stream));
@@ -1552,6 +1637,8 @@ extern "C" const char* flip_last_error(flip_engine* e) {
 extern "C" int flip_destroy(flip_engine* e) {
     if (!e) return FLIP_OK;
     cudaSetDevice(e->P.device);
+    if (e->up_stream) cudaStreamSynchronize(e->up_stream);
+    if (e->down_stream) cudaStreamSynchronize(e->down_stream);
     if (e->stream) cudaStreamSynchronize(e->stream);
     free_arena(e);
     free_ref_voxels(e);
@@ -1560,6 +1647,11 @@ extern "C" int flip_destroy(flip_engine* e) {
     if (e->h_state) cudaFreeHost(e->h_state);
     for (auto& v : e->ev) if (v) cudaEventDestroy(v);
     for (auto& v : e->solve_ev) if (v) cudaEventDestroy(v);
+    for (auto& v : e->ev_down) if (v) cudaEventDestroy(v);
+    cudaEvent_t evs[3] = {e->ev_start, e->ev_up, e->ev_step};
+    for (auto v : evs) if (v) cudaEventDestroy(v);
+    if (e->up_stream) cudaStreamDestroy(e->up_stream);
+    if (e->down_stream) cudaStreamDestroy(e->down_stream);
     if (e->lp_warena) cudaFree(e->lp_warena);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;

@@ -225,6 +225,16 @@ int flip_write_positions_bin(flip_engine* e, const char* path);
  * convergence reads of the pressure solve. */
 int flip_step(flip_engine* e, double dt);
 int flip_sync(flip_engine* e);
+/* NATIVE, no reference counterpart: a host round trip per step.  Uploads
+ * the particle state from the six host arrays (pinned memory lets the copies
+ * run asynchronously), takes one step and downloads the new state into the
+ * same arrays.  The copies run in 8 ranges on two copy streams; a range's
+ * upload waits only for the previous call's download of that range, so one
+ * call's download overlaps the next call's upload.  The call returns before
+ * its download has finished: flip_sync (and every other engine call) waits
+ * for it, and the host arrays must not be read or written before then. */
+int flip_step_streamed_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy, float* vz,
+                           uint64_t n, double dt);
 
 /* Buffers for inspection (device pointers lent, not transferred). */
 typedef enum {
