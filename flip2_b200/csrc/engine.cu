@@ -866,6 +866,10 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
     if (method == 1) {
         E_TRY(lp_ready(e));
         pcg_state_host(e, tol, max_learned, 1);
+        // a true-residual check every chunk: FCG gives up when a chunk reduces
+        // the residual by less than 10% (device state done = 4)
+        e->h_state->true_every = chunk;
+        e->h_state->next_check = chunk;
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
         E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
         const LpGrid G = lp_grid(e, &e->pcg.st->halt);

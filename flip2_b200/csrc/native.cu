@@ -448,6 +448,7 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     if (last_block_reduce<3>(vals, B.partials, &B.st->ticket, sh, out) && threadIdx.x == 0) {
         PcgState* st = B.st;
         st->bb = out[0];
+        st->rr_check = out[0];
         st->nfluid = out[2];
         st->inv_s = out[0] > 0.0 ? (float)(1.0 / sqrt(out[0] / fmax(out[2], 1.0))) : 1.0f;
         st->zq = 0.0;
@@ -838,7 +839,11 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
             }
             st->inv_s = (float)(1.0 / sqrt(out[0] / fmax(st->nfluid, 1.0)));
             if (st->iter >= st->max_iter) st->done = 2;
+            // flexible CG that has stopped converging: the true residual norm
+            // fell by less than 10% since the previous check
+            if (st->flexible && !st->done && out[0] > kFlexStall * st->rr_check) st->done = 4;
         }
+        st->rr_check = out[0];
         st->pending = 0;
         st->halt = st->done;
     }

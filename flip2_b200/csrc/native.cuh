@@ -28,7 +28,11 @@ struct PcgState {
     int flexible; // 1: FPCG (z = N(r) given), 0: Jacobi PCG
     double zq, nfluid;
     int chunks;   // chunks the device-side loop has run
+    double rr_check;  // r.r at the previous true-residual check (bb before the first)
 };
+// flexible CG gives up (done = 4) when the true r.r at a check exceeds this
+// fraction of the previous check's: the residual norm fell by less than 10%
+constexpr double kFlexStall = 0.81;
 
 constexpr int kPcgBlocks = 592;        // 148 SMs x 4 CTAs of 512 threads
 constexpr int kPcgUpdateBlocks = 592;  // 148 SMs x 4 CTAs of 256 threads (a warp per half tile, 10 loads in flight a lane)

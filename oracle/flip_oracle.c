@@ -1194,7 +1194,8 @@ double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float
 
 /* flexible CG (FCG(1)) with M(r) = N(r) + D^-1 r as preconditioner, in
  * FP64 apart from the network; returns iterations (max_iter + 1 if not
- * converged), x out, *rel_res = |b - A x| / |b| */
+ * converged or stalled: less than 10% residual reduction over 16
+ * iterations), x out, *rel_res = |b - A x| / |b| */
 int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
                 int round_bf16, double tol, int max_iter, double* x, double* rel_res) {
     lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
@@ -1212,7 +1213,7 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
     }
     const double bn = sqrt(bb);
     int it = 0;
-    double pq_prev = 0.0;
+    double pq_prev = 0.0, rr_check = bb;
     if (bn > 0.0) {
         for (it = 1; it <= max_iter + 1; ++it) {
             for (int64_t v = 0; v < nc; ++v) rf[v] = (float)r[v];
@@ -1240,6 +1241,12 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
                 rr += r[v] * r[v];
             }
             if (sqrt(rr) <= tol * bn) break;
+            /* the GPU solve's stagnation rule: every 16 iterations the residual
+             * norm must have fallen by 10% since the previous check */
+            if (it % 16 == 0) {
+                if (rr > 0.81 * rr_check) { it = max_iter + 1; break; }
+                rr_check = rr;
+            }
         }
     }
     lp_apply_A(&D, type, x, q);

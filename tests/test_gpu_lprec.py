@@ -209,8 +209,8 @@ def test_fpcg_vs_oracle_fpcg(trained):
         x = P.poisson_solution()
         assert rel_err(x, xo) < 2e-3
     else:
-        # it stalls in FP64 too: the GPU run hits its cap and Jacobi-PCG finishes
-        assert learned.fell_back == 1 and learned.iters == 400
+        # it stalls in FP64 too: the GPU run stops (cap or stagnation) and Jacobi-PCG finishes
+        assert learned.fell_back == 1 and learned.iters <= 400
         assert learned.plain_iters == plain.iters
         x = P.poisson_solution()
     assert solution_residual(typ, b, x, shape) <= 1.05e-6
