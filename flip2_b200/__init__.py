@@ -127,6 +127,7 @@ def lib():
         "flip_write_positions_csv": (i32, [vp, C.c_char_p]),
         "flip_write_positions_bin": (i32, [vp, C.c_char_p]),
         "flip_step_streamed_f32": (i32, [vp] * 7 + [u64, d]),
+        "flip_set_solid_velocity": (i32, [vp, d, d, d]),
         "flip_step": (i32, [vp, d]),
         "flip_sync": (i32, [vp]),
         "flip_get_buffer": (i32, [vp, i32, C.POINTER(vp), C.POINTER(u64), C.POINTER(u32)]),
@@ -437,6 +438,9 @@ class Particles:
     def set_solid_mask(self, mask):
         m = np.ascontiguousarray(mask, np.uint8)
         self._call("flip_set_solid_mask", m.ctypes.data_as(C.c_void_p), m.size)
+
+    def set_solid_velocity(self, ux, uy, uz):
+        self._call("flip_set_solid_velocity", ux, uy, uz)
 
     def buffer_ptr(self, which):
         p, c, es = C.c_void_p(), C.c_uint64(), C.c_uint32()

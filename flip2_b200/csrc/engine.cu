@@ -66,6 +66,7 @@ struct flip_engine {
     float *m[3] = {}, *w[3] = {}, *o[3] = {};
     uint8_t *type = nullptr, *solid_tiled = nullptr, *tile_flags = nullptr;
     bool has_solid = false;
+    float usolid[3] = {0.0f, 0.0f, 0.0f};  // velocity of the interior solid cells (native)
     uint32_t* grid_tiles = nullptr;
     PcgBuffers pcg{};
     uint8_t* cell_prev = nullptr;  // cell codes of the previous step's solve (warm start)
@@ -432,6 +433,16 @@ extern "C" int flip_download_particles_f64(flip_engine* e, double* px, double* p
     return FLIP_OK;
 }
 
+extern "C" int flip_set_solid_velocity(flip_engine* e, double ux, double uy, double uz) {
+    if (!e) return FLIP_ERR_ARG;
+    if (!std::isfinite(ux) || !std::isfinite(uy) || !std::isfinite(uz))
+        return e->fail(FLIP_ERR_ARG, "flip_set_solid_velocity: non-finite velocity");
+    e->usolid[0] = (float)ux;
+    e->usolid[1] = (float)uy;
+    e->usolid[2] = (float)uz;
+    return FLIP_OK;
+}
+
 extern "C" int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uint64_t n_voxels) {
     if (!e) return FLIP_ERR_ARG;
     E_TRY(rt_join(e));
@@ -673,7 +684,8 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
     E_TRY(nat_launch_tile_coords(e->node_keys, e->d_counts, e->D, e->pcg.tcoord, nat_grid(e, 2), e->stream));
     E_TRY(e->mark(7));
     E_TRY(nat_launch_normalize(e->grid_tiles, e->d_counts + 1, e->D, (float)(e->P.gravity_y * dt), e->m,
-                               (const float* const*)e->w, e->o, e->type, nat_grid(e, 4), e->stream));
+                               (const float* const*)e->w, e->o, e->type,
+                               make_float3(e->usolid[0], e->usolid[1], e->usolid[2]), nat_grid(e, 4), e->stream));
     E_TRY(e->mark(8));
     e->launches += 1 + (e->has_solid ? 1 : 0) + 3 + 1;
     e->have_voxels = true;

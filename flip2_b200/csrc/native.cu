@@ -318,8 +318,10 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
                                                              float* __restrict__ mw, const float* __restrict__ wu,
                                                              const float* __restrict__ wv, const float* __restrict__ ww,
                                                              float* __restrict__ ou, float* __restrict__ ov,
-                                                             float* __restrict__ ow, const uint8_t* __restrict__ type) {
+                                                             float* __restrict__ ow, const uint8_t* __restrict__ type,
+                                                             float3 usolid) {
     const uint32_t cnt = *d_count;
+    const float us[3] = {usolid.x, usolid.y, usolid.z};
     float* m[3] = {mu, mv, mw};
     const float* w[3] = {wu, wv, ww};
     float* o[3] = {ou, ov, ow};
@@ -335,7 +337,10 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
             float val = wt > 0.0f ? __fdiv_rn(m[c][s], wt) : 0.0f;
             o[c][s] = val;
             uint8_t ta = nat_type(type, i - (c == 0), j - (c == 1), k - (c == 2), D);
-            if (ta == kSolid || tb == kSolid) val = 0.0f;
+            // wall faces and faces between two solids 0; a face between a
+            // solid and a non-solid cell moves with the solid
+            const bool wall = (c == 0 ? i : (c == 1 ? j : k)) == 0;
+            if (ta == kSolid || tb == kSolid) val = (!wall && ((ta == kSolid) != (tb == kSolid))) ? us[c] : 0.0f;
             else if (c == 1 && (ta == kFluid || tb == kFluid)) val += gdt;
             m[c][s] = val;
         }
@@ -1098,8 +1103,9 @@ int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tile
     return FLIP_OK;
 }
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
-                         const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s) {
-    nat_normalize_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, gdt, m[0], m[1], m[2], w[0], w[1], w[2], o[0], o[1], o[2], type);
+                         const float* const* w, float* const* o, const uint8_t* type, float3 usolid, int grid,
+                         cudaStream_t s) {
+    nat_normalize_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, gdt, m[0], m[1], m[2], w[0], w[1], w[2], o[0], o[1], o[2], type, usolid);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -76,8 +76,11 @@ int nat_launch_solution_lin(const double* x, const float* xg, const uint8_t* cel
                             cudaStream_t s);
 int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s);
 int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s);
+// P2G sums -> face velocities; gravity on faces touching fluid; wall faces
+// 0; faces between a solid and a non-solid cell take usolid
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
-                         const float* const* w, float* const* o, const uint8_t* type, int grid, cudaStream_t s);
+                         const float* const* w, float* const* o, const uint8_t* type, float3 usolid, int grid,
+                         cudaStream_t s);
 // U == nullptr: the right-hand side is already in B.b (standalone Poisson problems).
 // cell_prev != nullptr: warm start from the previous solution (x + xg) on the
 // cells that were fluid in the previous solve (cell_prev: its cell codes)

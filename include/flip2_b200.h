@@ -194,6 +194,11 @@ int flip_download_particles_f32(flip_engine* e, float* px, float* py, float* pz,
                                 uint64_t n);
 /* Optional static solid cells (NATIVE): mask of nx*ny*nz voxels, x fastest. */
 int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uint64_t n_voxels);
+/* NATIVE, no reference counterpart (the reference's solids are static, walls
+ * only: particles.cu:479): the velocity of the interior solid cells.  Faces
+ * between a solid and a non-solid cell carry it, so the pressure solve and the
+ * projection see a moving obstacle; faces on the box walls stay 0. */
+int flip_set_solid_velocity(flip_engine* e, double ux, double uy, double uz);
 
 /* Per-stage methods of Particles (engine/particles.hu:17-43). */
 int flip_align_particles_to_grid(flip_engine* e);   /* alignParticlesToGrid, particles.cu:48-50    */

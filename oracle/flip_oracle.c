@@ -828,7 +828,10 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
     if (v_p2g) memcpy(v_p2g, U[1], 8 * (size_t)nc);
     if (w_p2g) memcpy(w_p2g, U[2], 8 * (size_t)nc);
     for (int c = 0; c < 3; ++c) memcpy(Uo[c], U[c], 8 * (size_t)nc);
-    /* face classification: solid-adjacent faces 0, fluid-adjacent faces get gravity */
+    /* face classification: wall faces and faces between two solid cells 0,
+     * faces between a solid and a non-solid cell the solid velocity, faces
+     * touching fluid get gravity */
+    const double us[3] = {P->solid_u, P->solid_v, P->solid_w};
     for (int c = 0; c < 3; ++c)
         for (int k = 0; k < P->nz; ++k)
             for (int j = 0; j < P->ny; ++j)
@@ -836,7 +839,11 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
                     int64_t id = nat_idx(P, i, j, k);
                     int ia = i - (c == 0), ja = j - (c == 1), ka = k - (c == 2);
                     int tb = nat_type(P, type, i, j, k), ta = nat_type(P, type, ia, ja, ka);
-                    if (ta == NAT_SOLID || tb == NAT_SOLID) { U[c][id] = 0.0; continue; }
+                    const int wall = ia < 0 || ja < 0 || ka < 0;
+                    if (ta == NAT_SOLID || tb == NAT_SOLID) {
+                        U[c][id] = (!wall && (ta == NAT_SOLID) != (tb == NAT_SOLID)) ? (double)(float)us[c] : 0.0;
+                        continue;
+                    }
                     if (c == 1 && (ta == NAT_FLUID || tb == NAT_FLUID)) U[c][id] += P->gravity_y * P->dt;
                 }
     /* divergence -> b = -div on fluid cells */

@@ -136,6 +136,9 @@ typedef struct {
     int32_t nx, ny, nz;
     double gravity_y, flip, dt, tol;
     int32_t max_iter;
+    /* velocity of the interior solid cells: faces between a solid and a
+     * non-solid cell take it; faces on the box walls stay 0 */
+    double solid_u, solid_v, solid_w;
 } orc_nat_params;
 
 /* Tile key of each particle (8^3-voxel tiles, x-fastest tile order). */

@@ -36,7 +36,7 @@ class NatParams(C.Structure):
     _fields_ = [("ox", C.c_double), ("oy", C.c_double), ("oz", C.c_double), ("h", C.c_double),
                 ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("gravity_y", C.c_double), ("flip", C.c_double), ("dt", C.c_double), ("tol", C.c_double),
-                ("max_iter", C.c_int32)]
+                ("max_iter", C.c_int32), ("solid_u", C.c_double), ("solid_v", C.c_double), ("solid_w", C.c_double)]
 
 
 class NatInfo(C.Structure):
@@ -220,8 +220,9 @@ def ref_substep(px, py, pz, vx, vy, vz, g, frame_dt=1.0 / 24.0, elapsed=0.0, per
 
 
 # ----------------------------------------------------------- north-star step
-def nat_params(nx, ny, nz, h, origin=(0.0, 0.0, 0.0), gravity_y=-9.8, flip=0.95, dt=1.0 / 240, tol=1e-6, max_iter=4000):
-    return NatParams(origin[0], origin[1], origin[2], h, nx, ny, nz, gravity_y, flip, dt, tol, max_iter)
+def nat_params(nx, ny, nz, h, origin=(0.0, 0.0, 0.0), gravity_y=-9.8, flip=0.95, dt=1.0 / 240, tol=1e-6, max_iter=4000,
+               solid_velocity=(0.0, 0.0, 0.0)):
+    return NatParams(origin[0], origin[1], origin[2], h, nx, ny, nz, gravity_y, flip, dt, tol, max_iter, *solid_velocity)
 
 
 def nat_keys(pos, P):

@@ -109,10 +109,12 @@ def test_native_warm_start(torch):
         assert np.max(np.abs(np.sort(pc[:, k]) - np.sort(pw[:, k]))) < 0.05 / nc
 
 
-def test_native_solid_sphere(torch):
+@pytest.mark.parametrize("usolid", [(0.0, 0.0, 0.0), (0.3, 0.5, -0.2)])
+def test_native_solid_sphere(torch, usolid):
     """Interior solid cells (the learned-preconditioner problems carry solid
-    spheres): faces touching solid cells stay zero, the solve converges, and
-    the result matches the oracle run with the same mask."""
+    spheres): faces between a solid and a non-solid cell carry the solid's
+    velocity (0 for a still solid), the solve converges, and the result
+    matches the oracle run with the same mask and velocity."""
     nc, dt = 32, 1.0 / 240
     pos, _ = scenes.dam_break(nc, block=(1.0, 0.5, 1.0), seed=3)
     vel = scenes.random_velocities(pos.shape[0], seed=4, scale=0.5)
@@ -121,11 +123,12 @@ def test_native_solid_sphere(torch):
     solid = (np.sum((c - np.array([0.5, 0.25, 0.5])) ** 2, -1) < 0.15 ** 2).astype(np.uint8).ravel()
     P = native(pos.shape[0], nc)
     P.set_solid_mask(solid)
+    P.set_solid_velocity(*usolid)
     P.upload(pos, vel)
     P.step(dt)
     info = P.info()
     assert info.converged == 1
-    Po = O.nat_params(nc, nc, nc, 1.0 / nc, dt=dt)
+    Po = O.nat_params(nc, nc, nc, 1.0 / nc, dt=dt, solid_velocity=usolid)
     ref = O.nat_step(pos, vel, Po, solid=solid)
     typ = tiled_to_linear(P.read(F.BUF_CELL_TYPE, np.uint8), nc, nc, nc)
     assert np.array_equal(typ == 2, solid == 1)
@@ -135,7 +138,11 @@ def test_native_solid_sphere(torch):
     solid3 = solid.reshape(nc, nc, nc)
     s_b = solid3.ravel() == 1
     s_a = np.roll(solid3, 1, axis=2).ravel() == 1
-    assert np.all(u[s_b | s_a] == 0.0)
+    assert np.all(u[s_b & s_a] == 0.0)
+    assert np.all(u[s_b ^ s_a] == np.float32(usolid[0]))  # the sphere is away from the walls
+    pg, vg = P.download()
+    perm = P.read(F.BUF_PERM)
+    assert rel_err(vg, ref["vel"][perm], floor=1.0) < 2e-3
     P.close()
 
 
