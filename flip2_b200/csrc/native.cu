@@ -20,11 +20,15 @@ __device__ __forceinline__ uint32_t nslot(int i, int j, int k, const NatDims& D)
     uint32_t t = (uint32_t)((i >> 3) + D.tx * ((j >> 3) + D.ty * (k >> 3)));
     return (t << 9) | (uint32_t)((i & 7) | ((j & 7) << 3) | ((k & 7) << 6));
 }
-__device__ __forceinline__ int nat_cell(float p, float o, float h, int n) {
-    float t = floorf(__fdiv_rn(__fsub_rn(p, o), h));
+// cell of grid coordinate g = (p - o) / h, clamped into [0, n)
+__device__ __forceinline__ int nat_cell_g(float g, int n) {
+    float t = floorf(g);
     int c = (t >= (float)n) ? n - 1 : (int)t;
     if (!(t > 0.0f)) c = 0;
     return c;
+}
+__device__ __forceinline__ int nat_cell(float p, float o, float h, int n) {
+    return nat_cell_g(__fdiv_rn(__fsub_rn(p, o), h), n);
 }
 __device__ __forceinline__ uint8_t nat_type(const uint8_t* type, int i, int j, int k, const NatDims& D) {
     if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return kSolid;
@@ -121,29 +125,37 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
         const uint32_t start = starts[t];
         const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
         for (uint64_t p = start + threadIdx.x; p < end; p += kP2GThreads) {
-            const float x = px[p], y = py[p], z = pz[p];
-            const float gx = __fdiv_rn(__fsub_rn(x, D.ox), D.h), gy = __fdiv_rn(__fsub_rn(y, D.oy), D.h),
-                        gz = __fdiv_rn(__fsub_rn(z, D.oz), D.h);
-            type[nslot(nat_cell(x, D.ox, D.h, D.nx), nat_cell(y, D.oy, D.h, D.ny), nat_cell(z, D.oz, D.h, D.nz), D)] = kFluid;
+            const float gx = __fdiv_rn(__fsub_rn(px[p], D.ox), D.h), gy = __fdiv_rn(__fsub_rn(py[p], D.oy), D.h),
+                        gz = __fdiv_rn(__fsub_rn(pz[p], D.oz), D.h);
+            type[nslot(nat_cell_g(gx, D.nx), nat_cell_g(gy, D.ny), nat_cell_g(gz, D.nz), D)] = kFluid;
             const float v[3] = {vx[p], vy[p], vz[p]};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 int i0, j0, k0;
                 float fx, fy, fz;
                 nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
+                const int li = i0 - bi, lj = j0 - bj, lk = k0 - bk;
+                // the 2 x 2 x 2 stencil lies inside the tile's box for every
+                // particle of the tile; the test guards the shared array
+                if ((unsigned)li >= (unsigned)(kBox - 1) || (unsigned)lj >= (unsigned)(kBox - 1) ||
+                    (unsigned)lk >= (unsigned)(kBox - 1))
+                    continue;
+                // per-axis weights, 0 on the wall faces of component c
+                float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+                if (c == 0) { if (i0 == 0) wx[0] = 0.0f; if (i0 + 1 == D.nx) wx[1] = 0.0f; }
+                if (c == 1) { if (j0 == 0) wy[0] = 0.0f; if (j0 + 1 == D.ny) wy[1] = 0.0f; }
+                if (c == 2) { if (k0 == 0) wz[0] = 0.0f; if (k0 + 1 == D.nz) wz[1] = 0.0f; }
+                const int l0 = li + kBox * (lj + kBox * lk);
 #pragma unroll
                 for (int dk = 0; dk < 2; ++dk)
 #pragma unroll
                     for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
                         for (int di = 0; di < 2; ++di) {
-                            int i = i0 + di, j = j0 + dj, k = k0 + dk;
-                            if (nat_wall(c, i, j, k, D)) continue;
-                            int li = i - bi, lj = j - bj, lk = k - bk;
-                            if ((unsigned)li >= (unsigned)kBox || (unsigned)lj >= (unsigned)kBox || (unsigned)lk >= (unsigned)kBox)
-                                continue;  // cannot happen for particles of this tile; guards the box
-                            float w = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) * (dk ? fz : 1.0f - fz);
-                            int l = li + kBox * (lj + kBox * lk);
+                            // a zero weight (a wall face) changes no sum
+                            const float w = wx[di] * wy[dj] * wz[dk];
+                            if (w == 0.0f) continue;
+                            const int l = l0 + di + kBox * (dj + kBox * dk);
                             atomicAdd(&sm[c][0][l], w * v[c]);
                             atomicAdd(&sm[c][1][l], w);
                         }
