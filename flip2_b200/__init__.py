@@ -56,7 +56,7 @@ class Params(C.Structure):
                 ("pcg_max_iter", C.c_int32), ("pcg_check_every", C.c_int32), ("true_residual_every", C.c_int32),
                 ("permute_velocities", C.c_int32), ("device", C.c_int32), ("pressure_method", C.c_int32),
                 ("max_substep_dt", C.c_double), ("learned_max_iter", C.c_int32), ("lp_cuda_cores", C.c_int32),
-                ("pcg_warm_start", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("pcg_warm_start", C.c_int32), ("mg_coarse", C.c_int32)]
 
 
 class PoissonSpec(C.Structure):
@@ -145,6 +145,8 @@ def lib():
         "flip_poisson_read_solution": (i32, [vp, vp]),
         "flip_lp_train_step": (i32, [vp, i32, C.c_float, C.POINTER(d)]),
         "flip_lp_eval": (i32, [vp, vp, vp, vp, C.POINTER(d), i32]),
+        "flip_mg_apply": (i32, [vp, vp, vp]),
+        "flip_mg_train_step": (i32, [vp, i32, C.c_float, C.POINTER(d)]),
         "flip_set_timing": (i32, [vp, i32]),
         "flip_get_stage_ms": (i32, [vp, C.POINTER(C.c_double), i32, i32]),
         "flip_last_error": (C.c_char_p, [vp]),
@@ -526,6 +528,21 @@ class Particles:
         self._call("flip_lp_eval", r.ctypes.data_as(C.c_void_p), ev.ctypes.data_as(C.c_void_p),
                    z.ctypes.data_as(C.c_void_p), C.byref(loss), 1 if want_grad else 0)
         return z, loss.value
+
+    def mg_apply(self, r_lin):
+        """One V-cycle of the multilevel preconditioner, z = M(r), x fastest."""
+        r = np.ascontiguousarray(r_lin, np.float32)
+        z = np.empty_like(r)
+        self._call("flip_mg_apply", r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p))
+        return z
+
+    def mg_train_step(self, sample, lr):
+        """Train the network as the V-cycle's coarsest solve.  sample >= 0:
+        the coarse right-hand side of the residual after that many Jacobi-PCG
+        iterations; -1: white-noise coarse error."""
+        loss = C.c_double()
+        self._call("flip_mg_train_step", sample, lr, C.byref(loss))
+        return loss.value
 
     def info(self):
         i = Info()

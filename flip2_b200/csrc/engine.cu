@@ -15,6 +15,7 @@
 #include <vector>
 #include "common.cuh"
 #include "lprec.cuh"
+#include "mg.cuh"
 #include "native.cuh"
 #include "ref_kernels.cuh"
 
@@ -93,6 +94,18 @@ struct flip_engine {
     bool lp_have_weights = false;
     cudaGraphExec_t fpcg_graph = nullptr;
     int fpcg_graph_iters = 0, fpcg_graph_limit = 0;
+    // multilevel preconditioner (pressure_method 2): levels per domain,
+    // allocated on first use; level 0 is the solver's grid
+    MgHierarchy mg{};
+    char* mg_arena = nullptr;
+    float* mg_zn = nullptr;      // network output on the coarsest level
+    float* mg_ev = nullptr;      // coarsest error sample (training)
+    float* mg_wbuf = nullptr;    // A m - r of the training loss
+    float* mg_gz = nullptr;      // dL/dN on the coarsest level
+    float* mg_s[3] = {};         // scratch of the coarsest CG
+    int* mg_iters = nullptr;     // iterations of the coarsest CG
+    cudaGraphExec_t mg_graph = nullptr;
+    int mg_graph_iters = 0, mg_graph_limit = 0, mg_graph_coarse = -1;
     bool poisson_ready = false;  // a standalone pressure problem is in place
     float4* gen_sph = nullptr;   // generator inputs (device)
     float* gen_imp = nullptr;
@@ -210,6 +223,7 @@ extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, 
 
 static void free_lp_activations(flip_engine* e) {
     if (e->fpcg_graph) { cudaGraphExecDestroy(e->fpcg_graph); e->fpcg_graph = nullptr; }
+    if (e->mg_graph) { cudaGraphExecDestroy(e->mg_graph); e->mg_graph = nullptr; }
     if (e->lp_aarena) cudaFree(e->lp_aarena);
     e->lp_aarena = nullptr;
     for (auto& a : e->lp.act) a = nullptr;
@@ -222,7 +236,14 @@ static void free_lp_activations(flip_engine* e) {
     e->lp_xs = e->lp_ev = nullptr;
     e->xstar_ready = false;
 }
+static void free_mg(flip_engine* e) {
+    if (e->mg_graph) { cudaGraphExecDestroy(e->mg_graph); e->mg_graph = nullptr; }
+    if (e->mg_arena) cudaFree(e->mg_arena);
+    e->mg_arena = nullptr;
+    e->mg = MgHierarchy{};
+}
 static void free_arena(flip_engine* e) {
+    free_mg(e);
     free_lp_activations(e);
     e->poisson_ready = false;
     if (e->pcg_graph) { cudaGraphExecDestroy(e->pcg_graph); e->pcg_graph = nullptr; }
@@ -822,6 +843,132 @@ static int lp_ready(flip_engine* e) {
     return lp_alloc_activations(e);
 }
 
+// ------------------------------------------------ multilevel preconditioner
+// the hierarchy of the domain: coarse levels allocated once per domain;
+// level 0 points at the solver's buffers (pcg.z lives with the network's)
+static int mg_ready(flip_engine* e, bool network) {
+    if (network) E_TRY(lp_ready(e));
+    else E_TRY(lp_alloc_activations(e));
+    MgHierarchy& H = e->mg;
+    if (!e->mg_arena) {
+        MgLevel L[kMgMaxLevels];
+        const int levels = mg_plan(e->D.nx, e->D.ny, e->D.nz, e->D.h, L, kMgMaxLevels);
+        const size_t fine = (size_t)e->nslots;
+        size_t total = 2 * al(4 * fine);
+        for (int l = 1; l < levels; ++l) {
+            const size_t n = (size_t)L[l].ntiles * 512u;
+            total += 2 * al(n) + al(L[l].ntiles) + al(4 * (size_t)L[l].ntiles) + 4 * al(4 * n) + 256;
+        }
+        const size_t nc = (size_t)L[levels - 1].ntiles * 512u;
+        total += 8 * al(4 * nc) + 1024;
+        E_CUDA(cudaMalloc((void**)&e->mg_arena, total));
+        E_CUDA(cudaMemsetAsync(e->mg_arena, 0, total, e->stream));
+        char* q = e->mg_arena;
+        auto take = [&](size_t b) { char* r = q; q += al(b); return r; };
+        L[0].t = (float*)take(4 * fine);
+        L[0].t2 = (float*)take(4 * fine);
+        std::vector<uint32_t> iota;
+        for (int l = 1; l < levels; ++l) {
+            MgLevel& c = L[l];
+            const size_t n = (size_t)c.ntiles * 512u;
+            c.type = (uint8_t*)take(n);
+            c.cell = (uint8_t*)take(n);
+            c.active = (uint8_t*)take(c.ntiles);
+            uint32_t* tiles = (uint32_t*)take(4 * (size_t)c.ntiles);
+            uint32_t* count = (uint32_t*)take(256);
+            c.r = (float*)take(4 * n);
+            c.z = (float*)take(4 * n);
+            c.t = (float*)take(4 * n);
+            c.t2 = (float*)take(4 * n);
+            c.tiles = tiles;
+            c.d_ntiles = count;
+            iota.resize(c.ntiles);
+            for (uint32_t t = 0; t < c.ntiles; ++t) iota[t] = t;
+            E_CUDA(cudaMemcpyAsync(tiles, iota.data(), 4 * (size_t)c.ntiles, cudaMemcpyHostToDevice, e->stream));
+            E_CUDA(cudaMemcpyAsync(count, &c.ntiles, 4, cudaMemcpyHostToDevice, e->stream));
+            E_CUDA(cudaMemsetAsync(c.active, 1, c.ntiles, e->stream));
+            E_CUDA(cudaStreamSynchronize(e->stream));  // iota and ntiles are host locals
+        }
+        e->mg_zn = (float*)take(4 * nc);
+        e->mg_ev = (float*)take(4 * nc);
+        e->mg_wbuf = (float*)take(4 * nc);
+        e->mg_gz = (float*)take(4 * nc);
+        for (auto& p : e->mg_s) p = (float*)take(4 * nc);
+        H.f0 = (float*)take(4 * nc);
+        H.inv_s = (float*)take(256);
+        e->mg_iters = (int*)take(256);
+        H.levels = levels;
+        for (int l = 0; l < levels; ++l) H.L[l] = L[l];
+    }
+    // level 0: the solver's grid and vectors
+    MgLevel& f = H.L[0];
+    f.D = e->D;
+    f.tiles = e->node_keys;
+    f.d_ntiles = e->d_counts;
+    f.type = e->type;
+    f.cell = e->pcg.cell;
+    f.r = e->pcg.r;
+    f.z = e->pcg.z;
+    f.ntiles = (uint32_t)e->ntiles_total;
+    return FLIP_OK;
+}
+// the network's view of the coarsest level (every tile active)
+static LpGrid mg_lp_grid(flip_engine* e, const int* halt) {
+    const MgLevel& c = e->mg.L[e->mg.levels - 1];
+    if (e->mg.levels == 1) {
+        LpGrid G = lp_grid(e, halt);
+        G.r = c.r;
+        return G;
+    }
+    LpGrid G{};
+    G.r = c.r;
+    G.type = c.type;
+    G.tile_active = c.active;
+    G.act_tiles = c.tiles;
+    G.d_nact = c.d_ntiles;
+    G.out_tiles = c.tiles;
+    G.d_nout = c.d_ntiles;
+    G.halt = halt;
+    G.cell = c.cell;
+    G.D = c.D;
+    return G;
+}
+static int mg_coarse_grid(flip_engine* e) {
+    const uint32_t n = e->mg.L[e->mg.levels - 1].ntiles;
+    return e->mg.levels == 1 ? nat_grid(e, 2) : (int)std::min<uint32_t>(n, (uint32_t)e->sms * 2u);
+}
+// kernels of one V-cycle (for the launch count)
+static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
+    return 4u * (uint32_t)(e->mg.levels - 1) + 3u + (network ? 5u : 0u);
+}
+// one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is done)
+static int mg_cycle(flip_engine* e, bool network, const int* halt) {
+    const int grid0 = nat_grid(e, 4);
+    E_TRY(mg_down(e->mg, halt, grid0, e->stream));
+    const float* zn = nullptr;
+    if (network) {
+        const LpGrid G = mg_lp_grid(e, halt);
+        E_TRY(mg_input_scale(e->mg, halt, e->stream));
+        E_TRY(lp_forward_dev(e->lp, G, e->mg.inv_s, e->mg.f0, e->mg_zn, mg_coarse_grid(e), e->stream));
+        zn = e->mg_zn;
+    }
+    E_TRY(mg_coarsest(e->mg, zn, halt, e->stream));
+    E_TRY(mg_up(e->mg, halt, grid0, e->stream));
+    return FLIP_OK;
+}
+// per problem: coarse types and codes (after pcg_init set level 0's codes)
+// and the network's f(0) on the coarsest level
+static int mg_setup_problem(flip_engine* e, bool network) {
+    E_TRY(mg_build(e->mg, nullptr, e->stream));
+    e->launches += 2u * (uint32_t)(e->mg.levels - 1);
+    if (network) {
+        const LpGrid G = mg_lp_grid(e, nullptr);
+        E_TRY(lp_bias_dev(e->lp, G, e->mg.inv_s, e->mg.f0, mg_coarse_grid(e), e->stream));
+        e->launches += 4;
+    }
+    return FLIP_OK;
+}
+
 // ------------------------------------------------------ pressure solves
 static void pcg_state_host(flip_engine* e, double tol, int max_iter, int flexible) {
     PcgState init{};
@@ -855,6 +1002,30 @@ static int nat_fpcg_graph(flip_engine* e, int iters, int max_iter) {
     return FLIP_OK;
 }
 
+static int nat_mgpcg_graph(flip_engine* e, int iters, int max_iter, bool network) {
+    const int limit = loop_limit(max_iter, iters);
+    const int mode = network ? 0 : 1;
+    if (e->mg_graph && e->mg_graph_iters == iters && e->mg_graph_limit == limit && e->mg_graph_coarse == mode)
+        return FLIP_OK;
+    if (e->mg_graph) { cudaGraphExecDestroy(e->mg_graph); e->mg_graph = nullptr; }
+    const int* halt = &e->pcg.st->halt;
+    E_TRY(build_loop_graph(e, [&]() {
+        int rc = FLIP_OK;
+        for (int k = 0; k < iters && rc == FLIP_OK; ++k) {
+            rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            if (rc == FLIP_OK && k == iters - 1)
+                rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            if (rc == FLIP_OK) rc = mg_cycle(e, network, halt);
+            if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream, 0);
+        }
+        return rc;
+    }, limit, &e->mg_graph));
+    e->mg_graph_iters = iters;
+    e->mg_graph_limit = limit;
+    e->mg_graph_coarse = mode;
+    return FLIP_OK;
+}
+
 // one launch of a solve's loop graph; the state comes back once at the end
 static int run_loop(flip_engine* e, cudaGraphExec_t g, uint32_t launches_per_chunk) {
     E_CUDA(cudaGraphLaunch(g, e->stream));
@@ -875,6 +1046,30 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
     if (e->timing || out) E_CUDA(cudaEventRecord(e->solve_ev[0], e->stream));
     bool need_plain = true;
+    if (method == 2) {
+        const bool network = e->P.mg_coarse == 0;
+        E_TRY(mg_ready(e, network));
+        pcg_state_host(e, tol, max_learned, 1);
+        e->h_state->true_every = chunk;
+        e->h_state->next_check = chunk;
+        E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
+        E_TRY(mg_setup_problem(e, network));
+        E_TRY(mg_cycle(e, network, &e->pcg.st->halt));
+        E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream, 0));
+        e->launches += 2u + mg_cycle_launches(e, network);
+        E_TRY(e->mark(9));
+        E_TRY(nat_mgpcg_graph(e, chunk, max_learned, network));
+        E_TRY(run_loop(e, e->mg_graph, (3u + mg_cycle_launches(e, network)) * (uint32_t)chunk + 1u));
+        E_TRY(lp_check_err(e));
+        const PcgState& s = *e->h_state;
+        info.iters = s.iter;
+        double rr = s.true_checks ? s.rr_true : s.rr;
+        info.rel_residual = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
+        info.converged = s.done == 1;
+        need_plain = s.done != 1;
+        if (need_plain) { info.fell_back = 1; U = nullptr; }  // b stays in pcg.b
+    }
     if (method == 1) {
         E_TRY(lp_ready(e));
         pcg_state_host(e, tol, max_learned, 1);
@@ -904,15 +1099,15 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
     if (need_plain) {
         pcg_state_host(e, tol, max_plain, 0);
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
-        const bool w = warm && method != 1;
+        const bool w = warm && method == 0;
         E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
                                   w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
-        if (method != 1) E_TRY(e->mark(9));
+        if (method == 0) E_TRY(e->mark(9));
         E_TRY(nat_pcg_graph(e, chunk, max_plain));
         E_TRY(run_loop(e, e->pcg_graph, 2u * (uint32_t)chunk + 1u));
         const PcgState& s = *e->h_state;
-        if (method == 1) info.plain_iters = s.iter;
+        if (method != 0) info.plain_iters = s.iter;
         else info.iters = s.iter;
         double rr = s.true_checks ? s.rr_true : s.rr;
         info.rel_residual = s.bb > 0.0 ? std::sqrt(rr / s.bb) : 0.0;
@@ -1490,11 +1685,11 @@ extern "C" int flip_poisson_set(flip_engine* e, const uint8_t* type_lin, const f
 extern "C" int flip_poisson_solve(flip_engine* e, int method, double tol, int max_iter, flip_solve_info* info) {
     CHECK_NATIVE("flip_poisson_solve");
     if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_poisson_solve: no problem (flip_poisson_generate/set)");
-    if ((method != 0 && method != 1) || !(tol > 0.0) || max_iter <= 0)
-        return e->fail(FLIP_ERR_ARG, "flip_poisson_solve: method 0/1, tol > 0, max_iter > 0");
+    if (method < 0 || method > 2 || !(tol > 0.0) || max_iter <= 0)
+        return e->fail(FLIP_ERR_ARG, "flip_poisson_solve: method 0/1/2, tol > 0, max_iter > 0");
     flip_solve_info local{};
     e->warm_ok = false;  // pcg.x will hold this problem's solution
-    const int plain = method == 1 ? e->P.pcg_max_iter : max_iter;
+    const int plain = method != 0 ? e->P.pcg_max_iter : max_iter;
     E_TRY(nat_solve(e, nullptr, method, tol, plain, max_iter, &local));
     if (info) *info = local;
     return FLIP_OK;
@@ -1617,6 +1812,73 @@ extern "C" int flip_lp_eval(flip_engine* e, const float* r_lin, const float* e_l
     if (z_lin) {
         E_TRY(nat_launch_lin_tiles_f32(e->pcg.z, e->pcg.p0, e->D, 0, e->stream));
         E_CUDA(cudaMemcpyAsync(z_lin, e->pcg.p0, 4 * e->nslots, cudaMemcpyDeviceToHost, e->stream));
+        e->launches += 1;
+    }
+    E_TRY(lp_read_loss(e, loss));
+    return lp_check_err(e);
+}
+
+// ------------------------------------------- multilevel preconditioner API
+extern "C" int flip_mg_apply(flip_engine* e, const float* r_lin, float* z_lin) {
+    CHECK_NATIVE("flip_mg_apply");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_mg_apply: no problem (flip_poisson_generate/set or a step)");
+    if (!r_lin || !z_lin) return e->fail(FLIP_ERR_ARG, "flip_mg_apply: null residual or output");
+    const bool network = e->P.mg_coarse == 0;
+    E_TRY(mg_ready(e, network));
+    pcg_state_host(e, 0.0, 0, 0);
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));  // cell codes
+    e->solution_fresh = false;
+    e->warm_ok = false;
+    E_CUDA(cudaMemcpyAsync(e->pcg.p0, r_lin, 4 * e->nslots, cudaMemcpyHostToDevice, e->stream));
+    E_TRY(nat_launch_lin_tiles_f32(e->pcg.p0, e->pcg.r, e->D, 1, e->stream));
+    E_TRY(mg_setup_problem(e, network));
+    E_TRY(mg_cycle(e, network, nullptr));
+    E_TRY(nat_launch_lin_tiles_f32(e->pcg.z, e->pcg.p0, e->D, 0, e->stream));
+    E_CUDA(cudaMemcpyAsync(z_lin, e->pcg.p0, 4 * e->nslots, cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    e->launches += 3u + mg_cycle_launches(e, network);
+    return lp_check_err(e);
+}
+
+extern "C" int flip_mg_train_step(flip_engine* e, int sample, float lr, double* loss) {
+    CHECK_NATIVE("flip_mg_train_step");
+    if (!e->poisson_ready) return e->fail(FLIP_ERR_STATE, "flip_mg_train_step: no problem (flip_poisson_generate/set or a step)");
+    if (sample < -1 || sample > 100000 || !(lr >= 0.0f)) return e->fail(FLIP_ERR_ARG, "flip_mg_train_step: bad arguments");
+    E_TRY(mg_ready(e, true));
+    pcg_state_host(e, 0.0, sample + 1, 0);
+    e->h_state->true_every = 0;
+    E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, nullU, e->type, e->pcg, e->stream));  // codes, r = b
+    e->solution_fresh = false;  // pcg.x will hold x_k
+    e->warm_ok = false;
+    E_TRY(mg_setup_problem(e, true));
+    const MgLevel& c = e->mg.L[e->mg.levels - 1];
+    const LpGrid G = mg_lp_grid(e, nullptr);
+    const int grid = mg_coarse_grid(e);
+    if (sample >= 0) {
+        // the coarsest right-hand side that one V-cycle makes of the residual
+        // after k Jacobi-PCG iterations, and its coarse solution (one-CTA CG)
+        for (int k = 0; k < sample; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_TRY(mg_down(e->mg, nullptr, nat_grid(e, 4), e->stream));
+        E_TRY(mg_cg(c, c.r, e->mg_ev, e->mg_s[0], e->mg_s[1], e->mg_s[2], 1e-6, 4000, e->mg_iters, e->stream));
+        e->launches += 2u * (uint32_t)sample + 3u * (uint32_t)(e->mg.levels - 1) + 1u;
+    } else {
+        // white noise e on the coarsest fluid cells and r = A e
+        E_TRY(lp_noise_sample(G, 0x9E3779B97F4A7C15ull + e->noise_counter++, e->mg_ev, c.r, grid, e->stream));
+        e->launches += 2;
+    }
+    E_TRY(mg_input_scale(e->mg, nullptr, e->stream));
+    E_TRY(lp_forward_dev(e->lp, G, e->mg.inv_s, e->mg.f0, e->mg_zn, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, 3 * sizeof(double), e->stream));
+    E_TRY(lp_loss_grad(G, e->mg_zn, e->mg_ev, e->mg_wbuf, e->mg_gz, e->lp_scalar, grid, e->stream));
+    E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));
+    E_TRY(lp_backward_dev(e->lp, G, e->mg.inv_s, e->mg_gz, grid, e->stream));
+    e->launches += 1u + 4u + 2u + 14u;
+    if (lr > 0.0f) {
+        E_TRY(lp_adam(e->lp, lr, e->stream));
         e->launches += 1;
     }
     E_TRY(lp_read_loss(e, loss));

@@ -927,7 +927,8 @@ __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __rest
 
 // flexible CG (Notay's FCG(1), the same recurrence as Polak-Ribiere PCG)
 // with the preconditioner M(r) = N(r) + D^-1 r.  This kernel adds the Jacobi
-// term to the network output z in place.  The new direction p' = z + beta p
+// term to the network output z in place (jacobi = 1; the multilevel
+// preconditioner's z is complete).  The new direction p' = z + beta p
 // is A-orthogonal to p for beta = -z.q / p.q (q = A p), and alpha = r.z /
 // p'.q' is the exact line search along p' (r is orthogonal to p).  A nonlinear N may give r.z < 0;
 // alpha is then negative and the step still minimises the A-norm error along
@@ -936,8 +937,8 @@ __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __rest
 __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __restrict__ tiles,
                                                            const uint32_t* __restrict__ d_ntiles, const float* __restrict__ r,
                                                            float* __restrict__ z, const float* __restrict__ q,
-                                                           const uint8_t* __restrict__ cell, int init, PcgState* st,
-                                                           double* partials) {
+                                                           const uint8_t* __restrict__ cell, int init, int jacobi,
+                                                           PcgState* st, double* partials) {
     if (st->halt) return;
     __shared__ double sh[32];
     const uint32_t nquads = *d_ntiles * 128u;
@@ -957,7 +958,7 @@ __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __rest
             const uint8_t c = (uint8_t)(c4 >> (8 * m));
             if (!(c & kCellFluid)) continue;
             const float d = (float)(c & 7u);
-            zv[m] = d > 0.0f ? zv[m] + rv[m] / d : zv[m];  // M(r) = N(r) + D^-1 r
+            if (jacobi) zv[m] = d > 0.0f ? zv[m] + rv[m] / d : zv[m];  // M(r) = N(r) + D^-1 r
             rz += (double)rv[m] * (double)zv[m];
             zq += (double)zv[m] * (double)qv[m];
         }
@@ -1148,8 +1149,9 @@ int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_nt
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s) {
-    fpcg_dot_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, B.r, B.z, B.q, B.cell, init, B.st, B.partials);
+int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s,
+                        int jacobi) {
+    fpcg_dot_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, B.r, B.z, B.q, B.cell, init, jacobi, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -89,7 +89,10 @@ int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const N
 // flexible PCG: direction from z (B.z), and the r.z / z.q reduction giving beta
 int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                                      cudaStream_t s);
-int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s);
+// jacobi = 1 adds D^-1 r to z first (the network preconditioner's Jacobi
+// term); the multilevel preconditioner's z is complete (jacobi = 0)
+int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuffers& B, int init, cudaStream_t s,
+                        int jacobi = 1);
 // one PCG iteration: fused direction update + matvec (+ p.Ap), then the
 // x/r update (+ r.r, r.z); the two p buffers alternate under device control
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,

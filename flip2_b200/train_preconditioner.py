@@ -14,9 +14,17 @@ error of x_k after k Jacobi-PCG iterations from x = 0 (k drawn from 0, 2, 5,
 white-noise errors e with r = A e.  The loss is the A-norm error of M(r) as
 an estimate of e, relative to |e|_A; Adam.
 
+With --mg the network is trained as the coarsest-level solve of the
+multilevel preconditioner (pressure_method 2): a sample is the coarsest
+right-hand side that one V-cycle makes of the residual after k Jacobi-PCG
+iterations (k as above; its coarse solution from CG on the coarsest grid),
+or a white-noise coarse error e with r = A e, and the loss is the same
+A-norm error on the coarsest grid.
+
 Evaluation: Jacobi-PCG against learned FPCG (tol 1e-6) on held-out generated
 problems and on dam-break steps, iterations and device milliseconds, one
-JSON line per problem kind.
+JSON line per problem kind; with --mg also the same V-cycle without the
+network.
 """
 import argparse
 import json
@@ -38,12 +46,12 @@ def make_engine(cells, pressure_method=0):
     return P, pos, vel
 
 
-def evaluate(P, cells, seeds, tol=1e-6, max_iter=100):
+def evaluate(P, cells, seeds, tol=1e-6, max_iter=100, method=1):
     rows = []
     for s in seeds:
         P.poisson_generate(seed=s)
         a = P.poisson_solve(0, tol, 20000)
-        b = P.poisson_solve(1, tol, max_iter)
+        b = P.poisson_solve(method, tol, max_iter)
         rows.append((a.iters, a.ms, b.iters, b.ms, b.fell_back, b.rel_residual))
     return rows
 
@@ -63,7 +71,9 @@ def main():
     ap.add_argument("--noise", type=float, default=0.3, help="fraction of white-noise error samples")
     ap.add_argument("--eval-max-iter", type=int, default=100, help="learned FCG cap in the evaluation")
     ap.add_argument("--eval-dam-steps", type=int, default=40, help="dam-break steps per method in the evaluation")
+    ap.add_argument("--mg", action="store_true", help="train the coarsest solve of the multilevel preconditioner")
     args = ap.parse_args()
+    method = 2 if args.mg else 1
 
     P, pos, vel = make_engine(args.cells)
     if args.init:
@@ -89,7 +99,7 @@ def main():
         lr = args.lr * (args.lr_final / args.lr) ** frac
         for _ in range(args.steps_per_problem):
             k = int(SAMPLE_ITERS[rng.integers(len(SAMPLE_ITERS))]) if rng.random() >= args.noise else -1
-            losses.append(P.lp_train_step(k, lr))
+            losses.append(P.mg_train_step(k, lr) if args.mg else P.lp_train_step(k, lr))
             step += 1
         if prob % 50 == 0:
             print(json.dumps({"step": step, "problems": prob, "loss": float(np.mean(losses[-50:])), "lr": lr,
@@ -100,16 +110,27 @@ def main():
     print(json.dumps({"trained_steps": step, "problems": prob, "seconds": round(train_s, 1),
                       "final_loss": float(np.mean(losses[-100:])), "out": args.out}), flush=True)
 
-    rows = evaluate(P, args.cells, range(900_000, 900_000 + args.eval_problems), max_iter=args.eval_max_iter)
+    seeds = range(900_000, 900_000 + args.eval_problems)
+    rows = evaluate(P, args.cells, seeds, max_iter=args.eval_max_iter, method=method)
     a = np.array(rows)
-    print(json.dumps({"eval": "generated", "cells": args.cells, "jacobi_iters": a[:, 0].tolist(),
+    print(json.dumps({"eval": "generated", "cells": args.cells, "method": method, "jacobi_iters": a[:, 0].tolist(),
                       "jacobi_ms": np.round(a[:, 1], 2).tolist(), "learned_iters": a[:, 2].tolist(),
                       "learned_ms": np.round(a[:, 3], 2).tolist(), "fell_back": int(a[:, 4].sum())}), flush=True)
     P.close()
+    if args.mg:
+        # the same V-cycle without the network
+        Q = Particles(1, mode=MODE_NATIVE, params=default_params(MODE_NATIVE, mg_coarse=1))
+        R = args.cells // 4
+        Q.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / args.cells)
+        a = np.array(evaluate(Q, args.cells, seeds, max_iter=args.eval_max_iter, method=2))
+        print(json.dumps({"eval": "generated", "cells": args.cells, "method": 2, "network": False,
+                          "iters": a[:, 2].tolist(), "ms": np.round(a[:, 3], 2).tolist(),
+                          "fell_back": int(a[:, 4].sum())}), flush=True)
+        Q.close()
     # dam-break steps with each method
-    for method in ((0, 1) if args.eval_dam_steps > 0 else ()):
-        Q, _, _ = make_engine(args.cells, pressure_method=method)
-        if method:
+    for m in ((0, method) if args.eval_dam_steps > 0 else ()):
+        Q, _, _ = make_engine(args.cells, pressure_method=m)
+        if m:
             Q.lp_set_weights(w)
         Q.set_timing(True)
         its, ms, fb = [], [], 0
@@ -119,7 +140,7 @@ def main():
             its.append(si.iters + si.plain_iters)
             ms.append(si.ms)
             fb += si.fell_back
-        print(json.dumps({"eval": "dam_break", "cells": args.cells, "method": method, "iters": its,
+        print(json.dumps({"eval": "dam_break", "cells": args.cells, "method": m, "iters": its,
                           "ms": np.round(ms, 2).tolist(), "fell_back": fb}), flush=True)
         Q.close()
 

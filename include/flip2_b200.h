@@ -161,7 +161,10 @@ typedef struct {
     int32_t true_residual_every; /* NATIVE: FP64 r = b - A x recomputation period   */
     int32_t permute_velocities;  /* REFERENCE: 0 = keep the reference's order (Q5)  */
     int32_t device;              /* CUDA device ordinal                             */
-    int32_t pressure_method;     /* NATIVE: 0 Jacobi-PCG, 1 learned-preconditioned FPCG */
+    int32_t pressure_method;     /* NATIVE: 0 Jacobi-PCG; 1 FPCG preconditioned by the
+                                    network on the solver's grid; 2 FPCG preconditioned
+                                    by a multigrid V-cycle whose coarsest level (16^3 or
+                                    less) the network solves                          */
     double max_substep_dt;       /* NATIVE: largest sub-step of solveFrame (1/240)  */
     int32_t learned_max_iter;    /* NATIVE: FPCG cap before the Jacobi-PCG restart   */
     int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers on CUDA
@@ -169,7 +172,9 @@ typedef struct {
     int32_t pcg_warm_start;      /* NATIVE: 1 (default) starts each step's Jacobi-PCG
                                     from the previous step's pressure on the cells
                                     fluid in both; the stop test stays |r| <= tol |b| */
-    int32_t reserved[1];
+    int32_t mg_coarse;           /* NATIVE, pressure_method 2: 0 (default) solves the
+                                    coarsest level with the network, 1 with Jacobi
+                                    sweeps only (the same V-cycle without the network) */
 } flip_params;
 
 /* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */
@@ -303,7 +308,10 @@ typedef struct {
  * its pressure problem stays in place for flip_poisson_solve,
  * flip_lp_train_step and flip_lp_eval until the next step. */
 int flip_get_solve_info(flip_engine* e, flip_solve_info* out);
-/* method 0: Jacobi-PCG; 1: learned FPCG with Jacobi-PCG fallback */
+/* method 0: Jacobi-PCG; 1: FPCG with the network preconditioner; 2: FPCG
+ * with the multilevel preconditioner (flip_params.mg_coarse picks the
+ * coarsest solve).  Methods 1 and 2 restart Jacobi-PCG from x = 0 when they
+ * miss tol within max_iter or stall. */
 int flip_poisson_solve(flip_engine* e, int method, double tol, int max_iter, flip_solve_info* info);
 /* solution (FP64) in x-fastest order */
 int flip_poisson_read_solution(flip_engine* e, double* x_lin);
@@ -320,6 +328,20 @@ int flip_lp_train_step(flip_engine* e, int sample, float lr, double* loss);
  * out (x fastest, may be NULL), the loss, and with want_grad the weight
  * gradient (flip_lp_get_grad) without updating the weights */
 int flip_lp_eval(flip_engine* e, const float* r_lin, const float* e_lin, float* z_lin, double* loss, int want_grad);
+
+/* Multilevel preconditioner (pressure_method 2).  No reference counterpart.
+ * The network's weights are the ones above; here they act on the coarsest
+ * level of the V-cycle.
+ * One V-cycle z = M(r) on the current problem, r and z x fastest (for
+ * checks against a CPU restatement). */
+int flip_mg_apply(flip_engine* e, const float* r_lin, float* z_lin);
+/* one training step of the network as the coarsest solve: sample k >= 0
+ * takes the coarsest right-hand side that a V-cycle makes of the residual
+ * after k Jacobi-PCG iterations on the current problem, with its coarse
+ * solution from CG; sample -1 a white-noise coarse error e and r = A e.
+ * Loss as flip_lp_train_step's (A-norm error of N(r) + D^-1 r on the
+ * coarsest level); lr = 0 computes loss and gradient without a step. */
+int flip_mg_train_step(flip_engine* e, int sample, float lr, double* loss);
 
 typedef struct {
     uint32_t nodes;          /* occupied root cells (REFERENCE) / tiles (NATIVE)   */

@@ -1264,3 +1264,221 @@ int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, co
     free(r); free(p); free(q); free(zd); free(rf); free(zf); free(dinv);
     return it;
 }
+
+/* ============================== multilevel preconditioner (method 2) ====
+ * One V-cycle over 2x coarsened grids with the network as the coarsest
+ * solve (no reference counterpart; the GPU form is flip2_b200/csrc/mg.cu).
+ * Level l+1 has ceil(n_l / 2) cells per axis, padded to a multiple of 8 with
+ * solid cells, until every axis has at most 16.  A coarse cell is air if any
+ * child is air, else fluid if any child is fluid, else solid.  Damped Jacobi
+ * (omega = 2/3): two sweeps from zero before the restriction (1/2 x the sum
+ * of the 8 children's residuals), two after adding the parent's correction;
+ * the coarsest level starts from N(r) + D^-1 r (network) or omega D^-1 r
+ * (mode 1) and takes two sweeps.  FP64 apart from the network. */
+#define MG_MAX_LEVELS 8
+#define MG_COARSEST 16
+#define MG_OMEGA (2.0 / 3.0)
+
+typedef struct {
+    lp_dims D; /* padded */
+    int ex, ey, ez;
+    uint8_t* type;
+    double *dinv, *r, *z, *t;
+} mg_level;
+
+static int mg_levels_plan(int nx, int ny, int nz, mg_level* L) {
+    int ex = nx, ey = ny, ez = nz, n = 0;
+    while (n < MG_MAX_LEVELS) {
+        mg_level* l = &L[n];
+        memset(l, 0, sizeof(*l));
+        l->ex = ex; l->ey = ey; l->ez = ez;
+        l->D.nx = (ex + 7) & ~7; l->D.ny = (ey + 7) & ~7; l->D.nz = (ez + 7) & ~7;
+        l->D.nc = (int64_t)l->D.nx * l->D.ny * l->D.nz;
+        ++n;
+        if (ex <= MG_COARSEST && ey <= MG_COARSEST && ez <= MG_COARSEST) break;
+        ex = (ex + 1) / 2; ey = (ey + 1) / 2; ez = (ez + 1) / 2;
+    }
+    return n;
+}
+
+static void mg_coarsen(const mg_level* F, mg_level* C) {
+    for (int K = 0; K < C->D.nz; ++K)
+        for (int J = 0; J < C->D.ny; ++J)
+            for (int I = 0; I < C->D.nx; ++I) {
+                uint8_t t = NAT_SOLID;
+                if (I < C->ex && J < C->ey && K < C->ez) {
+                    int air = 0, fluid = 0;
+                    for (int c = 0; c < 8; ++c) {
+                        int i = 2 * I + (c & 1), j = 2 * J + ((c >> 1) & 1), k = 2 * K + (c >> 2);
+                        if (i >= F->ex || j >= F->ey || k >= F->ez) continue;
+                        uint8_t ft = F->type[lp_at(&F->D, i, j, k)];
+                        air |= ft == NAT_AIR;
+                        fluid |= ft == NAT_FLUID;
+                    }
+                    t = air ? NAT_AIR : (fluid ? NAT_FLUID : NAT_SOLID);
+                }
+                C->type[lp_at(&C->D, I, J, K)] = t;
+            }
+}
+
+/* out = in + omega D^-1 (r - A in) on the fluid cells of L */
+static void mg_sweep(const mg_level* L, const double* in, double* out, double* tmp) {
+    lp_apply_A(&L->D, L->type, in, tmp);
+    for (int64_t v = 0; v < L->D.nc; ++v)
+        out[v] = L->type[v] == NAT_FLUID ? in[v] + MG_OMEGA * L->dinv[v] * (L->r[v] - tmp[v]) : 0.0;
+}
+
+static void mg_vcycle(mg_level* L, int levels, int l, const float* w, const int* dil, int round_bf16, int mode) {
+    mg_level* f = &L[l];
+    const int64_t nc = f->D.nc;
+    double* tmp = (double*)malloc(sizeof(double) * nc);
+    double* t2 = (double*)malloc(sizeof(double) * nc);
+    if (l == levels - 1) {
+        if (mode == 0) {
+            float* rf = (float*)malloc(sizeof(float) * nc);
+            float* zf = (float*)malloc(sizeof(float) * nc);
+            for (int64_t v = 0; v < nc; ++v) rf[v] = (float)f->r[v];
+            orc_lp_forward(f->D.nx, f->D.ny, f->D.nz, f->type, rf, w, dil, round_bf16, zf, NULL);
+            for (int64_t v = 0; v < nc; ++v) t2[v] = f->type[v] == NAT_FLUID ? (double)zf[v] + f->dinv[v] * f->r[v] : 0.0;
+            free(rf);
+            free(zf);
+        } else {
+            for (int64_t v = 0; v < nc; ++v) t2[v] = f->type[v] == NAT_FLUID ? MG_OMEGA * f->dinv[v] * f->r[v] : 0.0;
+        }
+        mg_sweep(f, t2, f->t, tmp);
+        mg_sweep(f, f->t, f->z, tmp);
+    } else {
+        mg_level* c = &L[l + 1];
+        for (int64_t v = 0; v < nc; ++v) t2[v] = f->type[v] == NAT_FLUID ? MG_OMEGA * f->dinv[v] * f->r[v] : 0.0;
+        mg_sweep(f, t2, f->t, tmp);
+        lp_apply_A(&f->D, f->type, f->t, tmp);
+        for (int64_t v = 0; v < c->D.nc; ++v) c->r[v] = 0.0;
+        for (int k = 0; k < f->D.nz; ++k)
+            for (int j = 0; j < f->D.ny; ++j)
+                for (int i = 0; i < f->D.nx; ++i) {
+                    int64_t v = lp_at(&f->D, i, j, k);
+                    if (f->type[v] != NAT_FLUID) continue;
+                    int64_t p = lp_at(&c->D, i >> 1, j >> 1, k >> 1);
+                    if (c->type[p] == NAT_FLUID) c->r[p] += 0.5 * (f->r[v] - tmp[v]);
+                }
+        mg_vcycle(L, levels, l + 1, w, dil, round_bf16, mode);
+        for (int k = 0; k < f->D.nz; ++k)
+            for (int j = 0; j < f->D.ny; ++j)
+                for (int i = 0; i < f->D.nx; ++i) {
+                    int64_t v = lp_at(&f->D, i, j, k);
+                    t2[v] = f->type[v] == NAT_FLUID ? f->t[v] + c->z[lp_at(&c->D, i >> 1, j >> 1, k >> 1)] : 0.0;
+                }
+        mg_sweep(f, t2, f->t, tmp);
+        mg_sweep(f, f->t, f->z, tmp);
+    }
+    free(tmp);
+    free(t2);
+}
+
+typedef struct {
+    int levels;
+    mg_level L[MG_MAX_LEVELS];
+} mg_hier;
+
+static void mg_hier_init(mg_hier* H, int nx, int ny, int nz, const uint8_t* type) {
+    H->levels = mg_levels_plan(nx, ny, nz, H->L);
+    for (int l = 0; l < H->levels; ++l) {
+        mg_level* c = &H->L[l];
+        const int64_t nc = c->D.nc;
+        c->type = (uint8_t*)malloc(nc);
+        c->dinv = (double*)malloc(sizeof(double) * nc);
+        c->r = (double*)calloc((size_t)nc, 8);
+        c->z = (double*)calloc((size_t)nc, 8);
+        c->t = (double*)calloc((size_t)nc, 8);
+        if (l == 0) memcpy(c->type, type, (size_t)nc);
+        else mg_coarsen(&H->L[l - 1], c);
+        lp_dinv(&c->D, c->type, c->dinv);
+    }
+}
+static void mg_hier_free(mg_hier* H) {
+    for (int l = 0; l < H->levels; ++l) {
+        mg_level* c = &H->L[l];
+        free(c->type); free(c->dinv); free(c->r); free(c->z); free(c->t);
+    }
+}
+
+int orc_mg_levels(int nx, int ny, int nz, int* dims) {
+    mg_level L[MG_MAX_LEVELS];
+    int n = mg_levels_plan(nx, ny, nz, L);
+    for (int l = 0; l < n && dims; ++l) {
+        dims[3 * l] = L[l].D.nx; dims[3 * l + 1] = L[l].D.ny; dims[3 * l + 2] = L[l].D.nz;
+    }
+    return n;
+}
+
+void orc_mg_apply(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                  int round_bf16, int mode, double* z) {
+    mg_hier H;
+    mg_hier_init(&H, nx, ny, nz, type);
+    const int64_t nc = H.L[0].D.nc;
+    for (int64_t v = 0; v < nc; ++v) H.L[0].r[v] = type[v] == NAT_FLUID ? (double)r[v] : 0.0;
+    mg_vcycle(H.L, H.levels, 0, w, dil, round_bf16, mode);
+    memcpy(z, H.L[0].z, sizeof(double) * nc);
+    mg_hier_free(&H);
+}
+
+/* FCG(1) with the V-cycle as preconditioner; the same loop and stagnation
+ * rule as orc_lp_fpcg */
+int orc_mg_fcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
+               int round_bf16, int mode, double tol, int max_iter, double* x, double* rel_res) {
+    lp_dims D = {nx, ny, nz, (int64_t)nx * ny * nz};
+    const int64_t nc = D.nc;
+    mg_hier H;
+    mg_hier_init(&H, nx, ny, nz, type);
+    double *r = (double*)calloc((size_t)nc, 8), *p = (double*)calloc((size_t)nc, 8), *q = (double*)calloc((size_t)nc, 8);
+    double bb = 0.0;
+    for (int64_t v = 0; v < nc; ++v) {
+        x[v] = 0.0;
+        r[v] = type[v] == NAT_FLUID ? b[v] : 0.0;
+        bb += r[v] * r[v];
+    }
+    const double bn = sqrt(bb);
+    int it = 0;
+    double pq_prev = 0.0, rr_check = bb;
+    if (bn > 0.0) {
+        for (it = 1; it <= max_iter + 1; ++it) {
+            /* the GPU's V-cycle reads r in FP32 */
+            for (int64_t v = 0; v < nc; ++v) H.L[0].r[v] = (double)(float)r[v];
+            mg_vcycle(H.L, H.levels, 0, w, dil, round_bf16, mode);
+            const double* zd = H.L[0].z;
+            double rzn = 0.0, zq = 0.0;
+            for (int64_t v = 0; v < nc; ++v) {
+                rzn += r[v] * zd[v];
+                zq += zd[v] * q[v];
+            }
+            if (rzn == 0.0 || !isfinite(rzn)) break;
+            const double beta = it == 1 ? 0.0 : -zq / pq_prev;
+            for (int64_t v = 0; v < nc; ++v) p[v] = zd[v] + beta * p[v];
+            lp_apply_A(&D, type, p, q);
+            double pq = 0.0;
+            for (int64_t v = 0; v < nc; ++v) pq += p[v] * q[v];
+            if (!(pq > 0.0)) break;
+            const double alpha = rzn / pq;
+            pq_prev = pq;
+            double rr = 0.0;
+            for (int64_t v = 0; v < nc; ++v) {
+                x[v] += alpha * p[v];
+                r[v] -= alpha * q[v];
+                rr += r[v] * r[v];
+            }
+            if (sqrt(rr) <= tol * bn) break;
+            if (it % 16 == 0) {
+                if (rr > 0.81 * rr_check) { it = max_iter + 1; break; }
+                rr_check = rr;
+            }
+        }
+    }
+    lp_apply_A(&D, type, x, q);
+    double rr = 0.0;
+    for (int64_t v = 0; v < nc; ++v)
+        if (type[v] == NAT_FLUID) { double d = b[v] - q[v]; rr += d * d; }
+    if (rel_res) *rel_res = bn > 0.0 ? sqrt(rr) / bn : 0.0;
+    free(r); free(p); free(q);
+    mg_hier_free(&H);
+    return it;
+}

@@ -174,6 +174,16 @@ double orc_lp_loss_grad(int nx, int ny, int nz, const uint8_t* type, const float
 int orc_lp_fpcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
                 int round_bf16, double tol, int max_iter, double* x, double* rel_res);
 
+/* Multilevel preconditioner (pressure_method 2, no reference counterpart):
+ * levels of the hierarchy below an nx x ny x nz grid (padded dims of each
+ * level into dims[3 l ..]), one V-cycle z = M(r) (mode 0: the network solves
+ * the coarsest level, 1: Jacobi sweeps only), and FCG with it. */
+int orc_mg_levels(int nx, int ny, int nz, int* dims);
+void orc_mg_apply(int nx, int ny, int nz, const uint8_t* type, const float* r, const float* w, const int* dil,
+                  int round_bf16, int mode, double* z);
+int orc_mg_fcg(int nx, int ny, int nz, const uint8_t* type, const double* b, const float* w, const int* dil,
+               int round_bf16, int mode, double tol, int max_iter, double* x, double* rel_res);
+
 #ifdef __cplusplus
 }
 #endif

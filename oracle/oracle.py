@@ -82,6 +82,9 @@ def lib():
             "orc_lp_forward": (None, [I, I, I, u8p, f32p, f32p, i32p, I, f32p, C.POINTER(D)]),
             "orc_lp_loss_grad": (D, [I, I, I, u8p, f32p, f32p, f32p, i32p, I, f32p, f64p]),
             "orc_lp_fpcg": (I, [I, I, I, u8p, f64p, f32p, i32p, I, D, I, f64p, C.POINTER(D)]),
+            "orc_mg_levels": (I, [I, I, I, i32p]),
+            "orc_mg_apply": (None, [I, I, I, u8p, f32p, f32p, i32p, I, I, f64p]),
+            "orc_mg_fcg": (I, [I, I, I, u8p, f64p, f32p, i32p, I, I, D, I, f64p, C.POINTER(D)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -296,4 +299,31 @@ def lp_fpcg(type_, b, w, shape, tol=1e-6, max_iter=1000, dil=LP_DIL, round_bf16=
     it = lib().orc_lp_fpcg(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(), np.ascontiguousarray(b, np.float64).ravel(),
                            np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16), tol,
                            max_iter, x, C.byref(rr))
+    return x, it, rr.value
+
+
+def mg_levels(shape):
+    """Padded (nx, ny, nz) of each level of the multilevel preconditioner."""
+    dims = np.zeros(3 * 8, np.int32)
+    n = lib().orc_mg_levels(shape[0], shape[1], shape[2], dims)
+    return [tuple(int(v) for v in dims[3 * l:3 * l + 3]) for l in range(n)]
+
+
+def mg_apply(type_, r, w, shape, mode=0, dil=LP_DIL, round_bf16=True):
+    """One V-cycle z = M(r) of the multilevel preconditioner (FP64 apart from the network)."""
+    nx, ny, nz = shape
+    z = np.empty(nx * ny * nz, np.float64)
+    lib().orc_mg_apply(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(), np.ascontiguousarray(r, np.float32).ravel(),
+                       np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16), int(mode), z)
+    return z
+
+
+def mg_fcg(type_, b, w, shape, mode=0, tol=1e-6, max_iter=1000, dil=LP_DIL, round_bf16=True):
+    """FCG with the multilevel preconditioner: (x, iterations, relative residual)."""
+    nx, ny, nz = shape
+    x = np.zeros(nx * ny * nz, np.float64)
+    rr = C.c_double(0.0)
+    it = lib().orc_mg_fcg(nx, ny, nz, np.ascontiguousarray(type_, np.uint8).ravel(), np.ascontiguousarray(b, np.float64).ravel(),
+                          np.ascontiguousarray(w, np.float32), np.ascontiguousarray(dil, np.int32), int(round_bf16), int(mode),
+                          tol, max_iter, x, C.byref(rr))
     return x, it, rr.value
