@@ -854,10 +854,10 @@ static int mg_ready(flip_engine* e, bool network) {
         MgLevel L[kMgMaxLevels];
         const int levels = mg_plan(e->D.nx, e->D.ny, e->D.nz, e->D.h, L, kMgMaxLevels);
         const size_t fine = (size_t)e->nslots;
-        size_t total = 2 * al(4 * fine);
+        size_t total = al(4 * fine);
         for (int l = 1; l < levels; ++l) {
             const size_t n = (size_t)L[l].ntiles * 512u;
-            total += 2 * al(n) + al(L[l].ntiles) + al(4 * (size_t)L[l].ntiles) + 4 * al(4 * n) + 256;
+            total += 2 * al(n) + al(L[l].ntiles) + al(4 * (size_t)L[l].ntiles) + 3 * al(4 * n) + 256;
         }
         const size_t nc = (size_t)L[levels - 1].ntiles * 512u;
         total += 8 * al(4 * nc) + 1024;
@@ -866,7 +866,6 @@ static int mg_ready(flip_engine* e, bool network) {
         char* q = e->mg_arena;
         auto take = [&](size_t b) { char* r = q; q += al(b); return r; };
         L[0].t = (float*)take(4 * fine);
-        L[0].t2 = (float*)take(4 * fine);
         std::vector<uint32_t> iota;
         for (int l = 1; l < levels; ++l) {
             MgLevel& c = L[l];
@@ -879,7 +878,6 @@ static int mg_ready(flip_engine* e, bool network) {
             c.r = (float*)take(4 * n);
             c.z = (float*)take(4 * n);
             c.t = (float*)take(4 * n);
-            c.t2 = (float*)take(4 * n);
             c.tiles = tiles;
             c.d_ntiles = count;
             iota.resize(c.ntiles);
@@ -939,7 +937,7 @@ static int mg_coarse_grid(flip_engine* e) {
 }
 // kernels of one V-cycle (for the launch count)
 static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
-    return 4u * (uint32_t)(e->mg.levels - 1) + 3u + (network ? 5u : 0u);
+    return 2u * (uint32_t)(e->mg.levels - 1) + 1u + (network ? 5u : 0u);
 }
 // one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is done)
 static int mg_cycle(flip_engine* e, bool network, const int* halt) {
@@ -1864,7 +1862,7 @@ extern "C" int flip_mg_train_step(flip_engine* e, int sample, float lr, double* 
         for (int k = 0; k < sample; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
         E_TRY(mg_down(e->mg, nullptr, nat_grid(e, 4), e->stream));
         E_TRY(mg_cg(c, c.r, e->mg_ev, e->mg_s[0], e->mg_s[1], e->mg_s[2], 1e-6, 4000, e->mg_iters, e->stream));
-        e->launches += 2u * (uint32_t)sample + 3u * (uint32_t)(e->mg.levels - 1) + 1u;
+        e->launches += 2u * (uint32_t)sample + (uint32_t)(e->mg.levels - 1) + 1u;
     } else {
         // white noise e on the coarsest fluid cells and r = A e
         E_TRY(lp_noise_sample(G, 0x9E3779B97F4A7C15ull + e->noise_counter++, e->mg_ev, c.r, grid, e->stream));

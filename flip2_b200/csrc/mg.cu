@@ -91,120 +91,260 @@ __global__ void __launch_bounds__(512) mg_codes_kernel(MgLevel C, const int* hal
 }
 
 // ------------------------------------------------------------ smoothing
-// pre-smoothing from zero: t1 = w D^-1 r, t = t1 + w D^-1 (r - A t1)
-__global__ void __launch_bounds__(512) mg_pre_kernel(MgLevel L, const int* halt) {
-    if (mg_halted(halt)) return;
-    const uint32_t n = *L.d_ntiles;
-    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
-        const uint32_t key = L.tiles[tt];
-        const uint32_t s = (key << 9) | threadIdx.x;
-        const uint8_t c = L.cell[s];
-        float out = 0.0f;
-        if (c & kCellFluid) {
-            int i, j, k;
-            mg_cell_of(key, threadIdx.x, L.D, i, j, k);
-            const float di = mg_dinv(c), r = L.r[s];
-            const float t1 = kMgOmega * di * r;
-            const float nb = mg_nb_sum(i, j, k, L.D, L.cell, [&](uint32_t u) { return kMgOmega * mg_dinv(L.cell[u]) * L.r[u]; });
-            const float at = (float)(c & 7u) * t1 - nb;
-            out = t1 + kMgOmega * di * (r - at);
-        }
-        L.t[s] = out;
+// The V-cycle's smoothing runs as two kernels per level.  Each CTA stages a
+// 12^3 box of its tile and a 2-cell halo in shared memory (cell codes, r and
+// the vector the sweeps start from); the first sweep is evaluated on the
+// 10^3 box of the tile and a 1-cell halo, the second (or the residual) on
+// the tile.  A neighbour that is not fluid contributes nothing, so halo cells
+// outside the grid or in tiles off the level's list (code 0) need no test
+// beyond the code.
+constexpr int kB12 = 12 * 12 * 12;
+constexpr int kB10 = 10 * 10 * 10;
+__device__ __forceinline__ void mg_origin(uint32_t key, const NatDims& D, int& ox, int& oy, int& oz) {
+    const uint32_t tyz = key / (uint32_t)D.tx;
+    ox = 8 * (int)(key - tyz * (uint32_t)D.tx);
+    oy = 8 * (int)(tyz % (uint32_t)D.ty);
+    oz = 8 * (int)(tyz / (uint32_t)D.ty);
+}
+// sum of the fluid neighbours' values of box cell b (row strides sx, sy, sz
+// = 1, W, W*W of a W-wide box), codes from the 12^3 box at b12
+__device__ __forceinline__ float mg_box_nb(const uint8_t* cb, int b12, const float* vb, int b, int W) {
+    const int W2 = W * W;
+    float s = 0.0f;
+    if (cb[b12 - 1] & kCellFluid) s += vb[b - 1];
+    if (cb[b12 + 1] & kCellFluid) s += vb[b + 1];
+    if (cb[b12 - 12] & kCellFluid) s += vb[b - W];
+    if (cb[b12 + 12] & kCellFluid) s += vb[b + W];
+    if (cb[b12 - 144] & kCellFluid) s += vb[b - W2];
+    if (cb[b12 + 144] & kCellFluid) s += vb[b + W2];
+    return s;
+}
+__device__ __forceinline__ int b12_of10(int v) {  // 10^3 box index -> 12^3 box index
+    const int x = v % 10, y = (v / 10) % 10, z = v / 100;
+    return (x + 1) + 12 * ((y + 1) + 12 * (z + 1));
+}
+
+// Both kernels run 256 threads per CTA (four CTAs per SM) and keep the
+// next tile's box loads in flight while the current tile computes.  A thread
+// owns up to seven box cells; which neighbour tile (3 x 3 x 3 around the
+// tile) and which slot in it each one is does not depend on the tile and is
+// worked out once.  Codes and values are loaded without waiting for the code
+// (every slot inside the grid is a valid address) and masked to the fluid
+// cells when they go to shared memory, where every vector is then zero off
+// the fluid cells: a neighbour sum needs no test.  1/d comes from a shared
+// table.
+constexpr int kMgThreads = 256;
+constexpr int kBoxPer = (kB12 + kMgThreads - 1) / kMgThreads;  // 7
+constexpr int kB10Per = (kB10 + kMgThreads - 1) / kMgThreads;  // 4
+
+// box cell v -> (neighbour tile offset + 1 per axis, local slot), packed
+// as local | (qx + 1) << 9 | (qy + 1) << 11 | (qz + 1) << 13; -1 past the box
+__device__ __forceinline__ int mg_box_map(int v) {
+    if (v >= kB12) return -1;
+    const int x = v % 12 - 2, y = (v / 12) % 12 - 2, z = v / 144 - 2;
+    const int qx = (x + 8) / 8 - 1, qy = (y + 8) / 8 - 1, qz = (z + 8) / 8 - 1;
+    const int local = (x - 8 * qx) | ((y - 8 * qy) << 3) | ((z - 8 * qz) << 6);
+    return local | ((qx + 1) << 9) | ((qy + 1) << 11) | ((qz + 1) << 13);
+}
+// slot of a mapped box cell around the tile at tile coordinates (tx, ty, tz),
+// or UINT32_MAX outside the grid; (i, j, k) of the cell out
+__device__ __forceinline__ uint32_t mg_map_slot(int map, int tx, int ty, int tz, const NatDims& D, int& i, int& j, int& k) {
+    const int ntx = tx + ((map >> 9) & 3) - 1, nty = ty + ((map >> 11) & 3) - 1, ntz = tz + ((map >> 13) & 3) - 1;
+    i = 8 * ntx + (map & 7);
+    j = 8 * nty + ((map >> 3) & 7);
+    k = 8 * ntz + ((map >> 6) & 7);
+    if (map < 0 || ntx < 0 || nty < 0 || ntz < 0 || ntx >= D.tx || nty >= D.ty || ntz >= D.tz) return 0xFFFFFFFFu;
+    return ((uint32_t)(ntx + D.tx * (nty + D.ty * ntz)) << 9) | (uint32_t)(map & 511);
+}
+__device__ __forceinline__ void mg_tile_xyz(uint32_t key, const NatDims& D, int& tx, int& ty, int& tz) {
+    const uint32_t tyz = key / (uint32_t)D.tx;
+    tx = (int)(key - tyz * (uint32_t)D.tx);
+    ty = (int)(tyz % (uint32_t)D.ty);
+    tz = (int)(tyz / (uint32_t)D.ty);
+}
+__device__ __forceinline__ float mg_sum6(const float* vb, int b, int W) {
+    return ((vb[b - 1] + vb[b + 1]) + (vb[b - W] + vb[b + W])) + (vb[b - W * W] + vb[b + W * W]);
+}
+__device__ __forceinline__ void mg_inv_table(float* inv) {
+    if (threadIdx.x < 8) {
+        const float d = (float)threadIdx.x;
+        inv[threadIdx.x] = threadIdx.x ? 1.0f / d : 0.0f;
     }
 }
 
-// residual r - A t on level F, restricted to C: C.r[parent] = 1/2 sum over
-// the children (fluid parents only).  C.r is cleared beforehand (parents of
-// tiles outside F's list keep 0).
-__global__ void __launch_bounds__(512) mg_restrict_kernel(MgLevel F, MgLevel C, const int* halt) {
+// pre-smoothing and restriction of level F into C:
+//   t1 = w D^-1 r, t = t1 + w D^-1 (r - A t1) (kept in F.t),
+//   C.r[parent] = 1/2 sum over the 8 children of r - A t (fluid parents; the
+//   parents of a tile are all written by it, and parents of tiles off the
+//   list are never fluid)
+__global__ void __launch_bounds__(kMgThreads, 4) mg_down_kernel(MgLevel F, MgLevel C, const int* halt) {
     if (mg_halted(halt)) return;
+    __shared__ uint8_t cb[kB12];
+    __shared__ float rb[kB12];
+    __shared__ float t1b[kB12];
+    __shared__ float tb[kB10];
     __shared__ float S[512];
+    __shared__ float inv[8];
+    mg_inv_table(inv);
+    const int tid = threadIdx.x;
+    int map[kBoxPer], b10m[kB10Per];
+#pragma unroll
+    for (int m = 0; m < kBoxPer; ++m) map[m] = mg_box_map(tid + m * kMgThreads);
+#pragma unroll
+    for (int m = 0; m < kB10Per; ++m) b10m[m] = tid + m * kMgThreads < kB10 ? b12_of10(tid + m * kMgThreads) : -1;
     const uint32_t n = *F.d_ntiles;
-    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
-        const uint32_t key = F.tiles[tt];
-        const uint32_t s = (key << 9) | threadIdx.x;
-        const uint8_t c = F.cell[s];
-        int i, j, k;
-        mg_cell_of(key, threadIdx.x, F.D, i, j, k);
-        float res = 0.0f;
-        if (c & kCellFluid) {
-            const float nb = mg_nb_sum(i, j, k, F.D, F.cell, [&](uint32_t u) { return F.t[u]; });
-            res = F.r[s] - ((float)(c & 7u) * F.t[s] - nb);
+    uint8_t pc[kBoxPer];
+    float pr[kBoxPer];
+    auto fetch = [&](uint32_t tt) {
+        int tx, ty, tz, i, j, k;
+        mg_tile_xyz(F.tiles[tt], F.D, tx, ty, tz);
+#pragma unroll
+        for (int m = 0; m < kBoxPer; ++m) {
+            const uint32_t sl = mg_map_slot(map[m], tx, ty, tz, F.D, i, j, k);
+            pc[m] = 0;
+            pr[m] = 0.0f;
+            if (sl != 0xFFFFFFFFu) {
+                pc[m] = F.cell[sl];
+                pr[m] = F.r[sl];
+            }
         }
-        S[threadIdx.x] = res;
+    };
+    uint32_t tt = blockIdx.x;
+    if (tt < n) fetch(tt);
+    __syncthreads();  // the 1/d table
+    for (; tt < n; tt += gridDim.x) {
+        const uint32_t key = F.tiles[tt];
+#pragma unroll
+        for (int m = 0; m < kBoxPer; ++m) {
+            const int v = tid + m * kMgThreads;
+            if (v < kB12) {
+                const uint8_t c = pc[m];
+                const bool fl = (c & kCellFluid) != 0;
+                const float r = fl ? pr[m] : 0.0f;
+                cb[v] = c;
+                rb[v] = r;
+                t1b[v] = kMgOmega * inv[c & 7u] * r;
+            }
+        }
         __syncthreads();
-        if ((threadIdx.x & 0x49u) == 0) {  // the (even, even, even) child of each 2^3 block
-            const int b = threadIdx.x;
+        if (tt + gridDim.x < n) fetch(tt + gridDim.x);  // in flight during this tile's work
+#pragma unroll
+        for (int m = 0; m < kB10Per; ++m) {
+            const int b = b10m[m];
+            if (b < 0) continue;
+            const uint8_t c = cb[b];
+            const float t1 = t1b[b];
+            tb[tid + m * kMgThreads] = (c & kCellFluid) ? t1 + kMgOmega * inv[c & 7u] * (rb[b] - ((float)(c & 7u) * t1 - mg_sum6(t1b, b, 12))) : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int cidx = tid + h * kMgThreads;
+            const int li = cidx & 7, lj = (cidx >> 3) & 7, lk = cidx >> 6;
+            const int b12 = (li + 2) + 12 * ((lj + 2) + 12 * (lk + 2));
+            const int b10 = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
+            const uint8_t c = cb[b12];
+            const float tv = tb[b10];
+            F.t[(key << 9) | cidx] = tv;
+            S[cidx] = (c & kCellFluid) ? rb[b12] - ((float)(c & 7u) * tv - mg_sum6(tb, b10, 10)) : 0.0f;
+        }
+        __syncthreads();
+        if (tid < 64) {  // the (even, even, even) child of each 2^3 block
+            int tx, ty, tz;
+            mg_tile_xyz(key, F.D, tx, ty, tz);
+            const int pi = tid & 3, pj = (tid >> 2) & 3, pk = tid >> 4;
+            const int b = 2 * pi + 16 * pj + 128 * pk;
             const float sum = ((S[b] + S[b + 1]) + (S[b + 8] + S[b + 9])) + ((S[b + 64] + S[b + 65]) + (S[b + 72] + S[b + 73]));
-            const uint32_t p = mg_slot(i >> 1, j >> 1, k >> 1, C.D);
+            const uint32_t p = mg_slot(4 * tx + pi, 4 * ty + pj, 4 * tz + pk, C.D);
             C.r[p] = (C.cell[p] & kCellFluid) ? 0.5f * sum : 0.0f;
         }
         __syncthreads();
     }
 }
 
-// prolongation and the first post-smoothing sweep: u = t + P e (e = C.z, the
-// parent's value on fluid cells), t2 = u + w D^-1 (r - A u)
-__global__ void __launch_bounds__(512) mg_post_kernel(MgLevel F, MgLevel C, const int* halt) {
+// two damped Jacobi sweeps from a start vector u: t2 = u + w D^-1 (r - A u),
+// L.z = t2 + w D^-1 (r - A t2).  MODE 0: u = L.t + C.z[parent] (prolongation
+// of the coarse correction; post-smoothing); MODE 1: u = zn + D^-1 r (the
+// coarsest level with the network output zn); MODE 2: u = w D^-1 r (the
+// coarsest level without the network).
+template <int MODE>
+__global__ void __launch_bounds__(kMgThreads, 4) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
+                                                                  const int* halt) {
     if (mg_halted(halt)) return;
-    const uint32_t n = *F.d_ntiles;
-    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
-        const uint32_t key = F.tiles[tt];
-        const uint32_t s = (key << 9) | threadIdx.x;
-        const uint8_t c = F.cell[s];
-        float out = 0.0f;
-        if (c & kCellFluid) {
-            int i, j, k;
-            mg_cell_of(key, threadIdx.x, F.D, i, j, k);
-            auto u_at = [&](uint32_t u, int a, int b, int cc) { return F.t[u] + C.z[mg_slot(a >> 1, b >> 1, cc >> 1, C.D)]; };
-            const float us = u_at(s, i, j, k);
-            const int oi[6] = {-1, 1, 0, 0, 0, 0}, oj[6] = {0, 0, -1, 1, 0, 0}, ok[6] = {0, 0, 0, 0, -1, 1};
-            float nb = 0.0f;
+    __shared__ uint8_t cb[kB12];
+    __shared__ float rb[kB12];
+    __shared__ float ub[kB12];
+    __shared__ float tb[kB10];
+    __shared__ float inv[8];
+    mg_inv_table(inv);
+    const int tid = threadIdx.x;
+    int map[kBoxPer], b10m[kB10Per];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const int a = i + oi[q], b = j + oj[q], cc = k + ok[q];
-                if (!mg_in(a, b, cc, F.D)) continue;
-                const uint32_t u = mg_slot(a, b, cc, F.D);
-                if (F.cell[u] & kCellFluid) nb += u_at(u, a, b, cc);
+    for (int m = 0; m < kBoxPer; ++m) map[m] = mg_box_map(tid + m * kMgThreads);
+#pragma unroll
+    for (int m = 0; m < kB10Per; ++m) b10m[m] = tid + m * kMgThreads < kB10 ? b12_of10(tid + m * kMgThreads) : -1;
+    const uint32_t n = *L.d_ntiles;
+    uint8_t pc[kBoxPer];
+    float pr[kBoxPer], pu[kBoxPer];
+    auto fetch = [&](uint32_t tt) {
+        int tx, ty, tz, i, j, k;
+        mg_tile_xyz(L.tiles[tt], L.D, tx, ty, tz);
+#pragma unroll
+        for (int m = 0; m < kBoxPer; ++m) {
+            const uint32_t sl = mg_map_slot(map[m], tx, ty, tz, L.D, i, j, k);
+            pc[m] = 0;
+            pr[m] = 0.0f;
+            pu[m] = 0.0f;
+            if (sl != 0xFFFFFFFFu) {
+                pc[m] = L.cell[sl];
+                pr[m] = L.r[sl];
+                if (MODE == 0) pu[m] = L.t[sl] + C.z[mg_slot(i >> 1, j >> 1, k >> 1, C.D)];
+                else if (MODE == 1) pu[m] = zn[sl];
             }
-            out = us + kMgOmega * mg_dinv(c) * (F.r[s] - ((float)(c & 7u) * us - nb));
         }
-        F.t2[s] = out;
-    }
-}
-
-// one damped Jacobi sweep: out = in + w D^-1 (r - A in)
-__global__ void __launch_bounds__(512) mg_smooth_kernel(MgLevel L, const float* __restrict__ in, float* __restrict__ out,
-                                                        const int* halt) {
-    if (mg_halted(halt)) return;
-    const uint32_t n = *L.d_ntiles;
-    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
+    };
+    uint32_t tt = blockIdx.x;
+    if (tt < n) fetch(tt);
+    __syncthreads();  // the 1/d table
+    for (; tt < n; tt += gridDim.x) {
         const uint32_t key = L.tiles[tt];
-        const uint32_t s = (key << 9) | threadIdx.x;
-        const uint8_t c = L.cell[s];
-        float v = 0.0f;
-        if (c & kCellFluid) {
-            int i, j, k;
-            mg_cell_of(key, threadIdx.x, L.D, i, j, k);
-            const float nb = mg_nb_sum(i, j, k, L.D, L.cell, [&](uint32_t u) { return in[u]; });
-            const float x = in[s];
-            v = x + kMgOmega * mg_dinv(c) * (L.r[s] - ((float)(c & 7u) * x - nb));
+#pragma unroll
+        for (int m = 0; m < kBoxPer; ++m) {
+            const int v = tid + m * kMgThreads;
+            if (v < kB12) {
+                const uint8_t c = pc[m];
+                const bool fl = (c & kCellFluid) != 0;
+                const float r = fl ? pr[m] : 0.0f;
+                float u = 0.0f;
+                if (fl) u = MODE == 0 ? pu[m] : (MODE == 1 ? pu[m] + inv[c & 7u] * r : kMgOmega * inv[c & 7u] * r);
+                cb[v] = c;
+                rb[v] = r;
+                ub[v] = u;
+            }
         }
-        out[s] = v;
-    }
-}
-
-// coarsest start: z = zn + D^-1 r with the network output zn, else w D^-1 r
-__global__ void __launch_bounds__(512) mg_coarse_start_kernel(MgLevel L, const float* __restrict__ zn, float* __restrict__ out,
-                                                              const int* halt) {
-    if (mg_halted(halt)) return;
-    const uint32_t n = *L.d_ntiles;
-    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
-        const uint32_t s = (L.tiles[tt] << 9) | threadIdx.x;
-        const uint8_t c = L.cell[s];
-        float v = 0.0f;
-        if (c & kCellFluid) v = zn ? zn[s] + mg_dinv(c) * L.r[s] : kMgOmega * mg_dinv(c) * L.r[s];
-        out[s] = v;
+        __syncthreads();
+        if (tt + gridDim.x < n) fetch(tt + gridDim.x);  // in flight during this tile's work
+#pragma unroll
+        for (int m = 0; m < kB10Per; ++m) {
+            const int b = b10m[m];
+            if (b < 0) continue;
+            const uint8_t c = cb[b];
+            const float u = ub[b];
+            tb[tid + m * kMgThreads] = (c & kCellFluid) ? u + kMgOmega * inv[c & 7u] * (rb[b] - ((float)(c & 7u) * u - mg_sum6(ub, b, 12))) : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int cidx = tid + h * kMgThreads;
+            const int li = cidx & 7, lj = (cidx >> 3) & 7, lk = cidx >> 6;
+            const int b12 = (li + 2) + 12 * ((lj + 2) + 12 * (lk + 2));
+            const int b10 = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
+            const uint8_t c = cb[b12];
+            const float tv = tb[b10];
+            L.z[(key << 9) | cidx] =
+                (c & kCellFluid) ? tv + kMgOmega * inv[c & 7u] * (rb[b12] - ((float)(c & 7u) * tv - mg_sum6(tb, b10, 10))) : 0.0f;
+        }
+        __syncthreads();
     }
 }
 
@@ -324,9 +464,11 @@ int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels) {
     return levels;
 }
 
+// CTAs of the smoothing kernels: four per SM (grid0 on level 0) and no more
+// than the level has tiles
 static int mg_grid(const MgLevel& L, int grid0, int level) {
     if (level == 0) return grid0;
-    return (int)(L.ntiles < 1184u ? L.ntiles : 1184u);
+    return (int)(L.ntiles < 592u ? L.ntiles : 592u);
 }
 
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
@@ -340,33 +482,25 @@ int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
 }
 
 int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
-    for (int l = 0; l + 1 < H.levels; ++l) {
-        const MgLevel &F = H.L[l], &C = H.L[l + 1];
-        mg_pre_kernel<<<mg_grid(F, grid0, l), 512, 0, s>>>(F, halt);
-        FLIP_CUDA_TRY(cudaMemsetAsync(C.r, 0, (size_t)C.ntiles * 512u * sizeof(float), s));
-        mg_restrict_kernel<<<mg_grid(F, grid0, l), 512, 0, s>>>(F, C, halt);
-    }
+    for (int l = 0; l + 1 < H.levels; ++l)
+        mg_down_kernel<<<mg_grid(H.L[l], grid0, l), kMgThreads, 0, s>>>(H.L[l], H.L[l + 1], halt);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
 int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s) {
-    const MgLevel& L = H.L[H.levels - 1];
-    const int g = mg_grid(L, 1184, H.levels - 1);
-    mg_coarse_start_kernel<<<g, 512, 0, s>>>(L, zn, L.z, halt);
-    mg_smooth_kernel<<<g, 512, 0, s>>>(L, L.z, L.t, halt);
-    mg_smooth_kernel<<<g, 512, 0, s>>>(L, L.t, L.z, halt);
+    const int c = H.levels - 1;
+    const MgLevel& L = H.L[c];
+    const int g = mg_grid(L, 592, c);
+    if (zn) mg_sweeps_kernel<1><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
+    else mg_sweeps_kernel<2><<<g, kMgThreads, 0, s>>>(L, L, nullptr, halt);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
 int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
-    for (int l = H.levels - 2; l >= 0; --l) {
-        const MgLevel &F = H.L[l], &C = H.L[l + 1];
-        const int g = mg_grid(F, grid0, l);
-        mg_post_kernel<<<g, 512, 0, s>>>(F, C, halt);
-        mg_smooth_kernel<<<g, 512, 0, s>>>(F, F.t2, F.z, halt);
-    }
+    for (int l = H.levels - 2; l >= 0; --l)
+        mg_sweeps_kernel<0><<<mg_grid(H.L[l], grid0, l), kMgThreads, 0, s>>>(H.L[l], H.L[l + 1], nullptr, halt);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

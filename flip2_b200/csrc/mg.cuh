@@ -42,8 +42,7 @@ struct MgLevel {
     uint8_t* active;        // [tiles] all 1 (coarse levels; the network's active flags)
     float* r;               // right-hand side of the level's correction problem
     float* z;               // the level's V-cycle output
-    float* t;               // smoothing iterate
-    float* t2;              // second smoothing iterate
+    float* t;               // pre-smoothing iterate (read back by the post-smoothing)
 };
 
 struct MgHierarchy {
@@ -58,12 +57,14 @@ int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels);
 // coarse types and cell codes of every level from level 0's types and codes
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s);
 // one V-cycle up to the coarsest level's input: smoothing and restriction
-// on levels 0 .. levels-2 (the coarsest right-hand side ends in L[levels-1].r)
+// on levels 0 .. levels-2, one kernel per level (the coarsest right-hand
+// side ends in L[levels-1].r)
 int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
 // the coarsest level's solve around a network output zn (nullptr: no
-// network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps
+// network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps (one kernel)
 int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s);
-// prolongation and post-smoothing back up to level 0 (its output in L[0].z)
+// prolongation and post-smoothing back up to level 0, one kernel per level
+// (the output in L[0].z)
 int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
 // x = A^-1 b on level L by Jacobi-PCG in one CTA (|r| <= tol |b| or
 // max_iter iterations; *iters = iterations run); r, p, q: scratch of the

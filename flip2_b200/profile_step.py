@@ -1,16 +1,25 @@
 """Run a few native steps of the dam-break scene and print per-stage times.
 
     python -m flip2_b200.profile_step [--cells 256] [--steps 2] [--dt 1/480]
+        [--method 0|1|2] [--poisson K]
 
 The scene is the benchmark's (block 0.5 x 0.5 x 1 of the unit box, 8
 jittered particles per voxel, seed 0).  Each step runs in full; stage times
-come from CUDA events on the engine stream.  Short enough to run under a
+come from CUDA events on the engine stream.  --method picks the pressure
+solve (1 and 2 load the committed weights of the learned preconditioner);
+--poisson K solves K generated pressure problems of the grid (seeds 900000
+and up) with that method instead of stepping.  Short enough to run under a
 profiler with a kernel filter.
 """
 import argparse
 import json
+import os
+
+import numpy as np
 
 from . import MODE_NATIVE, Particles, default_params, scenes
+
+WEIGHTS = {1: "lprec_weights.npy", 2: "mg_weights.npy"}
 
 
 def main():
@@ -19,11 +28,29 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--dt", type=float, default=1.0 / 480.0)
     ap.add_argument("--block", type=float, nargs=3, default=(0.5, 0.5, 1.0))
+    ap.add_argument("--method", type=int, default=0, choices=(0, 1, 2))
+    ap.add_argument("--lp-cuda-cores", type=int, default=0)
+    ap.add_argument("--poisson", type=int, default=0)
     args = ap.parse_args()
-    pos, vel = scenes.dam_break(args.cells, block=tuple(args.block), seed=0)
-    P = Particles(pos.shape[0], mode=MODE_NATIVE, params=default_params(MODE_NATIVE))
+    params = default_params(MODE_NATIVE, pressure_method=args.method, lp_cuda_cores=args.lp_cuda_cores)
     R = args.cells // 4
+    if args.poisson:
+        P = Particles(1, mode=MODE_NATIVE, params=params)
+        P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
+        if args.method:
+            P.lp_set_weights(np.load(os.path.join(os.path.dirname(__file__), "data", WEIGHTS[args.method])))
+        for k in range(args.poisson):
+            P.poisson_generate(seed=900_000 + k)
+            i = P.poisson_solve(args.method, 1e-6, 20000 if args.method == 0 else 100)
+            print(json.dumps({"problem": 900_000 + k, "method": args.method, "iters": i.iters, "ms": round(i.ms, 3),
+                              "fell_back": i.fell_back, "rel_residual": i.rel_residual}))
+        P.close()
+        return
+    pos, vel = scenes.dam_break(args.cells, block=tuple(args.block), seed=0)
+    P = Particles(pos.shape[0], mode=MODE_NATIVE, params=params)
     P.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / args.cells)
+    if args.method:
+        P.lp_set_weights(np.load(os.path.join(os.path.dirname(__file__), "data", WEIGHTS[args.method])))
     P.upload(pos, vel)
     P.set_timing(True)
     for k in range(args.steps):

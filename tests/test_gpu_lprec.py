@@ -257,7 +257,10 @@ def test_lp_errors(torch):
         P.lp_set_weights(np.zeros(10, np.float32))
     assert ei.value.status == ERR_ARG
     with pytest.raises(F.FlipError) as ei:
-        P.poisson_solve(method=2)
+        P.poisson_solve(method=2)  # the multilevel form needs the weights too
+    assert ei.value.status == ERR_STATE
+    with pytest.raises(F.FlipError) as ei:
+        P.poisson_solve(method=3)
     assert ei.value.status == ERR_ARG
     with pytest.raises(F.FlipError) as ei:
         P.poisson_generate(seed=0, surface=(0.9, 0.1))
