@@ -935,6 +935,17 @@ static int mg_coarse_grid(flip_engine* e) {
     const uint32_t n = e->mg.L[e->mg.levels - 1].ntiles;
     return e->mg.levels == 1 ? nat_grid(e, 2) : (int)std::min<uint32_t>(n, (uint32_t)e->sms * 2u);
 }
+// the network on the coarsest level: the small-grid kernels when it is a
+// coarse level, the solver-grid kernels when the solver's grid is itself the
+// coarsest
+static int mg_net_bias(flip_engine* e, const LpGrid& G) {
+    if (e->mg.levels == 1) return lp_bias_dev(e->lp, G, e->mg.inv_s, e->mg.f0, mg_coarse_grid(e), e->stream);
+    return lp_small_bias(e->lp, G, e->mg.L[e->mg.levels - 1].ntiles, e->mg.inv_s, e->mg.f0, e->stream);
+}
+static int mg_net_forward(flip_engine* e, const LpGrid& G) {
+    if (e->mg.levels == 1) return lp_forward_dev(e->lp, G, e->mg.inv_s, e->mg.f0, e->mg_zn, mg_coarse_grid(e), e->stream);
+    return lp_small_forward(e->lp, G, e->mg.L[e->mg.levels - 1].ntiles, e->mg.inv_s, e->mg.f0, e->mg_zn, e->stream);
+}
 // kernels of one V-cycle (for the launch count)
 static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
     return 2u * (uint32_t)(e->mg.levels - 1) + 1u + (network ? 5u : 0u);
@@ -947,7 +958,7 @@ static int mg_cycle(flip_engine* e, bool network, const int* halt) {
     if (network) {
         const LpGrid G = mg_lp_grid(e, halt);
         E_TRY(mg_input_scale(e->mg, halt, e->stream));
-        E_TRY(lp_forward_dev(e->lp, G, e->mg.inv_s, e->mg.f0, e->mg_zn, mg_coarse_grid(e), e->stream));
+        E_TRY(mg_net_forward(e, G));
         zn = e->mg_zn;
     }
     E_TRY(mg_coarsest(e->mg, zn, halt, e->stream));
@@ -961,7 +972,7 @@ static int mg_setup_problem(flip_engine* e, bool network) {
     e->launches += 2u * (uint32_t)(e->mg.levels - 1);
     if (network) {
         const LpGrid G = mg_lp_grid(e, nullptr);
-        E_TRY(lp_bias_dev(e->lp, G, e->mg.inv_s, e->mg.f0, mg_coarse_grid(e), e->stream));
+        E_TRY(mg_net_bias(e, G));
         e->launches += 4;
     }
     return FLIP_OK;
@@ -1869,7 +1880,7 @@ extern "C" int flip_mg_train_step(flip_engine* e, int sample, float lr, double* 
         e->launches += 2;
     }
     E_TRY(mg_input_scale(e->mg, nullptr, e->stream));
-    E_TRY(lp_forward_dev(e->lp, G, e->mg.inv_s, e->mg.f0, e->mg_zn, grid, e->stream));
+    E_TRY(mg_net_forward(e, G));
     E_CUDA(cudaMemsetAsync(e->lp_scalar, 0, 3 * sizeof(double), e->stream));
     E_TRY(lp_loss_grad(G, e->mg_zn, e->mg_ev, e->mg_wbuf, e->mg_gz, e->lp_scalar, grid, e->stream));
     E_CUDA(cudaMemsetAsync(e->lp.g, 0, sizeof(float) * kLpNumW, e->stream));

@@ -175,6 +175,174 @@ __global__ void __launch_bounds__(512) lp_out_kernel(LpGrid G, const __nv_bfloat
     }
 }
 
+// ------------------------------------------------- forward on small grids
+// The coarsest level of the multilevel preconditioner has at most eight
+// tiles (4,096 voxels).  One CTA per tile would occupy eight SMs and chain 27
+// dependent tap loads per thread, so these kernels give a CTA 16 voxels:
+// first the CTA gathers the inputs of all 27 taps of its voxels into shared
+// memory in one round of independent loads, then 16 threads per voxel (one
+// per output channel, or one per input channel for the last layer) compute
+// from shared memory.  Every tile of the small grid is active, so a tap
+// only tests the grid bounds.
+constexpr int kSmallThreads = 256;
+constexpr int kSmallVox = 16;
+
+__device__ __forceinline__ uint32_t small_slot(int i, int j, int k, const NatDims& D) {
+    if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return 0xFFFFFFFFu;
+    return lslot(i, j, k, D);
+}
+// cell (i, j, k) and slot of the CTA's voxel q (0..15), false past the grid
+__device__ __forceinline__ bool small_voxel(const LpGrid& G, int q, uint32_t& v, int& i, int& j, int& k) {
+    const uint32_t vx = blockIdx.x * kSmallVox + q;
+    if (vx >= *G.d_nact * 512u) return false;
+    const uint32_t key = G.act_tiles[vx >> 9];
+    int ox, oy, oz;
+    tile_origin(key, G.D, ox, oy, oz);
+    const int l = (int)(vx & 511u);
+    i = ox + (l & 7);
+    j = oy + ((l >> 3) & 7);
+    k = oz + (l >> 6);
+    v = (key << 9) | (uint32_t)l;
+    return true;
+}
+// X[q][tap][16] <- the 16 BF16 channels of in at tap of voxel q (0 outside)
+__device__ __forceinline__ void small_gather16(const LpGrid& G, int dil, const __nv_bfloat16* __restrict__ in, uint4* X) {
+    for (int e = threadIdx.x; e < kSmallVox * 27 * 2; e += kSmallThreads) {
+        const int q = e / 54, tap = (e % 54) >> 1, half = e & 1;
+        uint32_t v;
+        int i, j, k, dx, dy, dz;
+        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        if (small_voxel(G, q, v, i, j, k)) {
+            tap_off(tap, dx, dy, dz);
+            const uint32_t u = small_slot(i + dil * dx, j + dil * dy, k + dil * dz, G.D);
+            if (u != 0xFFFFFFFFu) val = reinterpret_cast<const uint4*>(in + (size_t)u * 16)[half];
+        }
+        X[e] = val;
+    }
+}
+__device__ __forceinline__ void unpack8(const uint4& q, float* x) {
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const float2 f = __bfloat1622float2(h[m]);
+        x[2 * m] = f.x;
+        x[2 * m + 1] = f.y;
+    }
+}
+
+// layer 0 (3 -> 16, ReLU); r = nullptr in G gives the zero-residual pass
+__global__ void __launch_bounds__(kSmallThreads) lp_small_in_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
+                                                                    const float* __restrict__ d_inv_s,
+                                                                    __nv_bfloat16* __restrict__ out) {
+    if (G.halt && *G.halt) return;
+    __shared__ float W[27 * 3 * 16];
+    __shared__ float X[kSmallVox * 27 * 3];
+    for (int q = threadIdx.x; q < 27 * 3 * 16; q += kSmallThreads) W[q] = __bfloat162float(wb[q]);
+    const float inv_s = *d_inv_s;
+    for (int e = threadIdx.x; e < kSmallVox * 27; e += kSmallThreads) {
+        const int q = e / 27, tap = e % 27;
+        uint32_t v;
+        int i, j, k, dx, dy, dz;
+        float in[3] = {0.0f, 0.0f, 0.0f};
+        if (small_voxel(G, q, v, i, j, k)) {
+            tap_off(tap, dx, dy, dz);
+            const uint32_t u = small_slot(i + dil * dx, j + dil * dy, k + dil * dz, G.D);
+            if (u != 0xFFFFFFFFu) input_channels(G, u, inv_s, in);
+        }
+        X[3 * e] = in[0];
+        X[3 * e + 1] = in[1];
+        X[3 * e + 2] = in[2];
+    }
+    __syncthreads();
+    const int co = threadIdx.x & 15, q = threadIdx.x >> 4;
+    uint32_t v;
+    int i, j, k;
+    if (!small_voxel(G, q, v, i, j, k)) return;
+    const float* x = X + q * 81;
+    float acc = 0.0f;
+#pragma unroll 27
+    for (int t = 0; t < 81; ++t) acc = fmaf(W[t * 16 + co], x[t], acc);
+    out[(size_t)v * 16 + co] = __float2bfloat16_rn(fmaxf(acc, 0.0f));
+}
+
+// layers 1, 2 (16 -> 16, ReLU)
+__global__ void __launch_bounds__(kSmallThreads) lp_small_mid_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
+                                                                     const __nv_bfloat16* __restrict__ in,
+                                                                     __nv_bfloat16* __restrict__ out) {
+    if (G.halt && *G.halt) return;
+    __shared__ float W[27 * 16 * 16];  // [tap][ci][co]
+    __shared__ uint4 X[kSmallVox * 27 * 2];
+    for (int q = threadIdx.x; q < 27 * 256; q += kSmallThreads) W[q] = __bfloat162float(wb[q]);
+    small_gather16(G, dil, in, X);
+    __syncthreads();
+    const int co = threadIdx.x & 15, q = threadIdx.x >> 4;
+    uint32_t v;
+    int i, j, k;
+    if (!small_voxel(G, q, v, i, j, k)) return;
+    float acc = 0.0f;
+    for (int tap = 0; tap < 27; ++tap) {
+        float x[16];
+        unpack8(X[(q * 27 + tap) * 2], x);
+        unpack8(X[(q * 27 + tap) * 2 + 1], x + 8);
+        const float* w = W + tap * 256 + co;
+#pragma unroll
+        for (int ci = 0; ci < 16; ++ci) acc = fmaf(w[ci * 16], x[ci], acc);
+    }
+    out[(size_t)v * 16 + co] = __float2bfloat16_rn(fmaxf(acc, 0.0f));
+}
+
+// layer 3 (16 -> 1) on the fluid cells: thread ci of a voxel sums its input
+// channel over the taps, a 16-lane shuffle adds the channels; z = f (raw)
+// or z = s (f - f0)
+__global__ void __launch_bounds__(kSmallThreads) lp_small_out_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
+                                                                     const __nv_bfloat16* __restrict__ in,
+                                                                     const float* __restrict__ d_inv_s,
+                                                                     const float* __restrict__ f0, int raw,
+                                                                     float* __restrict__ z) {
+    if (G.halt && *G.halt) return;
+    __shared__ float W[27 * 16];
+    __shared__ uint4 X[kSmallVox * 27 * 2];
+    for (int q = threadIdx.x; q < 27 * 16; q += kSmallThreads) W[q] = __bfloat162float(wb[q]);
+    small_gather16(G, dil, in, X);
+    __syncthreads();
+    const int ci = threadIdx.x & 15, q = threadIdx.x >> 4;
+    uint32_t v = 0;
+    int i, j, k;
+    const bool ok = small_voxel(G, q, v, i, j, k);
+    float acc = 0.0f;
+    if (ok) {
+        const __nv_bfloat16* xb = reinterpret_cast<const __nv_bfloat16*>(X + q * 54);
+        for (int tap = 0; tap < 27; ++tap) acc = fmaf(W[tap * 16 + ci], __bfloat162float(xb[tap * 16 + ci]), acc);
+    }
+#pragma unroll
+    for (int m = 8; m > 0; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    if (ok && ci == 0) {
+        float o = 0.0f;
+        if (G.type[v] == kFluid) o = raw ? acc : (acc - (f0 ? f0[v] : 0.0f)) * (1.0f / *d_inv_s);
+        z[v] = o;
+    }
+}
+
+static int lp_small_pass(const LpNet& net, const LpGrid& G, const float* d_inv_s, __nv_bfloat16* const* acts,
+                         const float* f0, int raw, float* z, uint32_t ntiles, cudaStream_t st) {
+    const int g = (int)(ntiles * 512u / kSmallVox);
+    lp_small_in_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, acts[0]);
+    lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1]);
+    lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2]);
+    lp_small_out_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], acts[2], d_inv_s, f0, raw, z);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int lp_small_bias(const LpNet& net, const LpGrid& G, uint32_t ntiles, const float* d_inv_s, float* f0, cudaStream_t st) {
+    LpGrid G0 = G;
+    G0.r = nullptr;
+    return lp_small_pass(net, G0, d_inv_s, net.actz, nullptr, 1, f0, ntiles, st);
+}
+int lp_small_forward(const LpNet& net, const LpGrid& G, uint32_t ntiles, const float* d_inv_s, const float* f0, float* z,
+                     cudaStream_t st) {
+    return lp_small_pass(net, G, d_inv_s, net.act, f0, 0, z, ntiles, st);
+}
+
 // --------------------------------------------------------------- backward
 // dL/d(layer-2 activations) from dL/dz: G2[u][ci] = relu'(A2[u][ci]) *
 // sum_tap W3[tap][ci] * s * gz(u - dil*off); gz is zero off fluid cells

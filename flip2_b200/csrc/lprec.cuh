@@ -69,6 +69,12 @@ int lp_bias_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* 
 // z = N(r) given f0
 int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, const float* f0, float* z, int grid,
                    cudaStream_t st);
+// the same two passes on a small grid whose every tile is in G's tile lists
+// (ntiles tiles, the coarsest level of the multilevel preconditioner): a CTA
+// per 16 voxels
+int lp_small_bias(const LpNet& net, const LpGrid& G, uint32_t ntiles, const float* d_inv_s, float* f0, cudaStream_t st);
+int lp_small_forward(const LpNet& net, const LpGrid& G, uint32_t ntiles, const float* d_inv_s, const float* f0, float* z,
+                     cudaStream_t st);
 // gradient of the loss with respect to the weights given dL/dz (gz, FP32 on
 // the slots of the active tiles, zero off fluid cells), through both the
 // f(r/s) and the f(0) activations; accumulates into net.g (caller zeroes it)
