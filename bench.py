@@ -34,6 +34,10 @@ WORKLOAD = ("dam-break 256^3 voxels (cell 1/256), block 0.5x0.5x1, 8 jittered pa
 # algorithmic bytes of one PCG iteration per active voxel, fused minimum:
 # matvec+pAp 9 B, x/r/z update with r.z 28 B, direction update 12 B
 PCG_BYTES_PER_VOXEL = 49.0
+# one learned multilevel FCG iteration on the fine level: direction+matvec and
+# update 49 B, V-cycle down (code, r in; t, coarse r out) 9.5 B and up (code,
+# r, t in; z out) 12.5 B, FCG dot (r, z, q in) 12 B; coarse levels not counted
+MG_BYTES_PER_VOXEL = 83
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -70,33 +74,53 @@ C4_SEED0 = 900_000
 def c4_pressure(F, device):
     """128^3 pressure problems (solid spheres of radius 4..16 voxels to 10% of
     the box, fluid surface at 50-85% height, Gaussian impulses plus gravity),
-    solved to 1e-6 by Jacobi-PCG and by learned FCG with the committed weights
-    (Jacobi-PCG restart after 100 FCG iterations).  Device ms from CUDA events
-    inside the engine; the relative residuals are FP64 true residuals."""
-    wpath = os.path.join(ROOT, "flip2_b200", "data", "lprec_weights.npy")
-    if not os.path.exists(wpath):
+    solved to 1e-6 by Jacobi-PCG and by the learned multilevel FCG
+    (pressure_method 2: V-cycle whose 16^3 coarsest level the committed
+    network solves), by the same V-cycle without the network, and by FCG
+    with the network on the solver's grid (pressure_method 1, committed
+    weights, Jacobi-PCG restart after 100 iterations).  Device ms from CUDA
+    events inside the engine; the relative residuals are FP64 true
+    residuals."""
+    data = os.path.join(ROOT, "flip2_b200", "data")
+    if not (os.path.exists(os.path.join(data, "mg_weights.npy")) and os.path.exists(os.path.join(data, "lprec_weights.npy"))):
         return None
-    P = F.Particles(1, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE, device=device))
     R = C4_CELLS // 4
-    P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
-    P.lp_set_weights(np.load(wpath))
-    P.poisson_generate(seed=C4_SEED0)
-    P.poisson_solve(0, 1e-6, 20000)  # warm-up: graphs and the network's buffers
-    P.poisson_solve(1, 1e-6, 4)
+    engines = {}
+    for name, kw, wfile in (("learned", {}, "mg_weights.npy"), ("no_network", {"mg_coarse": 1}, "mg_weights.npy"),
+                            ("fine_grid_network", {}, "lprec_weights.npy")):
+        P = F.Particles(1, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE, device=device, **kw))
+        P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
+        P.lp_set_weights(np.load(os.path.join(data, wfile)))
+        engines[name] = P
+    method = {"learned": 2, "no_network": 2, "fine_grid_network": 1}
+    for name, P in engines.items():  # warm-up: graphs and buffers
+        P.poisson_generate(seed=C4_SEED0)
+        P.poisson_solve(0, 1e-6, 20000)
+        P.poisson_solve(method[name], 1e-6, 4)
     rows = []
     for k in range(C4_PROBLEMS):
-        P.poisson_generate(seed=C4_SEED0 + k)
-        a = P.poisson_solve(0, 1e-6, 20000)
-        b = P.poisson_solve(1, 1e-6, 100)
-        rows.append({"plain_ms": a.ms, "plain_iters": a.iters, "plain_rel_residual": a.rel_residual,
-                     "learned_ms": b.ms, "learned_fcg_iters": b.iters, "fell_back": b.fell_back,
-                     "restart_iters": b.plain_iters, "learned_rel_residual": b.rel_residual})
-    P.close()
-    plain = sum(r["plain_ms"] for r in rows) / len(rows)
-    learned = sum(r["learned_ms"] for r in rows) / len(rows)
+        row = {}
+        for name, P in engines.items():
+            P.poisson_generate(seed=C4_SEED0 + k)
+            if name == "learned":
+                a = P.poisson_solve(0, 1e-6, 20000)
+                row.update({"plain_ms": a.ms, "plain_iters": a.iters, "plain_rel_residual": a.rel_residual})
+            b = P.poisson_solve(method[name], 1e-6, 100)
+            row.update({name + "_ms": b.ms, name + "_iters": b.iters, name + "_fell_back": b.fell_back,
+                        name + "_restart_iters": b.plain_iters, name + "_rel_residual": b.rel_residual})
+        rows.append(row)
+    for P in engines.values():
+        P.close()
+    mean = lambda key: sum(r[key] for r in rows) / len(rows)
     return {"workload": "128^3 generated pressure problems (seeds %d..%d), tol 1e-6" % (C4_SEED0, C4_SEED0 + C4_PROBLEMS - 1),
-            "plain_ms_mean": plain, "learned_ms_mean": learned, "speedup_learned_over_plain": plain / learned,
-            "fallback_rate": sum(r["fell_back"] for r in rows) / len(rows), "problems": rows}
+            "learned": "pressure_method 2: FCG, V-cycle (damped Jacobi, 4 levels) with the network solving the 16^3 level",
+            "plain_ms_mean": mean("plain_ms"), "learned_ms_mean": mean("learned_ms"),
+            "no_network_ms_mean": mean("no_network_ms"), "fine_grid_network_ms_mean": mean("fine_grid_network_ms"),
+            "plain_iters_mean": mean("plain_iters"), "learned_iters_mean": mean("learned_iters"),
+            "no_network_iters_mean": mean("no_network_iters"),
+            "speedup_learned_over_plain": mean("plain_ms") / mean("learned_ms"),
+            "speedup_learned_over_no_network": mean("no_network_ms") / mean("learned_ms"),
+            "fallback_rate": mean("learned_fell_back"), "problems": rows}
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -268,12 +292,12 @@ def main():
     n = pos.shape[0]
     stream = torch.cuda.Stream(device=dev)
     c5 = args.config == "c5"
-    params = F.default_params(F.MODE_NATIVE, device=local, pressure_method=1 if c5 else 0)
+    params = F.default_params(F.MODE_NATIVE, device=local, pressure_method=2 if c5 else 0)
     P = F.Particles(n, mode=F.MODE_NATIVE, params=params, stream=stream.cuda_stream)
     R = args.cells // 4
     P.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / args.cells)
     if c5:
-        P.lp_set_weights(np.load(os.path.join(ROOT, "flip2_b200", "data", "lprec_weights.npy")))
+        P.lp_set_weights(np.load(os.path.join(ROOT, "flip2_b200", "data", "mg_weights.npy")))
     # pinned host state for the end-to-end leg
     host = [torch.from_numpy(np.ascontiguousarray(pos[:, k])).pin_memory() for k in range(3)]
     host += [torch.from_numpy(np.ascontiguousarray(vel[:, k])).pin_memory() for k in range(3)]
@@ -349,7 +373,8 @@ def main():
     except (OSError, ValueError):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = PCG_BYTES_PER_VOXEL * voxels / (t_iter_ms / 1e3) / 1e9
+    per_voxel = MG_BYTES_PER_VOXEL if c5 else PCG_BYTES_PER_VOXEL
+    achieved = per_voxel * voxels / (t_iter_ms / 1e3) / 1e9
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
@@ -358,9 +383,13 @@ def main():
             traffic = traffic * voxels
     except (OSError, ValueError):
         pass
+    if c5:
+        traffic = None  # the ncu traffic figure covers the Jacobi-PCG iteration only
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "pcg iteration (matvec+pAp, x/r update with r.r and r.z, direction)",
-                "algorithmic_bytes": "49 B per active voxel per iteration x %d voxels" % voxels,
+                "traffic": traffic,
+                "kernel": ("learned multilevel FCG iteration (direction+matvec, update, V-cycle, FCG dot)" if c5 else
+                           "pcg iteration (matvec+pAp, x/r update with r.r and r.z, direction)"),
+                "algorithmic_bytes": "%d B per active voxel per iteration x %d voxels" % (per_voxel, voxels),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
 
     # the north-star particle metric: binning, P2G and G2P/advection only
@@ -379,7 +408,8 @@ def main():
         workload = WORKLOAD
         if c5:
             workload = WORKLOAD.replace("block 0.5x0.5x1", "block 0.5x0.5x1 + sphere r=0.15 at (0.5,0.75,0.5)").replace(
-                "Jacobi-PCG to 1e-6", "learned FCG (100-iteration cap, Jacobi-PCG restart) to 1e-6")
+                "Jacobi-PCG to 1e-6", "learned multilevel FCG (V-cycle, network on the 16^3 level; 100-iteration cap, "
+                "Jacobi-PCG restart) to 1e-6")
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -969,7 +969,7 @@ static int mg_cycle(flip_engine* e, bool network, const int* halt) {
 // and the network's f(0) on the coarsest level
 static int mg_setup_problem(flip_engine* e, bool network) {
     E_TRY(mg_build(e->mg, nullptr, e->stream));
-    e->launches += 2u * (uint32_t)(e->mg.levels - 1);
+    e->launches += 2u * (uint32_t)(e->mg.levels - 1) + 2u * (uint32_t)std::max(0, e->mg.levels - 2);
     if (network) {
         const LpGrid G = mg_lp_grid(e, nullptr);
         E_TRY(mg_net_bias(e, G));

@@ -298,7 +298,12 @@ __global__ void __launch_bounds__(kMgThreads, 4) mg_sweeps_kernel(MgLevel L, MgL
             if (sl != 0xFFFFFFFFu) {
                 pc[m] = L.cell[sl];
                 pr[m] = L.r[sl];
-                if (MODE == 0) pu[m] = L.t[sl] + C.z[mg_slot(i >> 1, j >> 1, k >> 1, C.D)];
+                if (MODE == 0) {
+                    // the parent's correction; a parent that is not fluid
+                    // may sit in a tile off the coarse list (stale z)
+                    const uint32_t ps = mg_slot(i >> 1, j >> 1, k >> 1, C.D);
+                    pu[m] = L.t[sl] + ((C.cell[ps] & kCellFluid) ? C.z[ps] : 0.0f);
+                }
                 else if (MODE == 1) pu[m] = zn[sl];
             }
         }
@@ -473,9 +478,17 @@ static int mg_grid(const MgLevel& L, int grid0, int level) {
 
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
     for (int l = 1; l < H.levels; ++l) {
-        const int g = (int)((H.L[l].ntiles + 0u) < 1184u ? H.L[l].ntiles : 1184u);
-        mg_coarsen_kernel<<<g, 512, 0, s>>>(H.L[l - 1], H.L[l], halt);
-        mg_codes_kernel<<<g, 512, 0, s>>>(H.L[l], halt);
+        const MgLevel& C = H.L[l];
+        const int g = (int)(C.ntiles < 1184u ? C.ntiles : 1184u);
+        mg_coarsen_kernel<<<g, 512, 0, s>>>(H.L[l - 1], C, halt);
+        mg_codes_kernel<<<g, 512, 0, s>>>(C, halt);
+        // the smoothing of an intermediate level walks its tiles with fluid
+        // cells (flags in C.active); the coarsest keeps every tile
+        if (l + 1 < H.levels) {
+            const int rc = nat_launch_fluid_tiles(C.type, C.active, C.ntiles, const_cast<uint32_t*>(C.tiles),
+                                                  const_cast<uint32_t*>(C.d_ntiles), (uint64_t)C.ntiles * 512u, s);
+            if (rc != FLIP_OK) return rc;
+        }
     }
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;

@@ -34,12 +34,14 @@ constexpr float kMgOmega = 2.0f / 3.0f;
 struct MgLevel {
     NatDims D;              // padded to whole tiles
     int ex, ey, ez;         // cells of the level; past them the grid is solid
-    uint32_t ntiles;        // level 0: capacity; coarse levels: every tile
-    const uint32_t* tiles;  // tile list (level 0: the occupied tiles)
+    uint32_t ntiles;        // tiles of the level's box
+    const uint32_t* tiles;  // tile list: the tiles with fluid cells (the
+                            // coarsest level: every tile)
     const uint32_t* d_ntiles;
     uint8_t* type;          // 0 air, 1 fluid, 2 solid
     uint8_t* cell;          // PCG cell code: bit 7 fluid, bits 0-2 non-solid neighbours
-    uint8_t* active;        // [tiles] all 1 (coarse levels; the network's active flags)
+    uint8_t* active;        // [tiles] the coarsest level: all 1 (the network's active
+                            // flags); intermediate levels: fluid-tile flags
     float* r;               // right-hand side of the level's correction problem
     float* z;               // the level's V-cycle output
     float* t;               // pre-smoothing iterate (read back by the post-smoothing)
@@ -54,7 +56,8 @@ struct MgHierarchy {
 
 // level dimensions below a fine grid of nx x ny x nz (multiples of 8) cells
 int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels);
-// coarse types and cell codes of every level from level 0's types and codes
+// coarse types and cell codes of every level from level 0's types and
+// codes, and the fluid-tile lists of the intermediate levels
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s);
 // one V-cycle up to the coarsest level's input: smoothing and restriction
 // on levels 0 .. levels-2, one kernel per level (the coarsest right-hand
