@@ -21,6 +21,37 @@ def rel_err(a, b, floor=0.0):
     return float(np.max(np.abs(a - b)) / den)
 
 
+def sealed_pockets(typ, shape):
+    """Labels of the fluid regions that touch no air cell (x fastest; 0 air,
+    1 fluid, 2 solid, outside the box solid) and their count.  The pressure
+    of such a region has pure Neumann boundaries: it is defined only up to a
+    constant, and different solvers that all meet the residual tolerance may
+    leave different constants there."""
+    from scipy import ndimage
+    nx, ny, nz = shape
+    t = np.asarray(typ).reshape(nz, ny, nx)
+    lab, n = ndimage.label(t == 1)
+    air = t == 0
+    near_air = np.zeros_like(air)
+    for ax in range(3):
+        near_air |= np.roll(air, 1, ax) & (np.arange(t.shape[ax]).reshape([-1 if a == ax else 1 for a in range(3)]) > 0)
+        near_air |= np.roll(air, -1, ax) & (np.arange(t.shape[ax]).reshape([-1 if a == ax else 1 for a in range(3)])
+                                            < t.shape[ax] - 1)
+    anchored = np.unique(lab[near_air & (lab > 0)])
+    sealed = np.setdiff1d(np.arange(1, n + 1), anchored)
+    pocket = np.where(np.isin(lab, sealed), lab, 0)
+    return pocket.ravel(), int(sealed.size)
+
+
+def remove_pocket_constants(x, ref, pocket):
+    """x with each sealed pocket shifted by the mean of ref - x over it."""
+    x = np.asarray(x, np.float64).copy()
+    for p in np.unique(pocket[pocket > 0]):
+        m = pocket == p
+        x[m] += float(np.mean(np.asarray(ref, np.float64)[m] - x[m]))
+    return x
+
+
 def u32(t):
     """torch int32 tensor holding u32 bits -> numpy uint32."""
     return t.cpu().numpy().view(np.uint32)
