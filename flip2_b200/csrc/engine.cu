@@ -952,7 +952,7 @@ static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
 }
 // one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is done)
 static int mg_cycle(flip_engine* e, bool network, const int* halt) {
-    const int grid0 = nat_grid(e, 4);
+    const int grid0 = nat_grid(e, 5);
     E_TRY(mg_down(e->mg, halt, grid0, e->stream));
     const float* zn = nullptr;
     if (network) {
@@ -1871,7 +1871,7 @@ extern "C" int flip_mg_train_step(flip_engine* e, int sample, float lr, double* 
         // the coarsest right-hand side that one V-cycle makes of the residual
         // after k Jacobi-PCG iterations, and its coarse solution (one-CTA CG)
         for (int k = 0; k < sample; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
-        E_TRY(mg_down(e->mg, nullptr, nat_grid(e, 4), e->stream));
+        E_TRY(mg_down(e->mg, nullptr, nat_grid(e, 5), e->stream));
         E_TRY(mg_cg(c, c.r, e->mg_ev, e->mg_s[0], e->mg_s[1], e->mg_s[2], 1e-6, 4000, e->mg_iters, e->stream));
         e->launches += 2u * (uint32_t)sample + (uint32_t)(e->mg.levels - 1) + 1u;
     } else {

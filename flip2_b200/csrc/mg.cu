@@ -92,63 +92,39 @@ __global__ void __launch_bounds__(512) mg_codes_kernel(MgLevel C, const int* hal
 
 // ------------------------------------------------------------ smoothing
 // The V-cycle's smoothing runs as two kernels per level.  Each CTA stages a
-// 12^3 box of its tile and a 2-cell halo in shared memory (cell codes, r and
-// the vector the sweeps start from); the first sweep is evaluated on the
-// 10^3 box of the tile and a 1-cell halo, the second (or the residual) on
-// the tile.  A neighbour that is not fluid contributes nothing, so halo cells
-// outside the grid or in tiles off the level's list (code 0) need no test
-// beyond the code.
-constexpr int kB12 = 12 * 12 * 12;
-constexpr int kB10 = 10 * 10 * 10;
-__device__ __forceinline__ void mg_origin(uint32_t key, const NatDims& D, int& ox, int& oy, int& oz) {
-    const uint32_t tyz = key / (uint32_t)D.tx;
-    ox = 8 * (int)(key - tyz * (uint32_t)D.tx);
-    oy = 8 * (int)(tyz % (uint32_t)D.ty);
-    oz = 8 * (int)(tyz / (uint32_t)D.ty);
-}
-// sum of the fluid neighbours' values of box cell b (row strides sx, sy, sz
-// = 1, W, W*W of a W-wide box), codes from the 12^3 box at b12
-__device__ __forceinline__ float mg_box_nb(const uint8_t* cb, int b12, const float* vb, int b, int W) {
-    const int W2 = W * W;
-    float s = 0.0f;
-    if (cb[b12 - 1] & kCellFluid) s += vb[b - 1];
-    if (cb[b12 + 1] & kCellFluid) s += vb[b + 1];
-    if (cb[b12 - 12] & kCellFluid) s += vb[b - W];
-    if (cb[b12 + 12] & kCellFluid) s += vb[b + W];
-    if (cb[b12 - 144] & kCellFluid) s += vb[b - W2];
-    if (cb[b12 + 144] & kCellFluid) s += vb[b + W2];
-    return s;
-}
-__device__ __forceinline__ int b12_of10(int v) {  // 10^3 box index -> 12^3 box index
-    const int x = v % 10, y = (v / 10) % 10, z = v / 100;
-    return (x + 1) + 12 * ((y + 1) + 12 * (z + 1));
-}
-
-// Both kernels run 256 threads per CTA (four CTAs per SM) and keep the
-// next tile's box loads in flight while the current tile computes.  A thread
-// owns up to seven box cells; which neighbour tile (3 x 3 x 3 around the
-// tile) and which slot in it each one is does not depend on the tile and is
-// worked out once.  Codes and values are loaded without waiting for the code
-// (every slot inside the grid is a valid address) and masked to the fluid
-// cells when they go to shared memory, where every vector is then zero off
-// the fluid cells: a neighbour sum needs no test.  1/d comes from a shared
-// table.
+// box of its tile and a 2-cell halo in shared memory: 16 cells wide in x
+// (x = -4 .. 11, so that every row is four 16-byte quads of the tile
+// layout: x 4..7 of the left tile, the tile's two quads, x 0..3 of the right
+// tile) and 12 in y and z (-2 .. 9).  The first sweep is evaluated on whole
+// quads of the rows y, z = -1 .. 8 (only x = -1 .. 8 of them is used), the
+// second sweep (or the residual) on the tile's 128 quads.  A thread handles
+// four cells: float4 global loads and stores, float4 shared rows.  Vectors
+// are zero off the fluid cells, so a neighbour sum needs no tests; 1/d comes
+// from a shared table.  Five CTAs per SM keep tiles in flight: one CTA's
+// loads overlap the others' barriers and arithmetic.
 constexpr int kMgThreads = 256;
-constexpr int kBoxPer = (kB12 + kMgThreads - 1) / kMgThreads;  // 7
-constexpr int kB10Per = (kB10 + kMgThreads - 1) / kMgThreads;  // 4
+constexpr int kBX = 16, kBY = 12, kBZ = 12;
+constexpr int kBoxQ = kBX * kBY * kBZ / 4;      // 576 quads in the box
+constexpr int kBoxF = kBX * kBY * kBZ;          // 2304 cells
+constexpr int kSw1Q = 4 * 10 * 10;              // 400 quads of the first sweep
+constexpr int kT1F = kBX * 10 * 10;             // its output box, 1600 cells
+constexpr int kQPer = (kBoxQ + kMgThreads - 1) / kMgThreads;  // 3
 
-// box cell v -> (neighbour tile offset + 1 per axis, local slot), packed
-// as local | (qx + 1) << 9 | (qy + 1) << 11 | (qz + 1) << 13; -1 past the box
-__device__ __forceinline__ int mg_box_map(int v) {
-    if (v >= kB12) return -1;
-    const int x = v % 12 - 2, y = (v / 12) % 12 - 2, z = v / 144 - 2;
-    const int qx = (x + 8) / 8 - 1, qy = (y + 8) / 8 - 1, qz = (z + 8) / 8 - 1;
-    const int local = (x - 8 * qx) | ((y - 8 * qy) << 3) | ((z - 8 * qz) << 6);
+// box quad q -> (neighbour tile offset + 1 per axis, local slot of its first
+// cell), packed as local | (qx + 1) << 9 | (qy + 1) << 11 | (qz + 1) << 13; -1 past the box
+__device__ __forceinline__ int mg_quad_map(int q) {
+    if (q >= kBoxQ) return -1;
+    const int seg = q & 3, row = q >> 2;
+    const int y = row % kBY - 2, z = row / kBY - 2;
+    const int qx = seg == 0 ? -1 : (seg == 3 ? 1 : 0);
+    const int lx = seg == 0 ? 4 : (seg == 3 ? 0 : 4 * (seg - 1));
+    const int qy = (y + 8) / 8 - 1, qz = (z + 8) / 8 - 1;
+    const int local = lx | ((y - 8 * qy) << 3) | ((z - 8 * qz) << 6);
     return local | ((qx + 1) << 9) | ((qy + 1) << 11) | ((qz + 1) << 13);
 }
-// slot of a mapped box cell around the tile at tile coordinates (tx, ty, tz),
-// or UINT32_MAX outside the grid; (i, j, k) of the cell out
-__device__ __forceinline__ uint32_t mg_map_slot(int map, int tx, int ty, int tz, const NatDims& D, int& i, int& j, int& k) {
+// slot of a mapped quad's first cell around the tile at tile coordinates
+// (tx, ty, tz), or UINT32_MAX outside the grid; the cell's (i, j, k) out
+__device__ __forceinline__ uint32_t mg_quad_slot(int map, int tx, int ty, int tz, const NatDims& D, int& i, int& j, int& k) {
     const int ntx = tx + ((map >> 9) & 3) - 1, nty = ty + ((map >> 11) & 3) - 1, ntz = tz + ((map >> 13) & 3) - 1;
     i = 8 * ntx + (map & 7);
     j = 8 * nty + ((map >> 3) & 7);
@@ -162,14 +138,41 @@ __device__ __forceinline__ void mg_tile_xyz(uint32_t key, const NatDims& D, int&
     ty = (int)(tyz % (uint32_t)D.ty);
     tz = (int)(tyz / (uint32_t)D.ty);
 }
-__device__ __forceinline__ float mg_sum6(const float* vb, int b, int W) {
-    return ((vb[b - 1] + vb[b + 1]) + (vb[b - W] + vb[b + W])) + (vb[b - W * W] + vb[b + W * W]);
-}
 __device__ __forceinline__ void mg_inv_table(float* inv) {
-    if (threadIdx.x < 8) {
-        const float d = (float)threadIdx.x;
-        inv[threadIdx.x] = threadIdx.x ? 1.0f / d : 0.0f;
+    if (threadIdx.x < 8) inv[threadIdx.x] = threadIdx.x ? 1.0f / (float)threadIdx.x : 0.0f;
+}
+__device__ __forceinline__ float f4(const float4& v, int m) { return m == 0 ? v.x : (m == 1 ? v.y : (m == 2 ? v.z : v.w)); }
+__device__ __forceinline__ void f4set(float4& v, int m, float x) {
+    if (m == 0) v.x = x; else if (m == 1) v.y = x; else if (m == 2) v.z = x; else v.w = x;
+}
+// one damped Jacobi sweep of a quad: out = u + w D^-1 (r - (d u - nb)) on its
+// fluid cells (0 elsewhere); nb: sums of the six neighbours per cell
+__device__ __forceinline__ float4 mg_quad_sweep(uint32_t c4, const float4& u, const float4& r, const float4& nb,
+                                                const float* inv) {
+    float4 o;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const uint32_t c = (c4 >> (8 * m)) & 0xFFu;
+        const float d = (float)(c & 7u);
+        const float um = f4(u, m);
+        f4set(o, m, (c & kCellFluid) ? um + kMgOmega * inv[c & 7u] * (f4(r, m) - (d * um - f4(nb, m))) : 0.0f);
     }
+    return o;
+}
+// neighbour sums of the quad at float index b of a box of row stride SY and
+// plane stride SZ (rows of 16 floats); qd = the quad's place in its row
+template <int SY, int SZ>
+__device__ __forceinline__ float4 mg_quad_nb(const float* v, int b, int qd) {
+    const float4 c = *reinterpret_cast<const float4*>(v + b);
+    const float4 ym = *reinterpret_cast<const float4*>(v + b - SY), yp = *reinterpret_cast<const float4*>(v + b + SY);
+    const float4 zm = *reinterpret_cast<const float4*>(v + b - SZ), zp = *reinterpret_cast<const float4*>(v + b + SZ);
+    const float l = qd > 0 ? v[b - 1] : 0.0f, r = qd < 3 ? v[b + 4] : 0.0f;
+    float4 s;
+    s.x = ((l + c.y) + (ym.x + yp.x)) + (zm.x + zp.x);
+    s.y = ((c.x + c.z) + (ym.y + yp.y)) + (zm.y + zp.y);
+    s.z = ((c.y + c.w) + (ym.z + yp.z)) + (zm.z + zp.z);
+    s.w = ((c.z + r) + (ym.w + yp.w)) + (zm.w + zp.w);
+    return s;
 }
 
 // pre-smoothing and restriction of level F into C:
@@ -177,84 +180,93 @@ __device__ __forceinline__ void mg_inv_table(float* inv) {
 //   C.r[parent] = 1/2 sum over the 8 children of r - A t (fluid parents; the
 //   parents of a tile are all written by it, and parents of tiles off the
 //   list are never fluid)
-__global__ void __launch_bounds__(kMgThreads, 4) mg_down_kernel(MgLevel F, MgLevel C, const int* halt) {
+__global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLevel C, const int* halt) {
     if (mg_halted(halt)) return;
-    __shared__ uint8_t cb[kB12];
-    __shared__ float rb[kB12];
-    __shared__ float t1b[kB12];
-    __shared__ float tb[kB10];
-    __shared__ float S[512];
+    __shared__ uint32_t cb[kBoxQ];                  // four codes per quad
+    __shared__ __align__(16) float rb[kBoxF];
+    __shared__ __align__(16) float ub[kBoxF];       // t1 = w D^-1 r
+    __shared__ __align__(16) float tb[kT1F];        // first sweep
+    __shared__ float S[256];                        // x-pair sums of the residual
     __shared__ float inv[8];
     mg_inv_table(inv);
     const int tid = threadIdx.x;
-    int map[kBoxPer], b10m[kB10Per];
+    int map[kQPer];
 #pragma unroll
-    for (int m = 0; m < kBoxPer; ++m) map[m] = mg_box_map(tid + m * kMgThreads);
-#pragma unroll
-    for (int m = 0; m < kB10Per; ++m) b10m[m] = tid + m * kMgThreads < kB10 ? b12_of10(tid + m * kMgThreads) : -1;
+    for (int m = 0; m < kQPer; ++m) map[m] = mg_quad_map(tid + m * kMgThreads);
     const uint32_t n = *F.d_ntiles;
-    uint8_t pc[kBoxPer];
-    float pr[kBoxPer];
+    uint32_t pc[kQPer];
+    float4 pr[kQPer];
     auto fetch = [&](uint32_t tt) {
         int tx, ty, tz, i, j, k;
         mg_tile_xyz(F.tiles[tt], F.D, tx, ty, tz);
 #pragma unroll
-        for (int m = 0; m < kBoxPer; ++m) {
-            const uint32_t sl = mg_map_slot(map[m], tx, ty, tz, F.D, i, j, k);
-            pc[m] = 0;
-            pr[m] = 0.0f;
+        for (int m = 0; m < kQPer; ++m) {
+            const uint32_t sl = mg_quad_slot(map[m], tx, ty, tz, F.D, i, j, k);
+            pc[m] = 0u;
+            pr[m] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (sl != 0xFFFFFFFFu) {
-                pc[m] = F.cell[sl];
-                pr[m] = F.r[sl];
+                pc[m] = *reinterpret_cast<const uint32_t*>(F.cell + sl);
+                pr[m] = *reinterpret_cast<const float4*>(F.r + sl);
             }
         }
     };
-    uint32_t tt = blockIdx.x;
-    if (tt < n) fetch(tt);
     __syncthreads();  // the 1/d table
-    for (; tt < n; tt += gridDim.x) {
+    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
         const uint32_t key = F.tiles[tt];
+        fetch(tt);
 #pragma unroll
-        for (int m = 0; m < kBoxPer; ++m) {
-            const int v = tid + m * kMgThreads;
-            if (v < kB12) {
-                const uint8_t c = pc[m];
-                const bool fl = (c & kCellFluid) != 0;
-                const float r = fl ? pr[m] : 0.0f;
-                cb[v] = c;
-                rb[v] = r;
-                t1b[v] = kMgOmega * inv[c & 7u] * r;
+        for (int m = 0; m < kQPer; ++m) {
+            const int q = tid + m * kMgThreads;
+            if (q < kBoxQ) {
+                const uint32_t c4 = pc[m];
+                float4 r, u;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t c = (c4 >> (8 * e)) & 0xFFu;
+                    const float rv = (c & kCellFluid) ? f4(pr[m], e) : 0.0f;
+                    f4set(r, e, rv);
+                    f4set(u, e, kMgOmega * inv[c & 7u] * rv);
+                }
+                cb[q] = c4;
+                *reinterpret_cast<float4*>(rb + 4 * q) = r;
+                *reinterpret_cast<float4*>(ub + 4 * q) = u;
             }
         }
         __syncthreads();
-        if (tt + gridDim.x < n) fetch(tt + gridDim.x);  // in flight during this tile's work
-#pragma unroll
-        for (int m = 0; m < kB10Per; ++m) {
-            const int b = b10m[m];
-            if (b < 0) continue;
-            const uint8_t c = cb[b];
-            const float t1 = t1b[b];
-            tb[tid + m * kMgThreads] = (c & kCellFluid) ? t1 + kMgOmega * inv[c & 7u] * (rb[b] - ((float)(c & 7u) * t1 - mg_sum6(t1b, b, 12))) : 0.0f;
+        for (int w = tid; w < kSw1Q; w += kMgThreads) {
+            const int qd = w & 3, row = w >> 2;
+            const int by = row % 10 + 1, bz = row / 10 + 1;
+            const int b = 4 * qd + kBX * (by + kBY * bz);
+            const float4 o = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(ub + b),
+                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * kBY>(ub, b, qd), inv);
+            *reinterpret_cast<float4*>(tb + 4 * qd + kBX * (row % 10 + 10 * (row / 10))) = o;
         }
         __syncthreads();
+        if (tid < 128) {
+            const int half = tid & 1, row = tid >> 1, ly = row & 7, lz = row >> 3;
+            const int qd = 1 + half;
+            const int b = 4 * qd + kBX * ((ly + 2) + kBY * (lz + 2));
+            const int t = 4 * qd + kBX * ((ly + 1) + 10 * (lz + 1));
+            const uint32_t c4 = cb[b >> 2];
+            const float4 tv = *reinterpret_cast<const float4*>(tb + t), r = *reinterpret_cast<const float4*>(rb + b);
+            const float4 nb = mg_quad_nb<kBX, kBX * 10>(tb, t, qd);
+            float res[4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int cidx = tid + h * kMgThreads;
-            const int li = cidx & 7, lj = (cidx >> 3) & 7, lk = cidx >> 6;
-            const int b12 = (li + 2) + 12 * ((lj + 2) + 12 * (lk + 2));
-            const int b10 = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
-            const uint8_t c = cb[b12];
-            const float tv = tb[b10];
-            F.t[(key << 9) | cidx] = tv;
-            S[cidx] = (c & kCellFluid) ? rb[b12] - ((float)(c & 7u) * tv - mg_sum6(tb, b10, 10)) : 0.0f;
+            for (int m = 0; m < 4; ++m) {
+                const uint32_t c = (c4 >> (8 * m)) & 0xFFu;
+                res[m] = (c & kCellFluid) ? f4(r, m) - ((float)(c & 7u) * f4(tv, m) - f4(nb, m)) : 0.0f;
+            }
+            *reinterpret_cast<float4*>(F.t + ((key << 9) | (uint32_t)(4 * half + 8 * ly + 64 * lz))) = tv;
+            S[(2 * half) + 4 * (ly + 8 * lz)] = res[0] + res[1];
+            S[(2 * half + 1) + 4 * (ly + 8 * lz)] = res[2] + res[3];
         }
         __syncthreads();
-        if (tid < 64) {  // the (even, even, even) child of each 2^3 block
+        if (tid < 64) {  // parent (pi, pj, pk) of the tile's 4^3 parents
             int tx, ty, tz;
             mg_tile_xyz(key, F.D, tx, ty, tz);
             const int pi = tid & 3, pj = (tid >> 2) & 3, pk = tid >> 4;
-            const int b = 2 * pi + 16 * pj + 128 * pk;
-            const float sum = ((S[b] + S[b + 1]) + (S[b + 8] + S[b + 9])) + ((S[b + 64] + S[b + 65]) + (S[b + 72] + S[b + 73]));
+            const int s0 = pi + 4 * (2 * pj + 8 * 2 * pk);
+            const float sum = (S[s0] + S[s0 + 4]) + (S[s0 + 32] + S[s0 + 36]);
             const uint32_t p = mg_slot(4 * tx + pi, 4 * ty + pj, 4 * tz + pk, C.D);
             C.r[p] = (C.cell[p] & kCellFluid) ? 0.5f * sum : 0.0f;
         }
@@ -268,86 +280,104 @@ __global__ void __launch_bounds__(kMgThreads, 4) mg_down_kernel(MgLevel F, MgLev
 // coarsest level with the network output zn); MODE 2: u = w D^-1 r (the
 // coarsest level without the network).
 template <int MODE>
-__global__ void __launch_bounds__(kMgThreads, 4) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
+__global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
                                                                   const int* halt) {
     if (mg_halted(halt)) return;
-    __shared__ uint8_t cb[kB12];
-    __shared__ float rb[kB12];
-    __shared__ float ub[kB12];
-    __shared__ float tb[kB10];
+    __shared__ uint32_t cb[kBoxQ];
+    __shared__ __align__(16) float rb[kBoxF];
+    __shared__ __align__(16) float ub[kBoxF];
+    __shared__ __align__(16) float tb[kT1F];
     __shared__ float inv[8];
     mg_inv_table(inv);
     const int tid = threadIdx.x;
-    int map[kBoxPer], b10m[kB10Per];
+    int map[kQPer];
 #pragma unroll
-    for (int m = 0; m < kBoxPer; ++m) map[m] = mg_box_map(tid + m * kMgThreads);
-#pragma unroll
-    for (int m = 0; m < kB10Per; ++m) b10m[m] = tid + m * kMgThreads < kB10 ? b12_of10(tid + m * kMgThreads) : -1;
+    for (int m = 0; m < kQPer; ++m) map[m] = mg_quad_map(tid + m * kMgThreads);
     const uint32_t n = *L.d_ntiles;
-    uint8_t pc[kBoxPer];
-    float pr[kBoxPer], pu[kBoxPer];
+    uint32_t pc[kQPer];
+    float4 pr[kQPer], pu[kQPer];
+    float2 pe[kQPer];      // MODE 0: the two parents' corrections
+    uint32_t pp[kQPer];    // MODE 0: the two parents' codes
     auto fetch = [&](uint32_t tt) {
         int tx, ty, tz, i, j, k;
         mg_tile_xyz(L.tiles[tt], L.D, tx, ty, tz);
 #pragma unroll
-        for (int m = 0; m < kBoxPer; ++m) {
-            const uint32_t sl = mg_map_slot(map[m], tx, ty, tz, L.D, i, j, k);
-            pc[m] = 0;
-            pr[m] = 0.0f;
-            pu[m] = 0.0f;
+        for (int m = 0; m < kQPer; ++m) {
+            const uint32_t sl = mg_quad_slot(map[m], tx, ty, tz, L.D, i, j, k);
+            pc[m] = 0u;
+            pp[m] = 0u;
+            pr[m] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            pu[m] = pr[m];
+            pe[m] = make_float2(0.0f, 0.0f);
             if (sl != 0xFFFFFFFFu) {
-                pc[m] = L.cell[sl];
-                pr[m] = L.r[sl];
+                pc[m] = *reinterpret_cast<const uint32_t*>(L.cell + sl);
+                pr[m] = *reinterpret_cast<const float4*>(L.r + sl);
                 if (MODE == 0) {
-                    // the parent's correction; a parent that is not fluid
-                    // may sit in a tile off the coarse list (stale z)
+                    pu[m] = *reinterpret_cast<const float4*>(L.t + sl);
+                    // parents of x, x+1 and of x+2, x+3: consecutive coarse cells
                     const uint32_t ps = mg_slot(i >> 1, j >> 1, k >> 1, C.D);
-                    pu[m] = L.t[sl] + ((C.cell[ps] & kCellFluid) ? C.z[ps] : 0.0f);
+                    pe[m] = *reinterpret_cast<const float2*>(C.z + ps);
+                    pp[m] = *reinterpret_cast<const uint16_t*>(C.cell + ps);
+                } else if (MODE == 1) {
+                    pu[m] = *reinterpret_cast<const float4*>(zn + sl);
                 }
-                else if (MODE == 1) pu[m] = zn[sl];
             }
         }
     };
-    uint32_t tt = blockIdx.x;
-    if (tt < n) fetch(tt);
     __syncthreads();  // the 1/d table
-    for (; tt < n; tt += gridDim.x) {
+    for (uint32_t tt = blockIdx.x; tt < n; tt += gridDim.x) {
         const uint32_t key = L.tiles[tt];
+        fetch(tt);
 #pragma unroll
-        for (int m = 0; m < kBoxPer; ++m) {
-            const int v = tid + m * kMgThreads;
-            if (v < kB12) {
-                const uint8_t c = pc[m];
-                const bool fl = (c & kCellFluid) != 0;
-                const float r = fl ? pr[m] : 0.0f;
-                float u = 0.0f;
-                if (fl) u = MODE == 0 ? pu[m] : (MODE == 1 ? pu[m] + inv[c & 7u] * r : kMgOmega * inv[c & 7u] * r);
-                cb[v] = c;
-                rb[v] = r;
-                ub[v] = u;
+        for (int m = 0; m < kQPer; ++m) {
+            const int q = tid + m * kMgThreads;
+            if (q < kBoxQ) {
+                const uint32_t c4 = pc[m];
+                float4 r, u;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t c = (c4 >> (8 * e)) & 0xFFu;
+                    const bool fl = (c & kCellFluid) != 0;
+                    const float rv = fl ? f4(pr[m], e) : 0.0f;
+                    float uv = 0.0f;
+                    if (fl) {
+                        if (MODE == 0) {
+                            // a parent that is not fluid may sit in a tile off
+                            // the coarse list (stale z): it contributes nothing
+                            const uint32_t cp = (pp[m] >> (8 * (e >> 1))) & 0xFFu;
+                            uv = f4(pu[m], e) + ((cp & kCellFluid) ? (e < 2 ? pe[m].x : pe[m].y) : 0.0f);
+                        } else if (MODE == 1) {
+                            uv = f4(pu[m], e) + inv[c & 7u] * rv;
+                        } else {
+                            uv = kMgOmega * inv[c & 7u] * rv;
+                        }
+                    }
+                    f4set(r, e, rv);
+                    f4set(u, e, uv);
+                }
+                cb[q] = c4;
+                *reinterpret_cast<float4*>(rb + 4 * q) = r;
+                *reinterpret_cast<float4*>(ub + 4 * q) = u;
             }
         }
         __syncthreads();
-        if (tt + gridDim.x < n) fetch(tt + gridDim.x);  // in flight during this tile's work
-#pragma unroll
-        for (int m = 0; m < kB10Per; ++m) {
-            const int b = b10m[m];
-            if (b < 0) continue;
-            const uint8_t c = cb[b];
-            const float u = ub[b];
-            tb[tid + m * kMgThreads] = (c & kCellFluid) ? u + kMgOmega * inv[c & 7u] * (rb[b] - ((float)(c & 7u) * u - mg_sum6(ub, b, 12))) : 0.0f;
+        for (int w = tid; w < kSw1Q; w += kMgThreads) {
+            const int qd = w & 3, row = w >> 2;
+            const int by = row % 10 + 1, bz = row / 10 + 1;
+            const int b = 4 * qd + kBX * (by + kBY * bz);
+            const float4 o = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(ub + b),
+                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * kBY>(ub, b, qd), inv);
+            *reinterpret_cast<float4*>(tb + 4 * qd + kBX * (row % 10 + 10 * (row / 10))) = o;
         }
         __syncthreads();
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int cidx = tid + h * kMgThreads;
-            const int li = cidx & 7, lj = (cidx >> 3) & 7, lk = cidx >> 6;
-            const int b12 = (li + 2) + 12 * ((lj + 2) + 12 * (lk + 2));
-            const int b10 = (li + 1) + 10 * ((lj + 1) + 10 * (lk + 1));
-            const uint8_t c = cb[b12];
-            const float tv = tb[b10];
-            L.z[(key << 9) | cidx] =
-                (c & kCellFluid) ? tv + kMgOmega * inv[c & 7u] * (rb[b12] - ((float)(c & 7u) * tv - mg_sum6(tb, b10, 10))) : 0.0f;
+        if (tid < 128) {
+            const int half = tid & 1, row = tid >> 1, ly = row & 7, lz = row >> 3;
+            const int qd = 1 + half;
+            const int b = 4 * qd + kBX * ((ly + 2) + kBY * (lz + 2));
+            const int t = 4 * qd + kBX * ((ly + 1) + 10 * (lz + 1));
+            const float4 z = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(tb + t),
+                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * 10>(tb, t, qd), inv);
+            *reinterpret_cast<float4*>(L.z + ((key << 9) | (uint32_t)(4 * half + 8 * ly + 64 * lz))) = z;
         }
         __syncthreads();
     }
@@ -469,11 +499,11 @@ int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels) {
     return levels;
 }
 
-// CTAs of the smoothing kernels: four per SM (grid0 on level 0) and no more
+// CTAs of the smoothing kernels: five per SM (grid0 on level 0) and no more
 // than the level has tiles
 static int mg_grid(const MgLevel& L, int grid0, int level) {
     if (level == 0) return grid0;
-    return (int)(L.ntiles < 592u ? L.ntiles : 592u);
+    return (int)(L.ntiles < 740u ? L.ntiles : 740u);
 }
 
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
@@ -504,7 +534,7 @@ int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
 int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s) {
     const int c = H.levels - 1;
     const MgLevel& L = H.L[c];
-    const int g = mg_grid(L, 592, c);
+    const int g = mg_grid(L, 740, c);
     if (zn) mg_sweeps_kernel<1><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
     else mg_sweeps_kernel<2><<<g, kMgThreads, 0, s>>>(L, L, nullptr, halt);
     FLIP_CUDA_TRY(cudaGetLastError());
