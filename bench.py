@@ -76,8 +76,9 @@ def c4_pressure(F, device):
     the box, fluid surface at 50-85% height, Gaussian impulses plus gravity),
     solved to 1e-6 by Jacobi-PCG and by the learned multilevel FCG
     (pressure_method 2: V-cycle whose 16^3 coarsest level the committed
-    network solves), by the same V-cycle without the network, and by FCG
-    with the network on the solver's grid (pressure_method 1, committed
+    network solves), by the same V-cycle without the network and with a
+    one-CTA Jacobi-PCG on the coarsest level instead of the network, and by
+    FCG with the network on the solver's grid (pressure_method 1, committed
     weights, Jacobi-PCG restart after 100 iterations).  Device ms from CUDA
     events inside the engine; the relative residuals are FP64 true
     residuals."""
@@ -87,12 +88,13 @@ def c4_pressure(F, device):
     R = C4_CELLS // 4
     engines = {}
     for name, kw, wfile in (("learned", {}, "mg_weights.npy"), ("no_network", {"mg_coarse": 1}, "mg_weights.npy"),
+                            ("coarse_cg", {"mg_coarse": 2}, "mg_weights.npy"),
                             ("fine_grid_network", {}, "lprec_weights.npy")):
         P = F.Particles(1, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE, device=device, **kw))
         P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
         P.lp_set_weights(np.load(os.path.join(data, wfile)))
         engines[name] = P
-    method = {"learned": 2, "no_network": 2, "fine_grid_network": 1}
+    method = {"learned": 2, "no_network": 2, "coarse_cg": 2, "fine_grid_network": 1}
     for name, P in engines.items():  # warm-up: graphs and buffers
         P.poisson_generate(seed=C4_SEED0)
         P.poisson_solve(0, 1e-6, 20000)
@@ -115,9 +117,10 @@ def c4_pressure(F, device):
     return {"workload": "128^3 generated pressure problems (seeds %d..%d), tol 1e-6" % (C4_SEED0, C4_SEED0 + C4_PROBLEMS - 1),
             "learned": "pressure_method 2: FCG, V-cycle (damped Jacobi, 4 levels) with the network solving the 16^3 level",
             "plain_ms_mean": mean("plain_ms"), "learned_ms_mean": mean("learned_ms"),
-            "no_network_ms_mean": mean("no_network_ms"), "fine_grid_network_ms_mean": mean("fine_grid_network_ms"),
+            "no_network_ms_mean": mean("no_network_ms"), "coarse_cg_ms_mean": mean("coarse_cg_ms"),
+            "fine_grid_network_ms_mean": mean("fine_grid_network_ms"),
             "plain_iters_mean": mean("plain_iters"), "learned_iters_mean": mean("learned_iters"),
-            "no_network_iters_mean": mean("no_network_iters"),
+            "no_network_iters_mean": mean("no_network_iters"), "coarse_cg_iters_mean": mean("coarse_cg_iters"),
             "speedup_learned_over_plain": mean("plain_ms") / mean("learned_ms"),
             "speedup_learned_over_no_network": mean("no_network_ms") / mean("learned_ms"),
             "fallback_rate": mean("learned_fell_back"), "problems": rows}

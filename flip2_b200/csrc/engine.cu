@@ -948,20 +948,32 @@ static int mg_net_forward(flip_engine* e, const LpGrid& G) {
 }
 // kernels of one V-cycle (for the launch count)
 static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
-    return 2u * (uint32_t)(e->mg.levels - 1) + 1u + (network ? 5u : 0u);
+    const uint32_t coarse = network ? 5u : (e->P.mg_coarse == 2 ? 1u : 0u);
+    return 2u * (uint32_t)(e->mg.levels - 1) + 1u + coarse;
 }
+// coarse CG of mg_coarse = 2: relative tolerance and iteration cap
+constexpr double kMgCoarseCgTol = 1e-3;
+constexpr int kMgCoarseCgIters = 64;
 // one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is done)
 static int mg_cycle(flip_engine* e, bool network, const int* halt) {
     const int grid0 = nat_grid(e, 5);
     E_TRY(mg_down(e->mg, halt, grid0, e->stream));
     const float* zn = nullptr;
+    bool solved = false;
     if (network) {
         const LpGrid G = mg_lp_grid(e, halt);
         E_TRY(mg_input_scale(e->mg, halt, e->stream));
         E_TRY(mg_net_forward(e, G));
         zn = e->mg_zn;
+    } else if (e->P.mg_coarse == 2) {
+        // the classical comparison: Jacobi-PCG on the coarsest level in one CTA
+        const MgLevel& c = e->mg.L[e->mg.levels - 1];
+        E_TRY(mg_cg(c, c.r, e->mg_zn, e->mg_s[0], e->mg_s[1], e->mg_s[2], kMgCoarseCgTol, kMgCoarseCgIters, e->mg_iters,
+                    e->stream, halt));
+        zn = e->mg_zn;
+        solved = true;
     }
-    E_TRY(mg_coarsest(e->mg, zn, halt, e->stream));
+    E_TRY(mg_coarsest(e->mg, zn, halt, e->stream, solved));
     E_TRY(mg_up(e->mg, halt, grid0, e->stream));
     return FLIP_OK;
 }
@@ -1013,7 +1025,7 @@ static int nat_fpcg_graph(flip_engine* e, int iters, int max_iter) {
 
 static int nat_mgpcg_graph(flip_engine* e, int iters, int max_iter, bool network) {
     const int limit = loop_limit(max_iter, iters);
-    const int mode = network ? 0 : 1;
+    const int mode = network ? 0 : e->P.mg_coarse;
     if (e->mg_graph && e->mg_graph_iters == iters && e->mg_graph_limit == limit && e->mg_graph_coarse == mode)
         return FLIP_OK;
     if (e->mg_graph) { cudaGraphExecDestroy(e->mg_graph); e->mg_graph = nullptr; }

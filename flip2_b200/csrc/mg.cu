@@ -278,7 +278,8 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
 // L.z = t2 + w D^-1 (r - A t2).  MODE 0: u = L.t + C.z[parent] (prolongation
 // of the coarse correction; post-smoothing); MODE 1: u = zn + D^-1 r (the
 // coarsest level with the network output zn); MODE 2: u = w D^-1 r (the
-// coarsest level without the network).
+// coarsest level without the network); MODE 3: u = zn (the coarsest level
+// after a CG solve into zn).
 template <int MODE>
 __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
                                                                   const int* halt) {
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
                     const uint32_t ps = mg_slot(i >> 1, j >> 1, k >> 1, C.D);
                     pe[m] = *reinterpret_cast<const float2*>(C.z + ps);
                     pp[m] = *reinterpret_cast<const uint16_t*>(C.cell + ps);
-                } else if (MODE == 1) {
+                } else if (MODE == 1 || MODE == 3) {
                     pu[m] = *reinterpret_cast<const float4*>(zn + sl);
                 }
             }
@@ -348,6 +349,8 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
                             uv = f4(pu[m], e) + ((cp & kCellFluid) ? (e < 2 ? pe[m].x : pe[m].y) : 0.0f);
                         } else if (MODE == 1) {
                             uv = f4(pu[m], e) + inv[c & 7u] * rv;
+                        } else if (MODE == 3) {
+                            uv = f4(pu[m], e);
                         } else {
                             uv = kMgOmega * inv[c & 7u] * rv;
                         }
@@ -409,7 +412,8 @@ __global__ void __launch_bounds__(1024) mg_scale_kernel(MgLevel L, float* inv_s,
 // the training targets of the coarsest solve.
 __global__ void __launch_bounds__(1024) mg_cg_kernel(MgLevel L, const float* __restrict__ b, float* __restrict__ x,
                                                      float* __restrict__ r, float* __restrict__ p, float* __restrict__ q,
-                                                     double tol, int max_iter, int* iters) {
+                                                     double tol, int max_iter, int* iters, const int* halt) {
+    if (mg_halted(halt)) return;
     __shared__ double sh[32];
     __shared__ double bc;
     const uint32_t n = *L.d_ntiles * 512u;
@@ -531,11 +535,12 @@ int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
     return FLIP_OK;
 }
 
-int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s) {
+int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s, bool solved) {
     const int c = H.levels - 1;
     const MgLevel& L = H.L[c];
     const int g = mg_grid(L, 740, c);
-    if (zn) mg_sweeps_kernel<1><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
+    if (zn && solved) mg_sweeps_kernel<3><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
+    else if (zn) mg_sweeps_kernel<1><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
     else mg_sweeps_kernel<2><<<g, kMgThreads, 0, s>>>(L, L, nullptr, halt);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
@@ -549,8 +554,8 @@ int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
 }
 
 int mg_cg(const MgLevel& L, const float* b, float* x, float* r, float* p, float* q, double tol, int max_iter, int* iters,
-          cudaStream_t s) {
-    mg_cg_kernel<<<1, 1024, 0, s>>>(L, b, x, r, p, q, tol, max_iter, iters);
+          cudaStream_t s, const int* halt) {
+    mg_cg_kernel<<<1, 1024, 0, s>>>(L, b, x, r, p, q, tol, max_iter, iters, halt);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

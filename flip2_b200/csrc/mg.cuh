@@ -64,8 +64,9 @@ int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s);
 // side ends in L[levels-1].r)
 int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
 // the coarsest level's solve around a network output zn (nullptr: no
-// network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps (one kernel)
-int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s);
+// network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps (one kernel);
+// solved: zn is already a coarse solution (z = zn, then the sweeps)
+int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s, bool solved = false);
 // prolongation and post-smoothing back up to level 0, one kernel per level
 // (the output in L[0].z)
 int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
@@ -73,7 +74,7 @@ int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
 // max_iter iterations; *iters = iterations run); r, p, q: scratch of the
 // level's size
 int mg_cg(const MgLevel& L, const float* b, float* x, float* r, float* p, float* q, double tol, int max_iter, int* iters,
-          cudaStream_t s);
+          cudaStream_t s, const int* halt = nullptr);
 // *inv_s = 1 / rms(r) over the fluid cells of the coarsest level (one CTA)
 int mg_input_scale(const MgHierarchy& H, const int* halt, cudaStream_t s);
 

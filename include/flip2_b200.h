@@ -174,7 +174,9 @@ typedef struct {
                                     fluid in both; the stop test stays |r| <= tol |b| */
     int32_t mg_coarse;           /* NATIVE, pressure_method 2: 0 (default) solves the
                                     coarsest level with the network, 1 with Jacobi
-                                    sweeps only (the same V-cycle without the network) */
+                                    sweeps only (the same V-cycle without the network),
+                                    2 with Jacobi-PCG in one CTA (relative tolerance
+                                    1e-3, at most 64 iterations; for comparison)       */
 } flip_params;
 
 /* Defaults for a mode (reference constants for FLIP_MODE_REFERENCE). */

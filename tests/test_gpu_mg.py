@@ -120,3 +120,15 @@ def test_native_step_with_method_2(torch):
     assert rel_err(phi2, phi0) < 2e-3
     for k in range(3):
         assert np.max(np.abs(np.sort(p2[:, k]) - np.sort(p0[:, k]))) < 1e-3 * (4.0 / nc)
+
+
+def test_coarse_cg_comparison_mode(torch):
+    # mg_coarse = 2 (one-CTA Jacobi-PCG on the coarsest level, a comparison
+    # without the network) is a valid preconditioner too: FCG meets tol
+    shape = (64, 64, 64)
+    P = mg_engine(shape, 2, seed=11)
+    info = P.poisson_solve(method=2, tol=1e-6, max_iter=400)
+    assert info.converged == 1 and info.fell_back == 0
+    typ, b = problem_arrays(P, shape)
+    assert solution_residual(typ, b, P.poisson_solution(), shape) <= 1.05e-6
+    P.close()
