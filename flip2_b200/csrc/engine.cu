@@ -1074,11 +1074,14 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         e->h_state->true_every = chunk;
         e->h_state->next_check = chunk;
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
-        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream));
+        // warm start as for Jacobi-PCG: from the previous step's pressure on
+        // the cells fluid in both solves (r = b - A x0 in FP64)
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
+                                  warm ? e->cell_prev : nullptr));
         E_TRY(mg_setup_problem(e, network));
         E_TRY(mg_cycle(e, network, &e->pcg.st->halt));
         E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream, 0));
-        e->launches += 2u + mg_cycle_launches(e, network);
+        e->launches += (warm ? 3u : 2u) + mg_cycle_launches(e, network);
         E_TRY(e->mark(9));
         E_TRY(nat_mgpcg_graph(e, chunk, max_learned, network));
         E_TRY(run_loop(e, e->mg_graph, (3u + mg_cycle_launches(e, network)) * (uint32_t)chunk + 1u));
@@ -1458,6 +1461,12 @@ extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64
         E_CUDA(cudaMemcpyAsync(e->h_small, e->d_counts, 8, cudaMemcpyDeviceToHost, e->stream));
         E_CUDA(cudaStreamSynchronize(e->stream));
         e->nodes = e->h_small[0];
+    }
+    if (!ref && which == FLIP_BUF_PRESSURE && e->pcg.x) {
+        // the solver keeps the increments since its last true-residual check
+        // in the FP32 part xg: hand out the whole solution
+        E_TRY(nat_launch_fold_pressure(e->pcg.x, e->pcg.xg, e->pcg.cell, e->nslots, e->stream));
+        e->launches += 1;
     }
     void* p = nullptr;
     uint64_t c = 0;

@@ -251,6 +251,15 @@ __global__ void nat_mark_fluid_tiles_kernel(const uint8_t* __restrict__ type, ui
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nslots && type[s] == kFluid) flags[s >> 9] = 1;
 }
+// the solution x + xg into x on the fluid cells of the last solve, 0
+// elsewhere; xg = 0 (the pressure buffer a caller reads)
+__global__ void nat_fold_pressure_kernel(double* __restrict__ x, float* __restrict__ xg, const uint8_t* __restrict__ cell,
+                                         uint64_t nslots) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    x[s] = (cell[s] & kCellFluid) ? x[s] + (double)xg[s] : 0.0;
+    xg[s] = 0.0f;
+}
 // x-fastest linear array -> tile-blocked slots (and back)
 __global__ void nat_lin_tiles_f32_kernel(const float* __restrict__ src, float* __restrict__ dst, NatDims D, int to_tiles) {
     const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1081,6 +1090,11 @@ int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_
     FLIP_CUDA_TRY(cudaMemsetAsync(flags, 0, ntiles_total, s));
     nat_mark_fluid_tiles_kernel<<<nb(nslots, 256), 256, 0, s>>>(type, flags, nslots);
     nat_compact_kernel<<<1, kCompactThreads, 0, s>>>(flags, ntiles_total, list, d_count);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_fold_pressure(double* x, float* xg, const uint8_t* cell, uint64_t nslots, cudaStream_t s) {
+    nat_fold_pressure_kernel<<<nb(nslots, 256), 256, 0, s>>>(x, xg, cell, nslots);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -72,6 +72,8 @@ int nat_launch_poisson_gen(const NatDims& D, float surface, const float4* sph, i
 int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_total, uint32_t* list, uint32_t* d_count,
                            uint64_t nslots, cudaStream_t s);
 int nat_launch_lin_tiles_f32(const float* src, float* dst, const NatDims& D, int to_tiles, cudaStream_t s);
+// x = x + xg on the fluid cells of the last solve (0 elsewhere), xg = 0
+int nat_launch_fold_pressure(double* x, float* xg, const uint8_t* cell, uint64_t nslots, cudaStream_t s);
 int nat_launch_solution_lin(const double* x, const float* xg, const uint8_t* cell, const NatDims& D, double* out,
                             cudaStream_t s);
 int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots, cudaStream_t s);

@@ -170,8 +170,9 @@ typedef struct {
     int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers on CUDA
                                     cores instead of tcgen05 (for comparison)         */
     int32_t pcg_warm_start;      /* NATIVE: 1 (default) starts each step's Jacobi-PCG
-                                    from the previous step's pressure on the cells
-                                    fluid in both; the stop test stays |r| <= tol |b| */
+                                    or multilevel FCG (pressure_method 0 or 2) from
+                                    the previous step's pressure on the cells fluid in
+                                    both; the stop test stays |r| <= tol |b|          */
     int32_t mg_coarse;           /* NATIVE, pressure_method 2: 0 (default) solves the
                                     coarsest level with the network, 1 with Jacobi
                                     sweeps only (the same V-cycle without the network),
@@ -261,7 +262,9 @@ typedef enum {
     FLIP_BUF_GRID_U_P2G, FLIP_BUF_GRID_V_P2G, FLIP_BUF_GRID_W_P2G,
     FLIP_BUF_COUNT
 } flip_buffer;
-/* elem_size: 1, 4 or 8 bytes; count: number of valid elements. */
+/* elem_size: 1, 4 or 8 bytes; count: number of valid elements.
+ * NATIVE FLIP_BUF_PRESSURE (FP64): the last solve's pressure on its fluid
+ * cells, 0 elsewhere (the call first folds the solver's FP32 increments in). */
 int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64_t* count, uint32_t* elem_size);
 /* Copy a buffer of flip_get_buffer to host memory (bytes <= count*elem_size),
  * synchronising the engine stream; CudaVec::download (cudaVec.cu:80-86). */
