@@ -327,8 +327,14 @@ static int lp_small_pass(const LpNet& net, const LpGrid& G, const float* d_inv_s
                          const float* f0, int raw, float* z, uint32_t ntiles, cudaStream_t st) {
     const int g = (int)(ntiles * 512u / kSmallVox);
     lp_small_in_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, acts[0]);
-    lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1]);
-    lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2]);
+    if (net.tensor_cores) {
+        int rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1], net.err, ntiles, st);
+        if (rc == FLIP_OK) rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2], net.err, ntiles, st);
+        if (rc != FLIP_OK) return rc;
+    } else {
+        lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1]);
+        lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2]);
+    }
     lp_small_out_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], acts[2], d_inv_s, f0, raw, z);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;

@@ -69,6 +69,10 @@ int lp_bias_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, float* 
 // z = N(r) given f0
 int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, const float* f0, float* z, int grid,
                    cudaStream_t st);
+// one 16 -> 16 layer on a small grid whose every tile is active, on the
+// tensor cores: a CTA per 128 voxels (lprec_tc.cu)
+int lp_small_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
+                            int* err, uint32_t ntiles, cudaStream_t st);
 // the same two passes on a small grid whose every tile is in G's tile lists
 // (ntiles tiles, the coarsest level of the multilevel preconditioner): a CTA
 // per 16 voxels

@@ -257,6 +257,161 @@ static int launch_mid_tc(const LpGrid& G, const __nv_bfloat16* wb, const __nv_bf
     return FLIP_OK;
 }
 
+// ------------------------------------------------------------ small grids
+// The 16 -> 16 layers on a small grid whose every tile is active (the
+// coarsest level of the multilevel preconditioner, at most 4,096 voxels):
+// one CTA per 128 consecutive voxels of the tile list.  The CTA gathers, for
+// each of the 27 taps, its voxels' 16 input channels into an A operand of
+// 128 rows (K-major, no swizzle: rows 16 B apart, 8-row groups 128 B apart,
+// the two 8-channel halves 2 KB apart), so that one thread issues 27 MMAs of
+// M=128 x N=16 x K=16 into one TMEM accumulator (row m in lane m).  Warps 0-3
+// read their 32 lanes back, apply ReLU and store BF16.  Waits are bounded as
+// in the per-tile kernel above.
+namespace {
+constexpr int kSmTcThreads = 256;
+constexpr int kSmTcRows = 128;
+constexpr int kSmTcA = 27 * kSmTcRows * 32;  // 27 taps x 128 rows x 16 BF16
+constexpr int kSmTcW = 27 * 512;
+constexpr int kSmTcBytes = kSmTcA + kSmTcW + 64;
+constexpr uint32_t kInstrDescM128 = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+}  // namespace
+
+__global__ void __launch_bounds__(kSmTcThreads) lp_small_mid_tc_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
+                                                                       const __nv_bfloat16* __restrict__ in,
+                                                                       __nv_bfloat16* __restrict__ out, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* asm_ = smem;
+    unsigned char* wsm = smem + kSmTcA;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kSmTcA + kSmTcW);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kSmTcA + kSmTcW + 16);
+    __shared__ int s_abort;
+    if (G.halt && *G.halt) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t nvox = *G.d_nact * 512u;
+    const uint32_t v0 = blockIdx.x * kSmTcRows;
+    if (v0 >= nvox) return;
+    // weights: global [tap][ci][co] -> per tap [ci/8][co][ci%8]; 27 per thread,
+    // loaded in batches of nine before they are stored
+#pragma unroll
+    for (int m0 = 0; m0 < 27; m0 += 9) {
+        __nv_bfloat16 w[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) w[j] = wb[tid + (m0 + j) * kSmTcThreads];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            const int e = tid + (m0 + j) * kSmTcThreads;
+            const int tap = e >> 8, ci = (e >> 4) & 15, co = e & 15;
+            *reinterpret_cast<__nv_bfloat16*>(wsm + tap * 512 + (ci >> 3) * 256 + co * 16 + (ci & 7) * 2) = w[j];
+        }
+    }
+    // A: for each tap, row r = voxel v0 + r, half h = channels 8h .. 8h+7.
+    // A thread keeps one (row, half) and walks the 27 taps: its voxel is
+    // worked out once, and the taps' loads go out nine at a time.
+    {
+        const int h = tid & 1, r = tid >> 1;  // 256 threads = 128 rows x 2 halves
+        const uint32_t vx = v0 + (uint32_t)r;
+        int ci = 0, cj = 0, ck = 0;
+        const bool have = vx < nvox;
+        if (have) {
+            int ox, oy, oz;
+            tile_origin_tc(G.act_tiles[vx >> 9], G.D, ox, oy, oz);
+            const int l = (int)(vx & 511u);
+            ci = ox + (l & 7);
+            cj = oy + ((l >> 3) & 7);
+            ck = oz + (l >> 6);
+        }
+        unsigned char* dst = asm_ + h * (kSmTcRows * 16) + r * 16;
+#pragma unroll
+        for (int t0 = 0; t0 < 27; t0 += 9) {
+            uint4 val[9];
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                const int tap = t0 + j;
+                const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                const int gx = ci + dil * dx, gy = cj + dil * dy, gz = ck + dil * dz;
+                val[j] = make_uint4(0u, 0u, 0u, 0u);
+                if (have && gx >= 0 && gy >= 0 && gz >= 0 && gx < G.D.nx && gy < G.D.ny && gz < G.D.nz) {
+                    const uint32_t tt = (uint32_t)((gx >> 3) + G.D.tx * ((gy >> 3) + G.D.ty * (gz >> 3)));
+                    const uint32_t sl = (tt << 9) | (uint32_t)((gx & 7) | ((gy & 7) << 3) | ((gz & 7) << 6));
+                    val[j] = *reinterpret_cast<const uint4*>(in + (size_t)sl * 16 + h * 8);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 9; ++j) *reinterpret_cast<uint4*>(dst + (t0 + j) * (kSmTcRows * 32)) = val[j];
+        }
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(32)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // the generic-proxy stores above become visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t a_s = smem_u32(asm_), w_s = smem_u32(wsm), mbar_s = smem_u32(mbar);
+    if (tid == 0) {
+        for (int tap = 0; tap < 27; ++tap) {
+            const uint64_t ad = umma_desc(a_s + (uint32_t)(tap * kSmTcRows * 32), kSmTcRows * 16, 128);
+            const uint64_t bd = umma_desc(w_s + (uint32_t)(tap * 512), 256, 128);
+            mma_f16(tmem, ad, bd, kInstrDescM128, tap > 0 ? 1u : 0u);
+        }
+        mma_commit(mbar_s);
+    }
+    // one decision for the whole CTA: the TMEM reads below are warp-collective
+    if (!mbar_wait(mbar_s, 0)) atomicExch(&s_abort, 1);
+    __syncthreads();
+    const bool ok = s_abort == 0;
+    tc_fence_after();
+    if (ok && warp < 4) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16), v);
+        const uint32_t vx = v0 + (uint32_t)(32 * warp + lane);
+        if (vx < nvox) {
+            const uint32_t sl = (G.act_tiles[vx >> 9] << 9) | (vx & 511u);
+            uint4 o0, o1;
+            __nv_bfloat162* h0 = reinterpret_cast<__nv_bfloat162*>(&o0);
+            __nv_bfloat162* h1 = reinterpret_cast<__nv_bfloat162*>(&o1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                h0[k] = __floats2bfloat162_rn(fmaxf(v[2 * k], 0.0f), fmaxf(v[2 * k + 1], 0.0f));
+                h1[k] = __floats2bfloat162_rn(fmaxf(v[8 + 2 * k], 0.0f), fmaxf(v[8 + 2 * k + 1], 0.0f));
+            }
+            uint4* dst = reinterpret_cast<uint4*>(out + (size_t)sl * 16);
+            dst[0] = o0;
+            dst[1] = o1;
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 1);
+        mbar_wait(mbar_s, 0);  // bounded: the MMAs before TMEM is freed
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+}
+
+int lp_small_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
+                            int* err, uint32_t ntiles, cudaStream_t st) {
+    static bool attr_set = false;  // per process; the attribute is per function
+    if (!attr_set) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(lp_small_mid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmTcBytes));
+        attr_set = true;
+    }
+    const int grid = (int)((ntiles * 512u + kSmTcRows - 1) / kSmTcRows);
+    lp_small_mid_tc_kernel<<<grid, kSmTcThreads, kSmTcBytes, st>>>(G, wb, dil, in, out, err);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
 int lp_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const __nv_bfloat16* in, __nv_bfloat16* out,
                       int* err, int sms, cudaStream_t st) {
     switch (dil) {

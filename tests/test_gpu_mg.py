@@ -132,3 +132,21 @@ def test_coarse_cg_comparison_mode(torch):
     typ, b = problem_arrays(P, shape)
     assert solution_residual(typ, b, P.poisson_solution(), shape) <= 1.05e-6
     P.close()
+
+
+def test_coarsest_network_tensor_cores_vs_cuda_cores(torch):
+    # the coarsest level's 16 -> 16 layers on tcgen05 (default) against the
+    # CUDA-core small-grid kernels: FP32 sums of the same BF16 products in a
+    # different order, so a few activations round to the neighbouring BF16
+    shape = (64, 64, 64)
+    zs = []
+    for cc in (0, 1):
+        P = engine(shape, lp_cuda_cores=cc)
+        P.poisson_generate(seed=3, radius=(3.0, 8.0))
+        P.lp_set_weights(np.load(WEIGHTS))
+        typ, _ = problem_arrays(P, shape)
+        r = np.where(typ == 1, np.random.default_rng(5).standard_normal(typ.size), 0.0).astype(np.float32)
+        zs.append(P.mg_apply(r))
+        assert P.info().error_flags == 0
+        P.close()
+    assert np.linalg.norm(zs[0] - zs[1]) <= 1e-3 * np.linalg.norm(zs[1])
