@@ -971,7 +971,7 @@ __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __rest
             rz += (double)rv[m] * (double)zv[m];
             zq += (double)zv[m] * (double)qv[m];
         }
-        *reinterpret_cast<float4*>(z + s) = z4;
+        if (jacobi) *reinterpret_cast<float4*>(z + s) = z4;  // else z is unchanged
     }
     double vals[2] = {rz, zq}, out[2];
     if (last_block_reduce<2>(vals, partials, &st->ticket, sh, out) && threadIdx.x == 0) {
