@@ -1,9 +1,11 @@
 // mg.cu -- V-cycle kernels of the multilevel learned preconditioner (mg.cuh).
 //
 // Every level is tile-blocked like the solver's grid (slot = tile * 512 +
-// (i & 7) + 8 (j & 7) + 64 (k & 7)).  The smoothing kernels walk a tile list
-// with one CTA of 512 threads per tile and one thread per cell; neighbours
-// come from global memory (the coarse levels are small enough to stay in L2).
+// (i & 7) + 8 (j & 7) + 64 (k & 7)).  Per level the hierarchy kernels
+// (coarse types, cell codes) walk every slot; the two smoothing kernels walk
+// the level's tile list and stage each tile with a 2-cell halo in shared
+// memory (see "smoothing" below); the coarsest level also has a one-CTA
+// Jacobi-PCG (training targets, and the comparison without the network).
 // Non-fluid cells carry 0 in every vector, so the 7-point operator needs only
 // the fluid bit and the non-solid neighbour count of the PCG cell code.
 #include "common.cuh"

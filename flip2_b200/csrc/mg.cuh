@@ -5,8 +5,9 @@
 //
 // Levels.  Level 0 is the solver's grid (its occupied tiles, PCG cell codes).
 // Level l+1 has ceil(n_l / 2) cells per axis, padded to whole 8^3 tiles;
-// cells past that extent are solid, and every tile of a coarse level is
-// processed.  A coarse cell is air if any of its 8 children is air (the
+// cells past that extent are solid.  The smoothing walks the tiles with
+// fluid cells of each level, and every tile of the coarsest (at most 8).
+// A coarse cell is air if any of its 8 children is air (the
 // Dirichlet condition of the free surface reaches the coarse problem), else
 // fluid if any child is fluid, else solid; its operator is the 7-point
 // Laplacian of those types on the coarse grid.
@@ -19,7 +20,8 @@
 //   t += P e  (P: the parent's value, fluid cells only), then two sweeps
 //        t += omega D^-1 (r - A t)                          (post-smoothing)
 // On the coarsest level z = N(r) + D^-1 r (N: the network) followed by two
-// sweeps, or without the network z = omega D^-1 r and the same sweeps.
+// sweeps, or without the network z = omega D^-1 r and the same sweeps (or,
+// for comparison, z = a Jacobi-PCG solution in one CTA and the sweeps).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
