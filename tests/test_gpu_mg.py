@@ -150,3 +150,31 @@ def test_coarsest_network_tensor_cores_vs_cuda_cores(torch):
         assert P.info().error_flags == 0
         P.close()
     assert np.linalg.norm(zs[0] - zs[1]) <= 1e-3 * np.linalg.norm(zs[1])
+
+
+def test_trained_network_gain(torch):
+    # what the trained network gains: the same V-cycle and FCG on the same
+    # problems, with the committed weights, without the network, and with an
+    # untrained (freshly initialised) network.  Iterations count the
+    # Jacobi-PCG restart of a solve that falls back (the untrained network's
+    # output is noise: FCG stalls and restarts)
+    shape = (128, 128, 128)
+    its, fell = {}, {}
+    for name, mode, w in (("trained", 0, "committed"), ("no_network", 1, "committed"), ("untrained", 0, "init")):
+        P = engine(shape, mg_coarse=mode)
+        if w == "init":
+            P.lp_init(seed=0)
+        else:
+            P.lp_set_weights(np.load(WEIGHTS))
+        its[name], fell[name] = [], 0
+        for s in range(900_000, 900_003):
+            P.poisson_generate(seed=s)
+            info = P.poisson_solve(method=2, tol=1e-6, max_iter=100)
+            assert info.converged == 1 and info.rel_residual <= 1e-6
+            its[name].append(info.iters + info.plain_iters)
+            fell[name] += info.fell_back
+        P.close()
+    print(its, fell)
+    assert fell["trained"] == 0 and fell["no_network"] == 0
+    assert sum(its["trained"]) < 0.6 * sum(its["no_network"])
+    assert sum(its["trained"]) < 0.6 * sum(its["untrained"])
