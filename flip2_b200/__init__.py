@@ -35,7 +35,8 @@ STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of device memory"
 (BUF_PX, BUF_PY, BUF_PZ, BUF_VX, BUF_VY, BUF_VZ, BUF_KEYS, BUF_PERM, BUF_FLAGS, BUF_STARTS, BUF_YTABLE,
  BUF_NODE_VOXELS, BUF_VOXEL_IDS, BUF_SOLIDS, BUF_UX, BUF_UY, BUF_UZ, BUF_DIVU, BUF_P, BUF_RES,
  BUF_GRID_U, BUF_GRID_V, BUF_GRID_W, BUF_CELL_TYPE, BUF_PRESSURE, BUF_TILE_LIST,
- BUF_GRID_U_P2G, BUF_GRID_V_P2G, BUF_GRID_W_P2G) = range(29)
+ BUF_GRID_U_P2G, BUF_GRID_V_P2G, BUF_GRID_W_P2G,
+ BUF_MG_COARSE_TYPE, BUF_MG_COARSE_R, BUF_MG_COARSE_E) = range(32)
 
 
 class FlipError(RuntimeError):

@@ -1498,6 +1498,17 @@ extern "C" int flip_get_buffer(flip_engine* e, int which, void** dev_ptr, uint64
     case FLIP_BUF_GRID_U_P2G: p = e->o[0]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_GRID_V_P2G: p = e->o[1]; c = ref ? 0 : e->nslots; break;
     case FLIP_BUF_GRID_W_P2G: p = e->o[2]; c = ref ? 0 : e->nslots; break;
+    case FLIP_BUF_MG_COARSE_TYPE:
+    case FLIP_BUF_MG_COARSE_R:
+    case FLIP_BUF_MG_COARSE_E: {
+        if (ref || !e->mg_arena) break;
+        const MgLevel& cl = e->mg.L[e->mg.levels - 1];
+        c = (uint64_t)cl.ntiles * 512u;
+        if (which == FLIP_BUF_MG_COARSE_TYPE) { p = cl.type; es = 1; }
+        else if (which == FLIP_BUF_MG_COARSE_R) p = cl.r;
+        else p = e->mg_ev;
+        break;
+    }
     default: return e->fail(FLIP_ERR_ARG, "unknown buffer id");
     }
     *dev_ptr = p;

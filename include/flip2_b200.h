@@ -260,6 +260,11 @@ typedef enum {
     FLIP_BUF_TILE_LIST,
     /* NATIVE grid velocity right after P2G (the FLIP "old" grid) */
     FLIP_BUF_GRID_U_P2G, FLIP_BUF_GRID_V_P2G, FLIP_BUF_GRID_W_P2G,
+    /* NATIVE multilevel preconditioner, its coarsest level (tile-blocked on
+     * that level's grid; empty until pressure_method 2 or flip_mg_* ran):
+     * cell types, the last right-hand side and the last training error
+     * sample of flip_mg_train_step */
+    FLIP_BUF_MG_COARSE_TYPE, FLIP_BUF_MG_COARSE_R, FLIP_BUF_MG_COARSE_E,
     FLIP_BUF_COUNT
 } flip_buffer;
 /* elem_size: 1, 4 or 8 bytes; count: number of valid elements.

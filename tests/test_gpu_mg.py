@@ -178,3 +178,37 @@ def test_trained_network_gain(torch):
     assert fell["trained"] == 0 and fell["no_network"] == 0
     assert sum(its["trained"]) < 0.6 * sum(its["no_network"])
     assert sum(its["trained"]) < 0.6 * sum(its["untrained"])
+
+
+@pytest.mark.parametrize("sample", [-1, 5])
+def test_coarse_training_loss_and_gradient_vs_oracle(torch, sample):
+    # the training step of the multilevel form on its coarsest level: the
+    # small-grid forward (tcgen05 16 -> 16 layers) and the backward kernels
+    # against the oracle's FP64 loss and gradient on the same coarse problem
+    # (types, right-hand side and error read back from the engine)
+    shape = (64, 64, 64)
+    P = engine(shape)
+    P.poisson_generate(seed=21, radius=(3.0, 8.0))
+    w = np.load(WEIGHTS)
+    P.lp_set_weights(w)
+    loss = P.mg_train_step(sample, 0.0)
+    g = P.lp_grad()
+    cshape = O.mg_levels(shape)[-1]
+    typ = tiled_to_linear(P.read(F.BUF_MG_COARSE_TYPE, np.uint8), *cshape)
+    r = tiled_to_linear(P.read(F.BUF_MG_COARSE_R, np.float32), *cshape)
+    ev = tiled_to_linear(P.read(F.BUF_MG_COARSE_E, np.float32), *cshape)
+    assert P.info().error_flags == 0
+    P.close()
+    assert np.any(typ == 1) and np.any(r[typ == 1] != 0.0)
+    lo, zo, go = O.lp_loss_grad(typ.reshape(cshape[::-1]), r, ev, w, cshape, round_bf16=True)
+    # the loss to 2e-3 as in the network's own parity test.  The gradient: FP32
+    # sums against FP64, and activations whose BF16 rounding flips between the
+    # two; on the 4,096 voxels of the coarsest level fewer of those flips
+    # average out than on the solver-grid tests (5e-3 there), so 1e-2 in L2
+    # over all weights and 2e-2 per layer
+    assert abs(loss - lo) <= 2e-3 * max(1.0, abs(lo))
+    assert np.linalg.norm(g - go) <= 1e-2 * np.linalg.norm(go)
+    offs = [0, 27 * 3 * 16, 27 * 3 * 16 + 27 * 256, 27 * 3 * 16 + 2 * 27 * 256, g.size]
+    for l in range(4):
+        a, b = offs[l], offs[l + 1]
+        assert np.linalg.norm(g[a:b] - go[a:b]) <= 2e-2 * np.linalg.norm(go[a:b])
