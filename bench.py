@@ -13,6 +13,7 @@ Multi-GPU: the step does not shard (one box per GPU), so N ranks run N
 independent replicas of the workload; the time is the maximum over ranks.
 """
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -40,7 +41,7 @@ PCG_BYTES_PER_VOXEL = 49.0
 MG_BYTES_PER_VOXEL = 83
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,timestamp")
 
 
 def parse_args():
@@ -166,17 +167,29 @@ def cpu_baseline(cells, budget_s=20.0):
 
 # ------------------------------------------------------------ clocks
 class Clocks:
+    """nvidia-smi sampling every 50 ms, started before the warm-up (the tool
+    takes a moment to start) and filtered to the timed window's host times;
+    a window shorter than the sampling interval reports the samples nearest
+    to it and says so."""
+
     def __init__(self, gpu_index):
         self.p = None
+        self.t0 = self.t1 = None
         self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
                                  ".bench_clocks_%d.csv" % gpu_index)
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + CLOCK_QUERY,
-                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.p = None
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if self.p is None:
@@ -198,11 +211,28 @@ class Clocks:
             pass
         if not rows:
             return None
+        window = "timed region"
+        if self.t0 is not None and self.t1 is not None:
+            def ts(r):
+                try:
+                    return datetime.datetime.strptime(r[9], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except (IndexError, ValueError):
+                    return None
+            stamped = [(ts(r), r) for r in rows if ts(r) is not None]
+            inside = [r for t, r in stamped if self.t0 <= t <= self.t1]
+            if inside:
+                rows = inside
+            elif stamped:
+                mid = 0.5 * (self.t0 + self.t1)
+                stamped.sort(key=lambda tr: abs(tr[0] - mid))
+                rows = [r for _, r in stamped[:2]]
+                window = "nearest samples (timed region shorter than the 50 ms sampling interval)"
         sm = [float(r[1]) for r in rows]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(float(r[2]) for r in rows),
-                "reasons": reasons, "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows),
+                "window": window}
 
 
 # ------------------------------------------------------------ reference arm
@@ -310,18 +340,19 @@ def main():
 
     barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    phys = int(vis[local]) if local < len(vis) and vis[local].strip().isdigit() else local
+    clocks = Clocks(phys)  # sampling from here; kept for the timed window only
     for _ in range(max(3, args.warmup)):
         P.step(DT)
     P.sync()
     l0 = P.info().launches
 
     # ---- device-resident timed region
-    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
-    phys = int(vis[local]) if local < len(vis) and vis[local].strip().isdigit() else local
-    clocks = Clocks(phys)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize(dev)
+    clocks.begin()
     ev0.record(stream)
     fell_back = 0
     for _ in range(args.steps):
@@ -330,6 +361,7 @@ def main():
             fell_back += P.solve_info().fell_back
     ev1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.end()
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
