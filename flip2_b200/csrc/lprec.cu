@@ -234,6 +234,7 @@ __device__ __forceinline__ void unpack8(const uint4& q, float* x) {
 __global__ void __launch_bounds__(kSmallThreads) lp_small_in_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
                                                                     const float* __restrict__ d_inv_s,
                                                                     __nv_bfloat16* __restrict__ out) {
+    pdl_wait();
     if (G.halt && *G.halt) return;
     __shared__ float W[27 * 3 * 16];
     __shared__ float X[kSmallVox * 27 * 3];
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(kSmallThreads) lp_small_in_kernel(LpGrid G, co
 __global__ void __launch_bounds__(kSmallThreads) lp_small_mid_kernel(LpGrid G, const __nv_bfloat16* __restrict__ wb, int dil,
                                                                      const __nv_bfloat16* __restrict__ in,
                                                                      __nv_bfloat16* __restrict__ out) {
+    pdl_wait();
     if (G.halt && *G.halt) return;
     __shared__ float W[27 * 16 * 16];  // [tap][ci][co]
     __shared__ uint4 X[kSmallVox * 27 * 2];
@@ -299,6 +301,7 @@ __global__ void __launch_bounds__(kSmallThreads) lp_small_out_kernel(LpGrid G, c
                                                                      const float* __restrict__ d_inv_s,
                                                                      const float* __restrict__ f0, int raw,
                                                                      float* __restrict__ z) {
+    pdl_wait();
     if (G.halt && *G.halt) return;
     __shared__ float W[27 * 16];
     __shared__ uint4 X[kSmallVox * 27 * 2];
@@ -326,16 +329,24 @@ __global__ void __launch_bounds__(kSmallThreads) lp_small_out_kernel(LpGrid G, c
 static int lp_small_pass(const LpNet& net, const LpGrid& G, const float* d_inv_s, __nv_bfloat16* const* acts,
                          const float* f0, int raw, float* z, uint32_t ntiles, cudaStream_t st) {
     const int g = (int)(ntiles * 512u / kSmallVox);
-    lp_small_in_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[0], net.dil[0], d_inv_s, acts[0]);
+    // dependent launches: each kernel's launch overlaps its predecessor's tail
+    const __nv_bfloat16* a0 = acts[0];
+    const __nv_bfloat16* a1 = acts[1];
+    const __nv_bfloat16* a2 = acts[2];
+    FLIP_CUDA_TRY(pdl_launch(lp_small_in_kernel, g, kSmallThreads, 0, st, G, (const __nv_bfloat16*)(net.wb + kLpWOff[0]),
+                             net.dil[0], d_inv_s, acts[0]));
     if (net.tensor_cores) {
-        int rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1], net.err, ntiles, st);
-        if (rc == FLIP_OK) rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2], net.err, ntiles, st);
+        int rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[1], net.dil[1], a0, acts[1], net.err, ntiles, st);
+        if (rc == FLIP_OK) rc = lp_small_mid_forward_tc(G, net.wb + kLpWOff[2], net.dil[2], a1, acts[2], net.err, ntiles, st);
         if (rc != FLIP_OK) return rc;
     } else {
-        lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], acts[0], acts[1]);
-        lp_small_mid_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], acts[1], acts[2]);
+        FLIP_CUDA_TRY(pdl_launch(lp_small_mid_kernel, g, kSmallThreads, 0, st, G,
+                                 (const __nv_bfloat16*)(net.wb + kLpWOff[1]), net.dil[1], a0, acts[1]));
+        FLIP_CUDA_TRY(pdl_launch(lp_small_mid_kernel, g, kSmallThreads, 0, st, G,
+                                 (const __nv_bfloat16*)(net.wb + kLpWOff[2]), net.dil[2], a1, acts[2]));
     }
-    lp_small_out_kernel<<<g, kSmallThreads, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], acts[2], d_inv_s, f0, raw, z);
+    FLIP_CUDA_TRY(pdl_launch(lp_small_out_kernel, g, kSmallThreads, 0, st, G, (const __nv_bfloat16*)(net.wb + kLpWOff[3]),
+                             net.dil[3], a2, d_inv_s, f0, raw, z));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

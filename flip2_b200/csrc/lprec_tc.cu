@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(kSmTcThreads) lp_small_mid_tc_kernel(LpGrid G,
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kSmTcA + kSmTcW);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kSmTcA + kSmTcW + 16);
     __shared__ int s_abort;
+    pdl_wait();
     if (G.halt && *G.halt) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t nvox = *G.d_nact * 512u;
@@ -407,7 +408,7 @@ int lp_small_mid_forward_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, c
         attr_set = true;
     }
     const int grid = (int)((ntiles * 512u + kSmTcRows - 1) / kSmTcRows);
-    lp_small_mid_tc_kernel<<<grid, kSmTcThreads, kSmTcBytes, st>>>(G, wb, dil, in, out, err);
+    FLIP_CUDA_TRY(pdl_launch(lp_small_mid_tc_kernel, grid, kSmTcThreads, kSmTcBytes, st, G, wb, dil, in, out, err));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -183,6 +183,7 @@ __device__ __forceinline__ float4 mg_quad_nb(const float* v, int b, int qd) {
 //   parents of a tile are all written by it, and parents of tiles off the
 //   list are never fluid)
 __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLevel C, const int* halt) {
+    pdl_wait();
     if (mg_halted(halt)) return;
     __shared__ uint32_t cb[kBoxQ];                  // four codes per quad
     __shared__ __align__(16) float rb[kBoxF];
@@ -285,6 +286,7 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
 template <int MODE>
 __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
                                                                   const int* halt) {
+    pdl_wait();
     if (mg_halted(halt)) return;
     __shared__ uint32_t cb[kBoxQ];
     __shared__ __align__(16) float rb[kBoxF];
@@ -390,6 +392,7 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
 
 // 1 / rms(r) over the fluid cells of a level (one CTA)
 __global__ void __launch_bounds__(1024) mg_scale_kernel(MgLevel L, float* inv_s, const int* halt) {
+    pdl_wait();
     if (mg_halted(halt)) return;
     __shared__ double sh[32];
     const uint32_t n = *L.d_ntiles;
@@ -532,7 +535,7 @@ int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
 
 int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
     for (int l = 0; l + 1 < H.levels; ++l)
-        mg_down_kernel<<<mg_grid(H.L[l], grid0, l), kMgThreads, 0, s>>>(H.L[l], H.L[l + 1], halt);
+        FLIP_CUDA_TRY(pdl_launch(mg_down_kernel, mg_grid(H.L[l], grid0, l), kMgThreads, 0, s, H.L[l], H.L[l + 1], halt));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -541,16 +544,18 @@ int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStre
     const int c = H.levels - 1;
     const MgLevel& L = H.L[c];
     const int g = mg_grid(L, 740, c);
-    if (zn && solved) mg_sweeps_kernel<3><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
-    else if (zn) mg_sweeps_kernel<1><<<g, kMgThreads, 0, s>>>(L, L, zn, halt);
-    else mg_sweeps_kernel<2><<<g, kMgThreads, 0, s>>>(L, L, nullptr, halt);
+    const float* z0 = zn;
+    if (zn && solved) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<3>, g, kMgThreads, 0, s, L, L, z0, halt));
+    else if (zn) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<1>, g, kMgThreads, 0, s, L, L, z0, halt));
+    else FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<2>, g, kMgThreads, 0, s, L, L, z0, halt));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
 int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
     for (int l = H.levels - 2; l >= 0; --l)
-        mg_sweeps_kernel<0><<<mg_grid(H.L[l], grid0, l), kMgThreads, 0, s>>>(H.L[l], H.L[l + 1], nullptr, halt);
+        FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<0>, mg_grid(H.L[l], grid0, l), kMgThreads, 0, s, H.L[l], H.L[l + 1],
+                                 (const float*)nullptr, halt));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -563,7 +568,7 @@ int mg_cg(const MgLevel& L, const float* b, float* x, float* r, float* p, float*
 }
 
 int mg_input_scale(const MgHierarchy& H, const int* halt, cudaStream_t s) {
-    mg_scale_kernel<<<1, 1024, 0, s>>>(H.L[H.levels - 1], H.inv_s, halt);
+    FLIP_CUDA_TRY(pdl_launch(mg_scale_kernel, 1, 1024, 0, s, H.L[H.levels - 1], H.inv_s, halt));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
