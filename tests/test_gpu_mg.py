@@ -13,7 +13,7 @@ import flip2_b200 as F
 from flip2_b200 import scenes
 from oracle import oracle as O
 from tests.test_gpu_lprec import engine, problem_arrays, solution_residual
-from tests.util import rel_err, tiled_to_linear
+from tests.util import rel_err, remove_pocket_constants, sealed_pockets, tiled_to_linear
 
 pytestmark = pytest.mark.gpu
 WEIGHTS = os.path.join(os.path.dirname(F.__file__), "data", "mg_weights.npy")
@@ -212,3 +212,23 @@ def test_coarse_training_loss_and_gradient_vs_oracle(torch, sample):
     for l in range(4):
         a, b = offs[l], offs[l + 1]
         assert np.linalg.norm(g[a:b] - go[a:b]) <= 2e-2 * np.linalg.norm(go[a:b])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fcg_on_padded_levels(torch, mode):
+    # a grid whose coarse levels need padding (48 x 40 x 56 -> 24 x 20 x 28
+    # padded to 24 x 24 x 32 -> 12 x 10 x 14 padded to 16^3): FCG with the
+    # V-cycle meets tol and its solution is the oracle's
+    shape = (48, 40, 56)
+    P = mg_engine(shape, mode, seed=13)
+    info = P.poisson_solve(method=2, tol=1e-6, max_iter=400)
+    assert info.converged == 1 and info.fell_back == 0 and info.rel_residual <= 1e-6
+    typ, b = problem_arrays(P, shape)
+    x = P.poisson_solution()
+    assert solution_residual(typ, b, x, shape) <= 1.05e-6
+    xo, ito, rro = O.mg_fcg(typ, b.astype(np.float64), np.load(WEIGHTS), shape, mode=mode, max_iter=400)
+    assert rro <= 1e-6
+    pocket, _ = sealed_pockets(typ, shape)
+    assert rel_err(remove_pocket_constants(x, xo, pocket), xo) < 2e-3
+    assert abs(info.iters - ito) <= max(4, ito // 8) + 16
+    P.close()
