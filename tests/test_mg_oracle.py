@@ -127,3 +127,21 @@ def test_fcg_beats_jacobi_pcg():
     _, itp, rrp = O.nat_pcg(t.ravel(), b.ravel(), O.nat_params(*shape, 1.0, tol=1e-6, max_iter=20000))
     assert rrp <= 1e-6
     assert it * 4 < itp
+
+
+def test_fcg_on_padded_levels():
+    # 48 x 40 x 56: the coarse levels are padded with solid cells to whole
+    # 8^3 tiles (24 x 24 x 32, then 16^3); the V-cycle still preconditions FCG
+    # to the tolerance, and its operator is still symmetric
+    shape = (48, 40, 56)
+    assert O.mg_levels(shape)[1:] == [(24, 24, 32), (16, 16, 16)]
+    t, b = problem(shape, 6)
+    w0 = np.zeros(O.lib().orc_lp_num_weights(), np.float32)
+    x, it, rr = O.mg_fcg(t.ravel(), b.ravel(), w0, shape, mode=1, max_iter=400)
+    assert rr <= 1e-6 and it < 200
+    rng = np.random.default_rng(7)
+    u = np.where(t == FLUID, rng.standard_normal(t.shape), 0.0).astype(np.float32).ravel()
+    v = np.where(t == FLUID, rng.standard_normal(t.shape), 0.0).astype(np.float32).ravel()
+    a = float(v @ O.mg_apply(t.ravel(), u, w0, shape, mode=1))
+    c = float(u @ O.mg_apply(t.ravel(), v, w0, shape, mode=1))
+    assert abs(a - c) <= 1e-10 * max(abs(a), 1.0)
