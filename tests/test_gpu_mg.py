@@ -232,3 +232,33 @@ def test_fcg_on_padded_levels(torch, mode):
     assert rel_err(remove_pocket_constants(x, xo, pocket), xo) < 2e-3
     assert abs(info.iters - ito) <= max(4, ito // 8) + 16
     P.close()
+
+
+def test_solve_frame_with_method_2(torch):
+    # one frame of Courant sub-steps (solveFrame) with the learned multilevel
+    # solve on a 32^3 grid (V-cycle 32^3 -> 16^3, the network on 16^3) against
+    # the same frame with Jacobi-PCG: every solve meets 1e-6, so the sub-step
+    # sequence and the particles agree to the solver tolerance (positions
+    # compared sorted per axis: the particle order follows the cell keys)
+    nc = 32
+    pos, _ = scenes.dam_break(nc, seed=0)
+    vel = scenes.random_velocities(pos.shape[0], seed=3, scale=2.0)
+    out = {}
+    for method in (0, 2):
+        params = F.default_params(F.MODE_NATIVE, pressure_method=method)
+        P = F.Particles(pos.shape[0], mode=F.MODE_NATIVE, params=params)
+        P.setDomain(0.0, 0.0, 0.0, nc // 4, nc // 4, nc // 4, 4.0 / nc)
+        if method:
+            P.lp_set_weights(np.load(WEIGHTS))
+        P.upload(pos, vel)
+        P.solveFrame(24.0)
+        info = P.info()
+        assert info.converged == 1 and info.error_flags == 0
+        si = P.solve_info()
+        assert si.fell_back == 0 and si.rel_residual <= 1e-6
+        out[method] = (P.download()[0], info.elapsed_time)
+        P.close()
+    (p0, t0), (p2, t2) = out[0], out[2]
+    assert abs(t0 - t2) < 1e-12
+    for k in range(3):
+        assert np.max(np.abs(np.sort(p2[:, k]) - np.sort(p0[:, k]))) < 1e-3 * (4.0 / nc)
