@@ -947,15 +947,19 @@ static int mg_net_forward(flip_engine* e, const LpGrid& G) {
     return lp_small_forward(e->lp, G, e->mg.L[e->mg.levels - 1].ntiles, e->mg.inv_s, e->mg.f0, e->mg_zn, e->stream);
 }
 // kernels of one V-cycle (for the launch count)
-static uint32_t mg_cycle_launches(flip_engine* e, bool network) {
+// kernels of one V-cycle; dot: with FCG's dot products (their own kernel
+// only when there is no level above the coarsest to fuse them into)
+static uint32_t mg_cycle_launches(flip_engine* e, bool network, bool dot = false) {
     const uint32_t coarse = network ? 5u : (e->P.mg_coarse == 2 ? 1u : 0u);
-    return 2u * (uint32_t)(e->mg.levels - 1) + 1u + coarse;
+    return 2u * (uint32_t)(e->mg.levels - 1) + 1u + coarse + (dot && e->mg.levels < 2 ? 1u : 0u);
 }
 // coarse CG of mg_coarse = 2: relative tolerance and iteration cap
 constexpr double kMgCoarseCgTol = 1e-3;
 constexpr int kMgCoarseCgIters = 64;
-// one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is done)
-static int mg_cycle(flip_engine* e, bool network, const int* halt) {
+// one V-cycle: z = M(r) from pcg.r into pcg.z (halt: stop when the solve is
+// done); dot_init >= 0: then FCG's dot products (init: beta = 0), fused into
+// level 0's post-smoothing
+static int mg_cycle(flip_engine* e, bool network, const int* halt, int dot_init = -1) {
     const int grid0 = nat_grid(e, 5);
     E_TRY(mg_down(e->mg, halt, grid0, e->stream));
     const float* zn = nullptr;
@@ -974,7 +978,10 @@ static int mg_cycle(flip_engine* e, bool network, const int* halt) {
         solved = true;
     }
     E_TRY(mg_coarsest(e->mg, zn, halt, e->stream, solved));
-    E_TRY(mg_up(e->mg, halt, grid0, e->stream));
+    const bool fuse = dot_init >= 0 && e->mg.levels >= 2;
+    const MgDot dot{e->pcg.q, e->pcg.st, e->pcg.partials, dot_init};
+    E_TRY(mg_up(e->mg, halt, grid0, e->stream, fuse ? &dot : nullptr));
+    if (dot_init >= 0 && !fuse) E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, dot_init, e->stream, 0));
     return FLIP_OK;
 }
 // per problem: coarse types and codes (after pcg_init set level 0's codes)
@@ -1036,8 +1043,7 @@ static int nat_mgpcg_graph(flip_engine* e, int iters, int max_iter, bool network
             rc = nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
             if (rc == FLIP_OK && k == iters - 1)
                 rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-            if (rc == FLIP_OK) rc = mg_cycle(e, network, halt);
-            if (rc == FLIP_OK) rc = nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 0, e->stream, 0);
+            if (rc == FLIP_OK) rc = mg_cycle(e, network, halt, 0);
         }
         return rc;
     }, limit, &e->mg_graph));
@@ -1079,12 +1085,11 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
                                   warm ? e->cell_prev : nullptr));
         E_TRY(mg_setup_problem(e, network));
-        E_TRY(mg_cycle(e, network, &e->pcg.st->halt));
-        E_TRY(nat_launch_fpcg_dot(e->node_keys, e->d_counts, e->pcg, 1, e->stream, 0));
-        e->launches += (warm ? 3u : 2u) + mg_cycle_launches(e, network);
+        E_TRY(mg_cycle(e, network, &e->pcg.st->halt, 1));
+        e->launches += (warm ? 2u : 1u) + mg_cycle_launches(e, network, true);
         E_TRY(e->mark(9));
         E_TRY(nat_mgpcg_graph(e, chunk, max_learned, network));
-        E_TRY(run_loop(e, e->mg_graph, (3u + mg_cycle_launches(e, network)) * (uint32_t)chunk + 1u));
+        E_TRY(run_loop(e, e->mg_graph, (2u + mg_cycle_launches(e, network, true)) * (uint32_t)chunk + 1u));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;

@@ -282,10 +282,11 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
 // of the coarse correction; post-smoothing); MODE 1: u = zn + D^-1 r (the
 // coarsest level with the network output zn); MODE 2: u = w D^-1 r (the
 // coarsest level without the network); MODE 3: u = zn (the coarsest level
-// after a CG solve into zn).
-template <int MODE>
+// after a CG solve into zn).  DOT (MODE 0 on level 0): FCG's dot products
+// of the z it writes (MgDot), reduced by the last CTA.
+template <int MODE, bool DOT = false>
 __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgLevel C, const float* __restrict__ zn,
-                                                                  const int* halt) {
+                                                                  const int* halt, MgDot dot) {
     pdl_wait();
     if (mg_halted(halt)) return;
     __shared__ uint32_t cb[kBoxQ];
@@ -293,8 +294,10 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
     __shared__ __align__(16) float ub[kBoxF];
     __shared__ __align__(16) float tb[kT1F];
     __shared__ float inv[8];
+    __shared__ double acc[DOT ? 2 * 128 : 1];  // r.z, z.q of each storing thread
     mg_inv_table(inv);
     const int tid = threadIdx.x;
+    if (DOT && tid < 128) acc[2 * tid] = acc[2 * tid + 1] = 0.0;
     int map[kQPer];
 #pragma unroll
     for (int m = 0; m < kQPer; ++m) map[m] = mg_quad_map(tid + m * kMgThreads);
@@ -382,11 +385,60 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
             const int qd = 1 + half;
             const int b = 4 * qd + kBX * ((ly + 2) + kBY * (lz + 2));
             const int t = 4 * qd + kBX * ((ly + 1) + 10 * (lz + 1));
-            const float4 z = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(tb + t),
-                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * 10>(tb, t, qd), inv);
-            *reinterpret_cast<float4*>(L.z + ((key << 9) | (uint32_t)(4 * half + 8 * ly + 64 * lz))) = z;
+            const uint32_t zs = (key << 9) | (uint32_t)(4 * half + 8 * ly + 64 * lz);
+            float4 q4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (DOT) q4 = *reinterpret_cast<const float4*>(dot.q + zs);
+            const uint32_t c4 = cb[b >> 2];
+            const float4 r4 = *reinterpret_cast<const float4*>(rb + b);
+            const float4 z = mg_quad_sweep(c4, *reinterpret_cast<const float4*>(tb + t), r4,
+                                           mg_quad_nb<kBX, kBX * 10>(tb, t, qd), inv);
+            *reinterpret_cast<float4*>(L.z + zs) = z;
+            if (DOT) {
+                double rz = 0.0, zq = 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    if (!((c4 >> (8 * m)) & kCellFluid)) continue;
+                    rz += (double)f4(r4, m) * (double)f4(z, m);
+                    zq += (double)f4(z, m) * (double)f4(q4, m);
+                }
+                acc[2 * tid] += rz;
+                acc[2 * tid + 1] += zq;
+            }
         }
         __syncthreads();
+    }
+    if (DOT) {
+        // per-CTA sums, then the last CTA to arrive sums the partials in CTA
+        // order (deterministic for a given grid) and sets the FCG state
+        __shared__ double sh[32];
+        __shared__ bool s_last;
+        double v[2] = {tid < 128 ? acc[2 * tid] : 0.0, tid < 128 ? acc[2 * tid + 1] : 0.0}, out[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const double s = block_sum_f64<kMgThreads>(v[q], sh);
+            if (tid == 0) dot.partials[q * gridDim.x + blockIdx.x] = s;
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = atomicAdd(&dot.st->ticket, 1u) == gridDim.x - 1;
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            double a = 0.0;
+            for (int b = tid; b < (int)gridDim.x; b += kMgThreads) a += ((volatile double*)dot.partials)[q * gridDim.x + b];
+            out[q] = block_sum_f64<kMgThreads>(a, sh);
+        }
+        if (tid == 0) {
+            PcgState* st = dot.st;
+            st->ticket = 0u;
+            st->beta = dot.init ? 0.0 : (st->pq > 0.0 ? -out[1] / st->pq : 0.0);
+            st->rz = out[0];
+            st->rz_prev = out[0];
+            st->zq = out[1];
+            if (out[0] == 0.0 || !isfinite(out[0]) || !isfinite(out[1])) { st->done = 3; st->halt = 1; }
+        }
     }
 }
 
@@ -545,17 +597,26 @@ int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStre
     const MgLevel& L = H.L[c];
     const int g = mg_grid(L, 740, c);
     const float* z0 = zn;
-    if (zn && solved) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<3>, g, kMgThreads, 0, s, L, L, z0, halt));
-    else if (zn) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<1>, g, kMgThreads, 0, s, L, L, z0, halt));
-    else FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<2>, g, kMgThreads, 0, s, L, L, z0, halt));
+    const MgDot nd{};
+    if (zn && solved) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<3>, g, kMgThreads, 0, s, L, L, z0, halt, nd));
+    else if (zn) FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<1>, g, kMgThreads, 0, s, L, L, z0, halt, nd));
+    else FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<2>, g, kMgThreads, 0, s, L, L, z0, halt, nd));
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 
-int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
-    for (int l = H.levels - 2; l >= 0; --l)
-        FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<0>, mg_grid(H.L[l], grid0, l), kMgThreads, 0, s, H.L[l], H.L[l + 1],
-                                 (const float*)nullptr, halt));
+int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s, const MgDot* dot) {
+    if (dot && (H.levels < 2 || 2 * grid0 > 4 * kPcgBlocks)) return FLIP_ERR_ARG;  // partials: 4 x kPcgBlocks
+    const MgDot nd{};
+    for (int l = H.levels - 2; l >= 0; --l) {
+        const int g = mg_grid(H.L[l], grid0, l);
+        if (l == 0 && dot)
+            FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<0, true>, g, kMgThreads, 0, s, H.L[l], H.L[l + 1],
+                                     (const float*)nullptr, halt, *dot));
+        else
+            FLIP_CUDA_TRY(pdl_launch(mg_sweeps_kernel<0>, g, kMgThreads, 0, s, H.L[l], H.L[l + 1], (const float*)nullptr,
+                                     halt, nd));
+    }
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

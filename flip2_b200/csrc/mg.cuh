@@ -69,9 +69,19 @@ int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
 // network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps (one kernel);
 // solved: zn is already a coarse solution (z = zn, then the sweeps)
 int mg_coarsest(const MgHierarchy& H, const float* zn, const int* halt, cudaStream_t s, bool solved = false);
+// FCG's dot products taken by level 0's post-smoothing as it writes z:
+// r.z and z.q over the fluid cells, then beta = -z.q / p.q (0 when init) and
+// the state's rz, rz_prev, zq -- what fpcg_dot_kernel does without the
+// Jacobi term.  partials: 2 x the level-0 grid doubles.
+struct MgDot {
+    const float* q;
+    PcgState* st;
+    double* partials;
+    int init;
+};
 // prolongation and post-smoothing back up to level 0, one kernel per level
-// (the output in L[0].z)
-int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
+// (the output in L[0].z); dot: fuse FCG's dot products into the last kernel
+int mg_up(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s, const MgDot* dot = nullptr);
 // x = A^-1 b on level L by Jacobi-PCG in one CTA (|r| <= tol |b| or
 // max_iter iterations; *iters = iterations run); r, p, q: scratch of the
 // level's size
