@@ -37,8 +37,9 @@ WORKLOAD = ("dam-break 256^3 voxels (cell 1/256), block 0.5x0.5x1, 8 jittered pa
 PCG_BYTES_PER_VOXEL = 49.0
 # one learned multilevel FCG iteration on the fine level: direction+matvec and
 # update 49 B, V-cycle down (code, r in; t, coarse r out) 9.5 B and up (code,
-# r, t in; z out) 12.5 B, FCG dot (r, z, q in) 12 B; coarse levels not counted
-MG_BYTES_PER_VOXEL = 83
+# r, t in; z out) 12.5 B, plus q in 4 B for the FCG dot products the up
+# kernel takes as it writes z; coarse levels not counted
+MG_BYTES_PER_VOXEL = 75
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,timestamp")
@@ -422,7 +423,7 @@ def main():
         traffic = None  # the ncu traffic figure covers the Jacobi-PCG iteration only
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic,
-                "kernel": ("learned multilevel FCG iteration (direction+matvec, update, V-cycle, FCG dot)" if c5 else
+                "kernel": ("learned multilevel FCG iteration (direction+matvec, update, V-cycle with the FCG dot fused)" if c5 else
                            "pcg iteration (matvec+pAp, x/r update with r.r and r.z, direction)"),
                 "algorithmic_bytes": "%d B per active voxel per iteration x %d voxels" % (per_voxel, voxels),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
