@@ -860,7 +860,7 @@ static int mg_ready(flip_engine* e, bool network) {
             total += 2 * al(n) + al(L[l].ntiles) + al(4 * (size_t)L[l].ntiles) + 3 * al(4 * n) + 256;
         }
         const size_t nc = (size_t)L[levels - 1].ntiles * 512u;
-        total += 8 * al(4 * nc) + 1024;
+        total += 8 * al(4 * nc) + 1024 + al(sizeof(double) * kMgScalePartials) + 256;
         E_CUDA(cudaMalloc((void**)&e->mg_arena, total));
         E_CUDA(cudaMemsetAsync(e->mg_arena, 0, total, e->stream));
         char* q = e->mg_arena;
@@ -894,6 +894,8 @@ static int mg_ready(flip_engine* e, bool network) {
         for (auto& p : e->mg_s) p = (float*)take(4 * nc);
         H.f0 = (float*)take(4 * nc);
         H.inv_s = (float*)take(256);
+        H.scale_partials = (double*)take(sizeof(double) * kMgScalePartials);
+        H.scale_ticket = (unsigned int*)take(256);
         e->mg_iters = (int*)take(256);
         H.levels = levels;
         for (int l = 0; l < levels; ++l) H.L[l] = L[l];
@@ -950,7 +952,8 @@ static int mg_net_forward(flip_engine* e, const LpGrid& G) {
 // kernels of one V-cycle; dot: with FCG's dot products (their own kernel
 // only when there is no level above the coarsest to fuse them into)
 static uint32_t mg_cycle_launches(flip_engine* e, bool network, bool dot = false) {
-    const uint32_t coarse = network ? 5u : (e->P.mg_coarse == 2 ? 1u : 0u);
+    // the network's four kernels, and its input scale when no down kernel takes it
+    const uint32_t coarse = network ? (e->mg.levels >= 2 ? 4u : 5u) : (e->P.mg_coarse == 2 ? 1u : 0u);
     return 2u * (uint32_t)(e->mg.levels - 1) + 1u + coarse + (dot && e->mg.levels < 2 ? 1u : 0u);
 }
 // coarse CG of mg_coarse = 2: relative tolerance and iteration cap
@@ -961,12 +964,15 @@ constexpr int kMgCoarseCgIters = 64;
 // level 0's post-smoothing
 static int mg_cycle(flip_engine* e, bool network, const int* halt, int dot_init = -1) {
     const int grid0 = nat_grid(e, 5);
-    E_TRY(mg_down(e->mg, halt, grid0, e->stream));
+    // with the network and a level above the coarsest, the last down kernel
+    // also takes the network's input scale
+    const bool fused_scale = network && e->mg.levels >= 2;
+    E_TRY(mg_down(e->mg, halt, grid0, e->stream, fused_scale));
     const float* zn = nullptr;
     bool solved = false;
     if (network) {
         const LpGrid G = mg_lp_grid(e, halt);
-        E_TRY(mg_input_scale(e->mg, halt, e->stream));
+        if (!fused_scale) E_TRY(mg_input_scale(e->mg, halt, e->stream));
         E_TRY(mg_net_forward(e, G));
         zn = e->mg_zn;
     } else if (e->P.mg_coarse == 2) {

@@ -112,6 +112,36 @@ constexpr int kSw1Q = 4 * 10 * 10;              // 400 quads of the first sweep
 constexpr int kT1F = kBX * 10 * 10;             // its output box, 1600 cells
 constexpr int kQPer = (kBoxQ + kMgThreads - 1) / kMgThreads;  // 3
 
+// Two FP64 sums over the grid of a level kernel: per-CTA sums into
+// partials[q * gridDim.x + CTA], then the last CTA to arrive adds the
+// partials in CTA order (deterministic for a given grid), resets the ticket
+// and returns true with the totals in thread 0's out.
+__device__ __forceinline__ bool mg_last_cta_sum2(double v0, double v1, double* partials, unsigned int* ticket,
+                                                 double (&out)[2]) {
+    __shared__ double sh[32];
+    __shared__ bool s_last;
+    const double v[2] = {v0, v1};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const double s = block_sum_f64<kMgThreads>(v[q], sh);
+        if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += kMgThreads) a += ((volatile double*)partials)[q * gridDim.x + b];
+        out[q] = block_sum_f64<kMgThreads>(a, sh);
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;
+}
+
 // box quad q -> (neighbour tile offset + 1 per axis, local slot of its first
 // cell), packed as local | (qx + 1) << 9 | (qy + 1) << 11 | (qz + 1) << 13; -1 past the box
 __device__ __forceinline__ int mg_quad_map(int q) {
@@ -182,9 +212,14 @@ __device__ __forceinline__ float4 mg_quad_nb(const float* v, int b, int qd) {
 //   C.r[parent] = 1/2 sum over the 8 children of r - A t (fluid parents; the
 //   parents of a tile are all written by it, and parents of tiles off the
 //   list are never fluid)
-__global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLevel C, const int* halt) {
+template <bool SCALE = false>
+__global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLevel C, const int* halt, MgScale sc) {
     pdl_wait();
     if (mg_halted(halt)) return;
+    // SCALE (C the coarsest level): the sum of C.r^2 and the count over the
+    // fluid parents this CTA writes, then *sc.inv_s as mg_scale_kernel sets it
+    __shared__ double acc[SCALE ? 2 * 64 : 1];
+    if (SCALE && threadIdx.x < 64) acc[2 * threadIdx.x] = acc[2 * threadIdx.x + 1] = 0.0;
     __shared__ uint32_t cb[kBoxQ];                  // four codes per quad
     __shared__ __align__(16) float rb[kBoxF];
     __shared__ __align__(16) float ub[kBoxF];       // t1 = w D^-1 r
@@ -271,9 +306,21 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
             const int s0 = pi + 4 * (2 * pj + 8 * 2 * pk);
             const float sum = (S[s0] + S[s0 + 4]) + (S[s0 + 32] + S[s0 + 36]);
             const uint32_t p = mg_slot(4 * tx + pi, 4 * ty + pj, 4 * tz + pk, C.D);
-            C.r[p] = (C.cell[p] & kCellFluid) ? 0.5f * sum : 0.0f;
+            const bool fl = (C.cell[p] & kCellFluid) != 0;
+            const float v = fl ? 0.5f * sum : 0.0f;
+            C.r[p] = v;
+            if (SCALE && fl) {
+                acc[2 * tid] += (double)v * (double)v;
+                acc[2 * tid + 1] += 1.0;
+            }
         }
         __syncthreads();
+    }
+    if (SCALE) {
+        double out[2];
+        const bool last = mg_last_cta_sum2(tid < 64 ? acc[2 * tid] : 0.0, tid < 64 ? acc[2 * tid + 1] : 0.0,
+                                           sc.partials, sc.ticket, out);
+        if (last && tid == 0) *sc.inv_s = out[0] > 0.0 ? (float)(1.0 / sqrt(out[0] / fmax(out[1], 1.0))) : 1.0f;
     }
 }
 
@@ -408,31 +455,11 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
         __syncthreads();
     }
     if (DOT) {
-        // per-CTA sums, then the last CTA to arrive sums the partials in CTA
-        // order (deterministic for a given grid) and sets the FCG state
-        __shared__ double sh[32];
-        __shared__ bool s_last;
-        double v[2] = {tid < 128 ? acc[2 * tid] : 0.0, tid < 128 ? acc[2 * tid + 1] : 0.0}, out[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const double s = block_sum_f64<kMgThreads>(v[q], sh);
-            if (tid == 0) dot.partials[q * gridDim.x + blockIdx.x] = s;
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) s_last = atomicAdd(&dot.st->ticket, 1u) == gridDim.x - 1;
-        __syncthreads();
-        if (!s_last) return;
-        __threadfence();
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            double a = 0.0;
-            for (int b = tid; b < (int)gridDim.x; b += kMgThreads) a += ((volatile double*)dot.partials)[q * gridDim.x + b];
-            out[q] = block_sum_f64<kMgThreads>(a, sh);
-        }
-        if (tid == 0) {
+        double out[2];
+        const bool last = mg_last_cta_sum2(tid < 128 ? acc[2 * tid] : 0.0, tid < 128 ? acc[2 * tid + 1] : 0.0,
+                                           dot.partials, &dot.st->ticket, out);
+        if (last && tid == 0) {
             PcgState* st = dot.st;
-            st->ticket = 0u;
             st->beta = dot.init ? 0.0 : (st->pq > 0.0 ? -out[1] / st->pq : 0.0);
             st->rz = out[0];
             st->rz_prev = out[0];
@@ -585,9 +612,19 @@ int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s) {
     return FLIP_OK;
 }
 
-int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s) {
-    for (int l = 0; l + 1 < H.levels; ++l)
-        FLIP_CUDA_TRY(pdl_launch(mg_down_kernel, mg_grid(H.L[l], grid0, l), kMgThreads, 0, s, H.L[l], H.L[l + 1], halt));
+int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s, bool scale) {
+    if (scale && H.levels < 2) return FLIP_ERR_ARG;
+    const MgScale ns{};
+    for (int l = 0; l + 1 < H.levels; ++l) {
+        const int g = mg_grid(H.L[l], grid0, l);
+        if (scale && l + 2 == H.levels) {
+            if (2 * g > kMgScalePartials) return FLIP_ERR_ARG;
+            const MgScale sc{H.scale_partials, H.scale_ticket, H.inv_s};
+            FLIP_CUDA_TRY(pdl_launch(mg_down_kernel<true>, g, kMgThreads, 0, s, H.L[l], H.L[l + 1], halt, sc));
+        } else {
+            FLIP_CUDA_TRY(pdl_launch(mg_down_kernel<false>, g, kMgThreads, 0, s, H.L[l], H.L[l + 1], halt, ns));
+        }
+    }
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -49,11 +49,22 @@ struct MgLevel {
     float* t;               // pre-smoothing iterate (read back by the post-smoothing)
 };
 
+constexpr int kMgScalePartials = 2048;  // doubles: 2 x the grid of a fused input scale
+
 struct MgHierarchy {
     int levels;
     MgLevel L[kMgMaxLevels];
     float* inv_s;   // 1 / rms of the coarsest right-hand side (the network's input scale)
     float* f0;      // f(0) on the coarsest level
+    double* scale_partials;      // kMgScalePartials doubles for the fused input scale
+    unsigned int* scale_ticket;  // its last-CTA ticket (0 between launches)
+};
+// the network's input scale taken by the last down kernel as it writes the
+// coarsest right-hand side: 1 / rms over the coarsest fluid cells into inv_s
+struct MgScale {
+    double* partials;
+    unsigned int* ticket;
+    float* inv_s;
 };
 
 // level dimensions below a fine grid of nx x ny x nz (multiples of 8) cells
@@ -63,8 +74,9 @@ int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels);
 int mg_build(const MgHierarchy& H, const int* halt, cudaStream_t s);
 // one V-cycle up to the coarsest level's input: smoothing and restriction
 // on levels 0 .. levels-2, one kernel per level (the coarsest right-hand
-// side ends in L[levels-1].r)
-int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s);
+// side ends in L[levels-1].r); scale: the last kernel also sets *H.inv_s as
+// mg_input_scale does (at least two levels)
+int mg_down(const MgHierarchy& H, const int* halt, int grid0, cudaStream_t s, bool scale = false);
 // the coarsest level's solve around a network output zn (nullptr: no
 // network): z = zn + D^-1 r (or omega D^-1 r), then two sweeps (one kernel);
 // solved: zn is already a coarse solution (z = zn, then the sweeps)

@@ -234,6 +234,30 @@ def test_fcg_on_padded_levels(torch, mode):
     P.close()
 
 
+@pytest.mark.parametrize("shape", [(16, 16, 16), (16, 8, 16)])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fcg_single_level(torch, shape, mode):
+    # every axis at most 16 cells: the hierarchy is the solver's grid alone,
+    # the network (or Jacobi) works on it directly, and FCG's dot products
+    # run as their own kernel (there is no post-smoothing kernel above the
+    # coarsest level to take them)
+    P = engine(shape, mg_coarse=mode)
+    P.poisson_generate(seed=17, radius=(2.0, 4.0))
+    P.lp_set_weights(np.load(WEIGHTS))
+    info = P.poisson_solve(method=2, tol=1e-6, max_iter=400)
+    assert info.converged == 1 and info.fell_back == 0 and info.rel_residual <= 1e-6
+    assert P.info().error_flags == 0
+    typ, b = problem_arrays(P, shape)
+    x = P.poisson_solution()
+    assert solution_residual(typ, b, x, shape) <= 1.05e-6
+    xo, ito, rro = O.mg_fcg(typ, b.astype(np.float64), np.load(WEIGHTS), shape, mode=mode, max_iter=400)
+    assert rro <= 1e-6
+    pocket, _ = sealed_pockets(typ, shape)
+    assert rel_err(remove_pocket_constants(x, xo, pocket), xo) < 2e-3
+    assert abs(info.iters - ito) <= max(4, ito // 8) + 16
+    P.close()
+
+
 def test_solve_frame_with_method_2(torch):
     # one frame of Courant sub-steps (solveFrame) with the learned multilevel
     # solve on a 32^3 grid (V-cycle 32^3 -> 16^3, the network on 16^3) against
