@@ -19,6 +19,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -178,8 +179,7 @@ class Clocks:
     def __init__(self, gpu_index):
         self.p = None
         self.t0 = self.t1 = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 ".bench_clocks_%d.csv" % gpu_index)
+        self.path = os.path.join(tempfile.gettempdir(), "flip2_b200_bench_clocks_%d_%d.csv" % (gpu_index, os.getpid()))
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + CLOCK_QUERY,
@@ -430,7 +430,7 @@ def main():
                 "algorithmic_bytes": "%d B per active voxel per iteration x %d voxels" % (per_voxel, voxels),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
 
-    # the north-star particle metric: binning, P2G and G2P/advection only
+    # the particle-stage metric: binning, P2G and G2P/advection only
     part_keys = ["keys", "sort", "gather", "segment_heads", "grid_clear", "p2g", "g2p_advect"]
     part_ms = sum(stages[k] for k in part_keys)
     particle_stages = {"value": n / (part_ms / 1e3), "unit": METRIC, "ms_per_step": part_ms, "stages": part_keys,

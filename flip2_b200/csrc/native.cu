@@ -1,4 +1,4 @@
-// native.cu -- the north-star fluid step on sm_100a (FP32 state).
+// native.cu -- the native-mode fluid step on sm_100a (FP32 state).
 //
 // Grid layout.  Voxel grids are dense, allocated once for the whole box
 // (256^3 voxels are 64 MiB per float field; a B200 holds 180 GB) and stored

@@ -8,7 +8,7 @@ namespace flip {
 // cell types
 constexpr uint8_t kAir = 0, kFluid = 1, kSolid = 2;
 
-// voxel grid of the north-star step: nx*ny*nz voxels (multiples of 8) of size
+// voxel grid of the native-mode step: nx*ny*nz voxels (multiples of 8) of size
 // h, tiles of 8^3 voxels
 struct NatDims {
     int nx, ny, nz;

@@ -277,7 +277,7 @@ int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint64_t bytes);
 
 /* ------------------------------------------------------------------ */
 /* 3. Learned pressure preconditioner and standalone pressure problems  */
-/*    (north-star additions: no reference counterpart)                  */
+/*    (native-mode additions: no reference counterpart)                 */
 /* ------------------------------------------------------------------ */
 /* The network: 3^3 convolutions 3 -> 16 -> 16 -> 16 -> 1 channels with
  * dilations 1, 2, 4, 1, ReLU after the first three, no biases; inputs are

@@ -623,7 +623,7 @@ int orc_ref_substep(int64_t n, double* px, double* py, double* pz, double* vx, d
     return 0;
 }
 
-/* ============================================ north-star step (FP64) ====
+/* =========================================== native-mode step (FP64) ====
  * Staggered MAC grid of nx*ny*nz cells of size h.  Face (i,j,k) of a
  * component is the negative face of cell (i,j,k); the positive domain wall
  * faces (i == nx) are not stored and read as 0.  Cell types: 0 air, 1 fluid,

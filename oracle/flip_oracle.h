@@ -9,8 +9,8 @@
  *               including its documented quirks, so that integer outputs
  *               (keys, permutation, prefix sums, compaction) are bit-exact and
  *               floating-point outputs agree to rounding.
- *   orc_nat_*   the north-star step (trilinear MAC P2G/G2P, FLIP blend, RK2,
- *               Jacobi-PCG) in FP64: no reference counterpart; the FP64 judge
+ *   orc_nat_*   the native-mode step (trilinear MAC P2G/G2P, FLIP blend, RK2,
+ *               Jacobi-PCG) in FP64: no reference counterpart; the FP64 check
  *               for the FP32 CUDA path.
  *
  * Parity pinning: the reference publishes no golden vectors.  The restatement
@@ -129,7 +129,7 @@ int orc_ref_substep(int64_t n, double* px, double* py, double* pz, double* vx, d
                     orc_grid g, double frameDt, double elapsedThisFrame, int permute_velocities,
                     orc_ref_step_info* info);
 
-/* ------------------------------------------------ north-star step (FP64) */
+/* ----------------------------------------------- native-mode step (FP64) */
 typedef struct {
     /* voxel grid: nx*ny*nz cells of size h, origin (ox,oy,oz) */
     double ox, oy, oz, h;
@@ -143,7 +143,7 @@ typedef struct {
 
 /* Tile key of each particle (8^3-voxel tiles, x-fastest tile order). */
 void orc_nat_keys(int64_t n, const float* pos /*xyz interleaved*/, const orc_nat_params* P, uint32_t* keys);
-/* Full north-star step on interleaved float3 positions/velocities (n*3).
+/* Full native-mode step on interleaved float3 positions/velocities (n*3).
  * solid: optional per-cell solid mask (nx*ny*nz, x fastest) or NULL.
  * Outputs the face grids after P2G (u_p2g, v_p2g, w_p2g; sizes nx*ny*nz,
  * face (i,j,k) = negative face of cell (i,j,k)), the pressure (phi),

@@ -222,7 +222,7 @@ def ref_substep(px, py, pz, vx, vy, vz, g, frame_dt=1.0 / 24.0, elapsed=0.0, per
     return arrs, info
 
 
-# ----------------------------------------------------------- north-star step
+# ---------------------------------------------------------- native-mode step
 def nat_params(nx, ny, nz, h, origin=(0.0, 0.0, 0.0), gravity_y=-9.8, flip=0.95, dt=1.0 / 240, tol=1e-6, max_iter=4000,
                solid_velocity=(0.0, 0.0, 0.0)):
     return NatParams(origin[0], origin[1], origin[2], h, nx, ny, nz, gravity_y, flip, dt, tol, max_iter, *solid_velocity)
@@ -236,7 +236,7 @@ def nat_keys(pos, P):
 
 
 def nat_step(pos, vel, P, solid=None):
-    """One north-star step in FP64.  pos/vel: (n,3) float32, updated copies returned."""
+    """One native-mode step in FP64.  pos/vel: (n,3) float32, updated copies returned."""
     pos = np.ascontiguousarray(pos, np.float32).copy()
     vel = np.ascontiguousarray(vel, np.float32).copy()
     nc = P.nx * P.ny * P.nz

@@ -1,4 +1,4 @@
-"""The north-star step (FLIP_MODE_NATIVE, FP32 state) against the FP64 oracle
+"""The native-mode step (FLIP_MODE_NATIVE, FP32 state) against the FP64 oracle
 of the same step: trilinear MAC P2G, Jacobi-PCG pressure with FP64
 reductions, projection, FLIP 0.95 blend and RK2 advection.  Tolerances are
 written per quantity below."""
