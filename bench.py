@@ -203,30 +203,39 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.p.kill()
         self.f.close()
-        rows = []
-        for line in open(self.path):
-            c = [x.strip() for x in line.split(",")]
-            if len(c) >= 9 and c[1].replace(".", "").isdigit():
-                rows.append(c)
+        with open(self.path) as f:
+            lines = f.read().splitlines()
         try:
             os.remove(self.path)
         except OSError:
             pass
+        return self.summarize(lines, self.t0, self.t1)
+
+    @staticmethod
+    def summarize(lines, t0, t1):
+        """Median SM clock, max clock, power and the active throttle reasons
+        of the CLOCK_QUERY csv lines sampled inside [t0, t1] (host times;
+        the two samples nearest the window's middle when none falls in it)."""
+        rows = []
+        for line in lines:
+            c = [x.strip() for x in line.split(",")]
+            if len(c) >= 9 and c[1].replace(".", "").isdigit():
+                rows.append(c)
         if not rows:
             return None
         window = "timed region"
-        if self.t0 is not None and self.t1 is not None:
+        if t0 is not None and t1 is not None:
             def ts(r):
                 try:
                     return datetime.datetime.strptime(r[9], "%Y/%m/%d %H:%M:%S.%f").timestamp()
                 except (IndexError, ValueError):
                     return None
             stamped = [(ts(r), r) for r in rows if ts(r) is not None]
-            inside = [r for t, r in stamped if self.t0 <= t <= self.t1]
+            inside = [r for t, r in stamped if t0 <= t <= t1]
             if inside:
                 rows = inside
             elif stamped:
-                mid = 0.5 * (self.t0 + self.t1)
+                mid = 0.5 * (t0 + t1)
                 stamped.sort(key=lambda tr: abs(tr[0] - mid))
                 rows = [r for _, r in stamped[:2]]
                 window = "nearest samples (timed region shorter than the 50 ms sampling interval)"
