@@ -145,3 +145,19 @@ def test_fcg_on_padded_levels():
     a = float(v @ O.mg_apply(t.ravel(), u, w0, shape, mode=1))
     c = float(u @ O.mg_apply(t.ravel(), v, w0, shape, mode=1))
     assert abs(a - c) <= 1e-10 * max(abs(a), 1.0)
+
+
+def test_single_level():
+    # every axis at most 16 cells: the hierarchy is the grid alone and the
+    # V-cycle is the coarsest level's start and two sweeps; FCG with it
+    # still meets the tolerance
+    for shape in ((16, 16, 16), (16, 8, 16)):
+        assert O.mg_levels(shape) == [shape]
+        t, b = problem(shape, 8)
+        r = np.where(t == FLUID, np.random.default_rng(9).standard_normal(t.shape), 0.0).astype(np.float32)
+        w0 = np.zeros(O.lib().orc_lp_num_weights(), np.float32)
+        z = O.mg_apply(t.ravel(), r.ravel(), w0, shape, mode=1)
+        zn = vcycle([t], 0, r.astype(np.float64))
+        assert np.max(np.abs(z - zn.ravel())) <= 1e-12 * np.max(np.abs(zn))
+        x, it, rr = O.mg_fcg(t.ravel(), b.ravel(), w0, shape, mode=1, max_iter=400)
+        assert rr <= 1e-6
