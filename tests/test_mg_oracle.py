@@ -161,3 +161,19 @@ def test_single_level():
         assert np.max(np.abs(z - zn.ravel())) <= 1e-12 * np.max(np.abs(zn))
         x, it, rr = O.mg_fcg(t.ravel(), b.ravel(), w0, shape, mode=1, max_iter=400)
         assert rr <= 1e-6
+
+
+def test_degenerate_problems():
+    # b = 0 on a fluid region, and a grid without fluid cells: both solves
+    # stop before their first iteration with x = 0 and a zero residual, and
+    # the V-cycle of a zero residual is zero
+    shape = (32, 32, 32)
+    t, _ = problem(shape, 10)
+    w0 = np.zeros(O.lib().orc_lp_num_weights(), np.float32)
+    for typ in (t, np.zeros_like(t)):
+        b = np.zeros(typ.size)
+        x, it, rr = O.mg_fcg(typ.ravel(), b, w0, shape, mode=1, max_iter=50)
+        assert it == 0 and rr == 0.0 and not np.any(x)
+        x, it, rr = O.nat_pcg(typ.ravel(), b, O.nat_params(*shape, 1.0, tol=1e-6, max_iter=50))
+        assert it == 0 and rr == 0.0 and not np.any(x)
+        assert not np.any(O.mg_apply(typ.ravel(), np.zeros(typ.size, np.float32), w0, shape, mode=1))
