@@ -96,6 +96,10 @@ def lib():
         "flip_inclusive_scan_scratch_bytes": (sz, [u64]),
         "flip_inclusive_scan_u32": (i32, [vp, vp, u64, vp, sz, vp]),
         "flip_inclusive_scan_u32_noalloc": (i32, [vp, vp, u64, vp]),
+        "flip_inclusive_scan_u32_noalloc_status": (i32, [vp, C.POINTER(u32)]),
+        "flip_scratch_status": (i32, [vp, vp, C.POINTER(u32)]),
+        "flip_test_lookback_timeout": (i32, [i32, vp, vp, vp, u64, u32, vp, sz, vp, C.POINTER(u32)]),
+        "flip_binary_version": (i32, [C.POINTER(i32)]),
         "flip_segment_heads_scratch_bytes": (sz, [u64]),
         "flip_segment_heads": (i32, [vp, u64, vp, vp, vp, vp, vp, sz, vp]),
         "flip_ref_ydim_rows": (i32, [vp, vp, u32, gp, vp, vp]),

@@ -36,7 +36,11 @@ struct flip_engine {
 
     // shared binning buffers
     uint32_t *keys = nullptr, *perm = nullptr, *flags = nullptr, *starts = nullptr, *node_keys = nullptr;
-    uint32_t* d_counts = nullptr;  // [0] nodes/tiles, [1] grid tiles, [2..] spare
+    uint32_t* d_counts = nullptr;  // [0] nodes/tiles, [1] grid tiles, [2] speed bits, [4] device error word, rest spare
+    // d_counts + 4: the look-back timeout bit of every sort and scan this
+    // engine runs accumulates here; read at the host sync points below
+    uint32_t* d_err = nullptr;
+    uint32_t err_seen = 0;         // device error bits reported so far (flip_get_info)
     void* sort_scratch = nullptr;
     size_t sort_scratch_bytes = 0;
     void* scan_scratch = nullptr;
@@ -161,6 +165,29 @@ static int rt_join(flip_engine* e) {
     E_CUDA(cudaStreamWaitEvent(e->stream, e->ev_down[flip_engine::kRtChunks - 1], 0));
     e->rt_down_pending = false;
     return FLIP_OK;
+}
+
+// The engine's device error word: dev_err_fetch queues its copy into the
+// pinned readback area before a synchronisation the caller makes anyway;
+// dev_err_eval, after that synchronisation, turns a set bit into
+// FLIP_ERR_TIMEOUT (and clears the word for the next call).
+static int dev_err_fetch(flip_engine* e) {
+    return e->cuda(cudaMemcpyAsync(e->h_small + 4, e->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+                   "cudaMemcpyAsync(error word)");
+}
+static int dev_err_eval(flip_engine* e) {
+    const uint32_t w = e->h_small[4];
+    if (!w) return FLIP_OK;
+    e->h_small[4] = 0;
+    e->err_seen |= w;
+    E_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream));
+    return e->fail(FLIP_ERR_TIMEOUT, "a decoupled look-back wait of the sort or scan timed out; the binning of this "
+                                     "step is invalid");
+}
+static int dev_err_check(flip_engine* e) {
+    E_TRY(dev_err_fetch(e));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    return dev_err_eval(e);
 }
 
 extern "C" void flip_default_params(int mode, flip_params* out) {
@@ -343,6 +370,9 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
     e->arena_bytes = total;
     size_t off = 0;
     for (auto& pr : plan) { *pr.first = e->arena + off; off += al(pr.second ? pr.second : 1); }
+    e->d_err = e->d_counts + 4;
+    e->err_seen = 0;
+    E_CUDA(cudaMemsetAsync(e->d_counts, 0, 64, e->stream));
     if (e->P.mode == FLIP_MODE_NATIVE) {
         // zero everything once so that stale tiles read as zero
         E_CUDA(cudaMemsetAsync(e->arena, 0, total, e->stream));
@@ -494,8 +524,8 @@ static int ref_align(flip_engine* e) {
 }
 
 static int ref_sort(flip_engine* e) {
-    E_TRY(flip_sort_pairs(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
-                          e->stream));
+    E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
+                        e->stream, e->d_err, kSpinLimit, 0));
     // sortParticles gathers positions only (particles.cu:69-71); velocities
     // keep their order unless permute_velocities is set
     int na = e->P.permute_velocities ? 6 : 3;
@@ -522,18 +552,24 @@ static int ensure_voxels(flip_engine* e, uint64_t need) {
 
 static int ref_generate_voxels(flip_engine* e) {
     if (!e->binned) return e->fail(FLIP_ERR_STATE, "generateVoxels before sortParticles");
-    E_TRY(flip_segment_heads(e->keys, e->n, e->flags, e->starts, nullptr, e->d_counts, e->scan_scratch,
-                             e->scan_scratch_bytes, e->stream));
+    if (e->n == 0) return e->fail(FLIP_ERR_STATE, "generateVoxels without particles");
+    E_TRY(launch_scan(1, e->keys, e->flags, e->n, e->scan_scratch, e->scan_scratch_bytes, e->stream, e->starts, nullptr,
+                      e->d_counts, e->d_err, kSpinLimit, 0));
     E_CUDA(cudaMemcpyAsync(e->h_small, e->d_counts, 4, cudaMemcpyDeviceToHost, e->stream));
+    E_TRY(dev_err_fetch(e));
     E_CUDA(cudaStreamSynchronize(e->stream));
+    E_TRY(dev_err_eval(e));
     e->nodes = e->h_small[0];
     if (e->nodes == 0 || e->nodes > e->node_cap) return e->fail(FLIP_ERR_STATE, "node count out of range");
     E_TRY(ref_launch_ydim(e->starts, e->keys, e->nodes, e->grid, e->ytable, e->stream));
     E_TRY(ref_launch_voxel_counts(e->starts, e->keys, e->nodes, e->n, e->pd[0], e->pd[1], e->pd[2], e->grid, e->counts,
                                   e->masks, e->stream));
-    E_TRY(flip_inclusive_scan_u32(e->counts, e->node_voxels, e->nodes, e->scan_scratch, e->scan_scratch_bytes, e->stream));
+    E_TRY(launch_scan(0, e->counts, e->node_voxels, e->nodes, e->scan_scratch, e->scan_scratch_bytes, e->stream, nullptr,
+                      nullptr, nullptr, e->d_err, kSpinLimit, 0));
     E_CUDA(cudaMemcpyAsync(e->h_small, e->node_voxels + e->nodes - 1, 4, cudaMemcpyDeviceToHost, e->stream));
+    E_TRY(dev_err_fetch(e));
     E_CUDA(cudaStreamSynchronize(e->stream));
+    E_TRY(dev_err_eval(e));
     e->voxels = e->h_small[0];
     E_TRY(ensure_voxels(e, e->voxels));
     E_TRY(ref_launch_voxel_ids(e->keys, e->nodes, e->masks, e->node_voxels, e->grid, e->voxel_ids, e->solids, e->stream));
@@ -668,14 +704,18 @@ static int nat_bin(flip_engine* e) {
     E_TRY(e->mark(0));
     E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
     E_TRY(e->mark(1));
-    E_TRY(flip_sort_pairs(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
-                          e->stream));
+    E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
+                        e->stream, e->d_err, kSpinLimit, 0));
     E_TRY(e->mark(2));
     E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
     for (int a = 0; a < 6; ++a) std::swap(e->fp[a], e->fq[a]);
     E_TRY(e->mark(3));
-    E_TRY(flip_segment_heads(e->keys, e->n, nullptr, e->starts, e->node_keys, e->d_counts, e->scan_scratch,
-                             e->scan_scratch_bytes, e->stream));
+    if (e->n == 0) {
+        E_CUDA(cudaMemsetAsync(e->d_counts, 0, sizeof(uint32_t), e->stream));
+    } else {
+        E_TRY(launch_scan(1, e->keys, nullptr, e->n, e->scan_scratch, e->scan_scratch_bytes, e->stream, e->starts,
+                          e->node_keys, e->d_counts, e->d_err, kSpinLimit, 0));
+    }
     E_TRY(e->mark(4));
     e->launches += 1 + 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 1;
     e->binned = true;
@@ -1063,9 +1103,10 @@ static int nat_mgpcg_graph(flip_engine* e, int iters, int max_iter, bool network
 static int run_loop(flip_engine* e, cudaGraphExec_t g, uint32_t launches_per_chunk) {
     E_CUDA(cudaGraphLaunch(g, e->stream));
     E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
+    E_TRY(dev_err_fetch(e));
     E_CUDA(cudaStreamSynchronize(e->stream));
     e->launches += (launches_per_chunk + 1u) * (uint32_t)e->h_state->chunks;
-    return FLIP_OK;
+    return dev_err_eval(e);
 }
 
 // Solve A x = b on the occupied tiles.  U: face velocities giving b = -div U,
@@ -1318,8 +1359,7 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
             E_TRY(ref_generate_voxels(e));
             if (++guard > 1000000) return e->fail(FLIP_ERR_STATE, "solveFrame: dt collapsed");
         }
-        E_CUDA(cudaStreamSynchronize(e->stream));
-        return FLIP_OK;
+        return dev_err_check(e);
     }
     // sub-steps of min(max_substep_dt, the Courant limit, what is left of the frame)
     const double frameDt = 1.0 / fps;
@@ -1333,8 +1373,7 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
         E_TRY(nat_step(e, dt));
         t += dt;
     }
-    E_CUDA(cudaStreamSynchronize(e->stream));
-    return FLIP_OK;
+    return dev_err_check(e);
 }
 
 extern "C" int flip_step(flip_engine* e, double dt) {
@@ -1366,8 +1405,11 @@ extern "C" int flip_step(flip_engine* e, double dt) {
 extern "C" int flip_sync(flip_engine* e) {
     if (!e) return FLIP_ERR_ARG;
     E_TRY(rt_join(e));  // the last streamed download, in the engine stream's order
-    E_CUDA(cudaStreamSynchronize(e->stream));
-    return FLIP_OK;
+    if (!e->have_domain) {
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        return FLIP_OK;
+    }
+    return dev_err_check(e);
 }
 
 static int rt_setup(flip_engine* e) {
@@ -1555,21 +1597,19 @@ extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
             out->pressure_iters = e->last_iters;
             out->converged = e->last_converged;
             out->residual = e->last_rel;
-            uint32_t ew[3] = {0, 0, 0};
-            E_CUDA(cudaMemcpy(ew, e->sort_scratch, 4, cudaMemcpyDeviceToHost));
-            E_CUDA(cudaMemcpy(ew + 1, e->scan_scratch, 4, cudaMemcpyDeviceToHost));
-            if (e->lp.err) E_CUDA(cudaMemcpy(ew + 2, e->lp.err, 4, cudaMemcpyDeviceToHost));
-            out->error_flags = ew[0] | ew[1] | (ew[2] ? 0x4u : 0u);
+            uint32_t ew[2] = {0, 0};
+            E_CUDA(cudaMemcpy(ew, e->d_err, 4, cudaMemcpyDeviceToHost));
+            if (e->lp.err) E_CUDA(cudaMemcpy(ew + 1, e->lp.err, 4, cudaMemcpyDeviceToHost));
+            out->error_flags = e->err_seen | ew[0] | (ew[1] ? 0x4u : 0u);
         } else {
             out->nodes = e->nodes;
             out->voxels = e->voxels;
             out->pressure_iters = (int32_t)e->gs_iters;
             out->converged = e->residual < 0.01 ? 1 : 0;
             out->residual = e->residual;
-            uint32_t ew[2] = {0, 0};
-            E_CUDA(cudaMemcpy(ew, e->sort_scratch, 4, cudaMemcpyDeviceToHost));
-            E_CUDA(cudaMemcpy(ew + 1, e->scan_scratch, 4, cudaMemcpyDeviceToHost));
-            out->error_flags = ew[0] | ew[1];
+            uint32_t w = 0;
+            E_CUDA(cudaMemcpy(&w, e->d_err, 4, cudaMemcpyDeviceToHost));
+            out->error_flags = e->err_seen | w;
         }
     }
     out->dt = e->dt;

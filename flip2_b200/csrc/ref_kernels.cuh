@@ -43,7 +43,8 @@ int ref_gather_f64(const uint32_t* perm, uint64_t n, const double* in, double* o
 
 // scan.cu
 int launch_scan(int mode, const uint32_t* in, uint32_t* out, uint64_t n, void* scratch, size_t bytes, cudaStream_t s,
-                uint32_t* starts, uint32_t* node_keys, uint32_t* d_count);
+                uint32_t* starts, uint32_t* node_keys, uint32_t* d_count, uint32_t* err_accum, uint32_t spin_limit,
+                uint32_t tile_base);
 size_t scan_scratch_bytes(uint64_t n);
 
 }  // namespace flip

@@ -93,7 +93,8 @@ template <bool kIota>
 __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, uint64_t n, int shift, const uint32_t* __restrict__ offsets,
-    uint32_t* __restrict__ status, uint32_t* __restrict__ tile_ctr, uint32_t* __restrict__ err) {
+    uint32_t* __restrict__ status, uint32_t* __restrict__ tile_ctr, uint32_t* __restrict__ err, uint32_t spin_limit,
+    uint32_t tile_base) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_whist[kSortWarps][kRadix];  // warp counts, then warp offsets within the digit
     __shared__ uint32_t s_blk[kRadix];                // tile-local exclusive offset of each digit
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     __shared__ uint32_t s_vals[kSortTile];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u) + tile_base;
     for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&s_whist[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
             uint32_t s = ld_relaxed_u32(status + (size_t)t * kRadix + d);
             uint32_t f = s & ~kValueMask;
             if (f == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
                     break;
                 }
@@ -200,9 +201,9 @@ using namespace flip;
 
 extern "C" size_t flip_sort_pairs_scratch_bytes(uint64_t n) { return sort_layout(n).total; }
 
-extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
-                               uint32_t* vals_out, uint64_t n, int key_bits, void* scratch, size_t scratch_bytes,
-                               void* stream_) {
+int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                        uint64_t n, int key_bits, void* scratch, size_t scratch_bytes, cudaStream_t s,
+                        uint32_t* err_accum, uint32_t spin_limit, uint32_t tile_base) {
     if (n == 0) return FLIP_OK;
     if (!keys_in || !keys_out || !vals_out || !scratch || key_bits < 1 || key_bits > 32 || n >= (1ull << 30)) {
         set_error_text("flip_sort_pairs: bad argument (null pointer, key_bits outside 1..32 or n >= 2^30)");
@@ -213,9 +214,8 @@ extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in,
         set_error_text("flip_sort_pairs: scratch too small");
         return FLIP_ERR_ARG;
     }
-    cudaStream_t s = as_stream(stream_);
     char* S = (char*)scratch;
-    uint32_t* err = (uint32_t*)(S + L.err);
+    uint32_t* err = err_accum ? err_accum : (uint32_t*)(S + L.err);
     uint32_t* hist = (uint32_t*)(S + L.hist);
     uint32_t* offs = (uint32_t*)(S + L.offsets);
     uint32_t* ctr = (uint32_t*)(S + L.ctr);
@@ -224,6 +224,11 @@ extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in,
     uint32_t* av = (uint32_t*)(S + L.alt_v);
     const int passes = (key_bits + 7) / 8;
     const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    if (tile_base >= tiles) {
+        set_error_text("flip_sort_pairs: tile_base beyond the tile count");
+        return FLIP_ERR_ARG;
+    }
+    const unsigned grid = (unsigned)(tiles - tile_base);
     // error word, histograms, offsets, counters and look-back words are
     // contiguous at the start of the scratch: clear them in one memset
     FLIP_CUDA_TRY(cudaMemsetAsync(S, 0, L.status + sizeof(uint32_t) * passes * tiles * kRadix, s));
@@ -245,11 +250,11 @@ extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in,
         uint32_t* ov = to_out ? vals_out : av;
         uint32_t* pstat = status + (size_t)p * tiles * kRadix;
         if (p == 0 && cv == nullptr)
-            onesweep_kernel<true><<<(unsigned)tiles, kSortThreads, 0, s>>>(ck, nullptr, ok, ov, n, 8 * p, offs + p * kRadix,
-                                                                          pstat, ctr + p, err);
+            onesweep_kernel<true><<<grid, kSortThreads, 0, s>>>(ck, nullptr, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
+                                                                ctr + p, err, spin_limit, tile_base);
         else
-            onesweep_kernel<false><<<(unsigned)tiles, kSortThreads, 0, s>>>(ck, cv, ok, ov, n, 8 * p, offs + p * kRadix,
-                                                                           pstat, ctr + p, err);
+            onesweep_kernel<false><<<grid, kSortThreads, 0, s>>>(ck, cv, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
+                                                                 ctr + p, err, spin_limit, tile_base);
         ck = ok;
         cv = ov;
     }
@@ -259,4 +264,11 @@ extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in,
     }
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
+}
+
+extern "C" int flip_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                               uint32_t* vals_out, uint64_t n, int key_bits, void* scratch, size_t scratch_bytes,
+                               void* stream) {
+    return sort_pairs_ex(keys_in, vals_in, keys_out, vals_out, n, key_bits, scratch, scratch_bytes, as_stream(stream),
+                         nullptr, kSpinLimit, 0);
 }

@@ -49,6 +49,10 @@ typedef struct {
 /* Library version and the status string of the last failure on this thread. */
 const char* flip_version(void);
 const char* flip_status_string(int status);
+/* Architecture of the device code the runtime loaded for this library
+ * (cudaFuncAttributes::binaryVersion of its scan kernel): 100 for sm_100a.
+ * Needs a visible device.  No reference counterpart. */
+int flip_binary_version(int* version);
 
 /* ------------------------------------------------------------------ */
 /* 1. Primitives                                                       */
@@ -85,8 +89,34 @@ int flip_inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, void*
  * in and out are passed.  n <= 2^28, else FLIP_ERR_ARG.  Calls share that
  * array: calls that overlap on the GPU race and must be serialised.  The
  * first call on each device resolves the array's address; make it before any
- * stream capture. */
+ * stream capture (a failed lookup is retried by the next call).  The call
+ * returns before its kernel runs, so a look-back wait that gives up is
+ * reported by flip_inclusive_scan_u32_noalloc_status, not by this call. */
 int flip_inclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint64_t n, void* stream);
+/* Companion of flip_inclusive_scan_u32_noalloc (no counterpart in the
+ * reference; allocates nothing): waits for `stream`, then copies the static
+ * array's error word of the last call on the current device into *flags.
+ * Returns FLIP_ERR_TIMEOUT when bit 0 (a look-back wait gave up) is set: that
+ * call's output is invalid. */
+int flip_inclusive_scan_u32_noalloc_status(void* stream, uint32_t* flags);
+
+/* Device status of the last flip_sort_pairs, flip_inclusive_scan_u32 or
+ * flip_segment_heads call that used `scratch` (no reference counterpart: the
+ * reference's kernels have no failure word).  Waits for `stream`, then copies
+ * the scratch's first word into *flags.  Bit 0 means a decoupled look-back
+ * wait gave up after its poll limit (the kernel returned, but its output is
+ * invalid): FLIP_ERR_TIMEOUT is returned. */
+int flip_scratch_status(const void* scratch, void* stream, uint32_t* flags);
+/* Test hook for those bounded waits (no reference counterpart): the scan
+ * (which = 0, out_keys receives the scan) or the sort with the index payload
+ * (which = 1, 32-bit keys) of n > 4096 keys from `in`, run with tile 0 never
+ * claimed, so that tile 1's look-back polls a word nothing publishes and
+ * gives up after spin_limit polls.  Returns flip_scratch_status's result:
+ * FLIP_ERR_TIMEOUT with bit 0 in *flags.  The outputs are invalid; the
+ * context stays usable. */
+int flip_test_lookback_timeout(int which, const uint32_t* in, uint32_t* out_keys, uint32_t* out_vals, uint64_t n,
+                               uint32_t spin_limit, void* scratch, size_t scratch_bytes, void* stream,
+                               uint32_t* flags);
 
 /* Segment heads of sorted keys, fused: replaces cudaMarkUniqueGridCellsAndCount
  * + cudaMapNodeIndicesToParticles (particleToGridFunctions.cu:303-345).
@@ -362,9 +392,13 @@ typedef struct {
     double residual;         /* last terminating residual (relative for NATIVE)  */
     double elapsed_time;
     uint64_t n;
-    uint32_t error_flags;    /* device error word (bit 0: look-back timeout;
-                                bit 2: a tensor-core wait of the learned
-                                preconditioner timed out)                        */
+    uint32_t error_flags;    /* device error bits seen since setDomain (bit 0: a
+                                look-back wait of a sort or scan timed out, which
+                                the next synchronising call -- flip_sync,
+                                flip_solve_frame, generateVoxels, the end of each
+                                native pressure solve -- also returns as
+                                FLIP_ERR_TIMEOUT; bit 2: a tensor-core wait of the
+                                learned preconditioner timed out)                */
     uint32_t launches;       /* kernels this engine launched since creation      */
 } flip_info;
 int flip_get_info(flip_engine* e, flip_info* out);

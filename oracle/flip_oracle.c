@@ -677,6 +677,34 @@ static inline int nat_wall(const orc_nat_params* P, int c, int i, int j, int k) 
     return k == 0 || k == P->nz;
 }
 
+/* P2G of one particle into the face sums (wall faces skipped) */
+static void nat_p2g_particle(const orc_nat_params* P, int64_t nc, const float* pos, const float* vel, int64_t p,
+                             double* const* comp, double* wt) {
+    double gx = ((double)pos[3 * p] - P->ox) / P->h;
+    double gy = ((double)pos[3 * p + 1] - P->oy) / P->h;
+    double gz = ((double)pos[3 * p + 2] - P->oz) / P->h;
+    for (int c = 0; c < 3; ++c) {
+        int i0, j0, k0;
+        double fx, fy, fz;
+        nat_stencil(P, c, gx, gy, gz, &i0, &j0, &k0, &fx, &fy, &fz);
+        for (int dk = 0; dk < 2; ++dk)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int di = 0; di < 2; ++di) {
+                    int i = i0 + di, j = j0 + dj, k = k0 + dk;
+                    if (nat_wall(P, c, i, j, k)) continue;
+                    double ww = (di ? fx : 1.0 - fx) * (dj ? fy : 1.0 - fy) * (dk ? fz : 1.0 - fz);
+                    int64_t id = nat_idx(P, i, j, k);
+                    comp[c][id] += ww * (double)vel[3 * p + c];
+                    wt[(int64_t)c * nc + id] += ww;
+                }
+    }
+}
+
+/* Trilinear P2G onto the staggered faces, sums in FP64.  Particles are
+ * bucketed by 8-cell slabs of z; a particle of slab s touches nodes of z in
+ * [8s-1, 8s+8] only, so slabs two apart never share a node: the even slabs
+ * run in parallel, then the odd ones.  Within a slab particles keep their
+ * input order, so the result does not depend on the thread count. */
 void orc_nat_p2g(int64_t n, const float* pos, const float* vel, const orc_nat_params* P,
                  double* u, double* v, double* w, uint8_t* fluid) {
     int64_t nc = (int64_t)P->nx * P->ny * P->nz;
@@ -685,30 +713,29 @@ void orc_nat_p2g(int64_t n, const float* pos, const float* vel, const orc_nat_pa
     for (int c = 0; c < 3; ++c) memset(comp[c], 0, sizeof(double) * (size_t)nc);
     if (fluid) memset(fluid, 0, (size_t)nc);
     float fox = (float)P->ox, foy = (float)P->oy, foz = (float)P->oz, fh = (float)P->h;
+    const int nslab = (P->nz + 7) / 8;
+    int64_t* cnt = (int64_t*)calloc((size_t)nslab + 1, sizeof(int64_t));
+    int* slab = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     for (int64_t p = 0; p < n; ++p) {
-        double gx = ((double)pos[3 * p] - P->ox) / P->h;
-        double gy = ((double)pos[3 * p + 1] - P->oy) / P->h;
-        double gz = ((double)pos[3 * p + 2] - P->oz) / P->h;
-        if (fluid) fluid[nat_idx(P, nat_cell(pos[3 * p], fox, fh, P->nx), nat_cell(pos[3 * p + 1], foy, fh, P->ny),
-                                 nat_cell(pos[3 * p + 2], foz, fh, P->nz))] = 1;
-        for (int c = 0; c < 3; ++c) {
-            int i0, j0, k0;
-            double fx, fy, fz;
-            nat_stencil(P, c, gx, gy, gz, &i0, &j0, &k0, &fx, &fy, &fz);
-            for (int dk = 0; dk < 2; ++dk)
-                for (int dj = 0; dj < 2; ++dj)
-                    for (int di = 0; di < 2; ++di) {
-                        int i = i0 + di, j = j0 + dj, k = k0 + dk;
-                        if (nat_wall(P, c, i, j, k)) continue;
-                        double ww = (di ? fx : 1.0 - fx) * (dj ? fy : 1.0 - fy) * (dk ? fz : 1.0 - fz);
-                        int64_t id = nat_idx(P, i, j, k);
-                        comp[c][id] += ww * (double)vel[3 * p + c];
-                        wt[(int64_t)c * nc + id] += ww;
-                    }
-        }
+        int kc = nat_cell(pos[3 * p + 2], foz, fh, P->nz);
+        slab[p] = kc / 8;
+        cnt[slab[p] + 1]++;
+        if (fluid) fluid[nat_idx(P, nat_cell(pos[3 * p], fox, fh, P->nx), nat_cell(pos[3 * p + 1], foy, fh, P->ny), kc)] = 1;
     }
-    for (int c = 0; c < 3; ++c)
-        for (int64_t id = 0; id < nc; ++id) {
+    for (int s2 = 0; s2 < nslab; ++s2) cnt[s2 + 1] += cnt[s2];
+    int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+    int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)nslab);
+    memcpy(fill, cnt, sizeof(int64_t) * (size_t)nslab);
+    for (int64_t p = 0; p < n; ++p) order[fill[slab[p]]++] = p;
+    for (int phase = 0; phase < 2; ++phase) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int sl = phase; sl < nslab; sl += 2)
+            for (int64_t q = cnt[sl]; q < cnt[sl + 1]; ++q) nat_p2g_particle(P, nc, pos, vel, order[q], comp, wt);
+    }
+    free(cnt); free(slab); free(order); free(fill);
+#pragma omp parallel for schedule(static)
+    for (int64_t id = 0; id < nc; ++id)
+        for (int c = 0; c < 3; ++c) {
             double ww = wt[(int64_t)c * nc + id];
             comp[c][id] = ww > 0.0 ? comp[c][id] / ww : 0.0;
         }
@@ -746,50 +773,98 @@ static double nat_dot(int64_t nc, const double* a, const double* b) {
     return s;
 }
 
+/* Jacobi-PCG over the fluid cells, FP64 throughout.  The work runs on the
+ * list of fluid cells (OpenMP); dot products are OpenMP reductions. */
 int orc_nat_pcg(const uint8_t* type, const double* b, double* x, const orc_nat_params* P, double* rel_res) {
     static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
     int64_t nc = (int64_t)P->nx * P->ny * P->nz;
+    int64_t nf = 0;
+    for (int64_t i = 0; i < nc; ++i) nf += (type[i] == NAT_FLUID);
+    int64_t* fl = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nf > 0 ? nf : 1));
+    /* neighbour slots of each fluid cell: -1 solid (no coupling), -2 air (Dirichlet 0) */
+    int64_t* nb = (int64_t*)malloc(sizeof(int64_t) * 6 * (size_t)(nf > 0 ? nf : 1));
     double* r = (double*)calloc((size_t)nc, 8);
     double* z = (double*)calloc((size_t)nc, 8);
     double* p = (double*)calloc((size_t)nc, 8);
     double* q = (double*)calloc((size_t)nc, 8);
     double* dinv = (double*)calloc((size_t)nc, 8);
-    for (int k = 0; k < P->nz; ++k)
-        for (int j = 0; j < P->ny; ++j)
-            for (int i = 0; i < P->nx; ++i) {
-                int64_t id = nat_idx(P, i, j, k);
-                if (type[id] != NAT_FLUID) continue;
-                int d = 0;
-                for (int s = 0; s < 6; ++s)
-                    if (nat_type(P, type, i + off[s][0], j + off[s][1], k + off[s][2]) != NAT_SOLID) ++d;
-                dinv[id] = d ? 1.0 / d : 0.0;
-            }
-    for (int64_t i = 0; i < nc; ++i) { x[i] = 0.0; r[i] = (type[i] == NAT_FLUID) ? b[i] : 0.0; z[i] = r[i] * dinv[i]; p[i] = z[i]; }
-    double bn = sqrt(nat_dot(nc, r, r));
-    double rz = nat_dot(nc, r, z);
+    {
+        int64_t f = 0;
+        for (int k = 0; k < P->nz; ++k)
+            for (int j = 0; j < P->ny; ++j)
+                for (int i = 0; i < P->nx; ++i) {
+                    int64_t id = nat_idx(P, i, j, k);
+                    if (type[id] != NAT_FLUID) continue;
+                    int d = 0;
+                    for (int s = 0; s < 6; ++s) {
+                        int ii = i + off[s][0], jj = j + off[s][1], kk = k + off[s][2];
+                        int t = nat_type(P, type, ii, jj, kk);
+                        if (t != NAT_SOLID) ++d;
+                        nb[6 * f + s] = (t == NAT_SOLID) ? -1 : (t == NAT_FLUID ? nat_idx(P, ii, jj, kk) : -2);
+                    }
+                    dinv[id] = d ? 1.0 / d : 0.0;
+                    fl[f++] = id;
+                }
+    }
+#define PCG_FOR _Pragma("omp parallel for schedule(static)") for (int64_t f = 0; f < nf; ++f)
+    double bb = 0.0;
+#pragma omp parallel for reduction(+ : bb) schedule(static)
+    for (int64_t f = 0; f < nf; ++f) { int64_t id = fl[f]; bb += b[id] * b[id]; }
+    PCG_FOR { int64_t id = fl[f]; r[id] = b[id]; z[id] = r[id] * dinv[id]; p[id] = z[id]; }
+    for (int64_t i = 0; i < nc; ++i) x[i] = 0.0;
+    double bn = sqrt(bb);
+    double rz = 0.0;
+#pragma omp parallel for reduction(+ : rz) schedule(static)
+    for (int64_t f = 0; f < nf; ++f) { int64_t id = fl[f]; rz += r[id] * z[id]; }
     int it = 0;
     if (bn > 0.0) {
         for (it = 1; it <= P->max_iter; ++it) {
-            orc_nat_apply_A(type, p, q, P);
-            double alpha = rz / nat_dot(nc, p, q);
-            for (int64_t i = 0; i < nc; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
-            double rr = nat_dot(nc, r, r);
+            double pq = 0.0;
+#pragma omp parallel for reduction(+ : pq) schedule(static)
+            for (int64_t f = 0; f < nf; ++f) {
+                int64_t id = fl[f];
+                double d = 0.0, sn = 0.0;
+                for (int s = 0; s < 6; ++s) {
+                    int64_t m = nb[6 * f + s];
+                    if (m == -1) continue;
+                    d += 1.0;
+                    if (m >= 0) sn += p[m];
+                }
+                q[id] = d * p[id] - sn;
+                pq += p[id] * q[id];
+            }
+            double alpha = rz / pq;
+            double rr = 0.0;
+#pragma omp parallel for reduction(+ : rr) schedule(static)
+            for (int64_t f = 0; f < nf; ++f) {
+                int64_t id = fl[f];
+                x[id] += alpha * p[id];
+                r[id] -= alpha * q[id];
+                rr += r[id] * r[id];
+            }
             if (sqrt(rr) <= P->tol * bn) break;
-            for (int64_t i = 0; i < nc; ++i) z[i] = r[i] * dinv[i];
-            double rzn = nat_dot(nc, r, z);
+            double rzn = 0.0;
+#pragma omp parallel for reduction(+ : rzn) schedule(static)
+            for (int64_t f = 0; f < nf; ++f) {
+                int64_t id = fl[f];
+                z[id] = r[id] * dinv[id];
+                rzn += r[id] * z[id];
+            }
             double beta = rzn / rz;
             rz = rzn;
-            for (int64_t i = 0; i < nc; ++i) p[i] = z[i] + beta * p[i];
+            PCG_FOR { int64_t id = fl[f]; p[id] = z[id] + beta * p[id]; }
         }
         if (it > P->max_iter) it = P->max_iter;
     }
+#undef PCG_FOR
     if (rel_res) {
         orc_nat_apply_A(type, x, q, P);
         double s = 0.0;
-        for (int64_t i = 0; i < nc; ++i) if (type[i] == NAT_FLUID) { double e = b[i] - q[i]; s += e * e; }
+#pragma omp parallel for reduction(+ : s) schedule(static)
+        for (int64_t f = 0; f < nf; ++f) { int64_t id = fl[f]; double e = b[id] - q[id]; s += e * e; }
         *rel_res = bn > 0.0 ? sqrt(s) / bn : 0.0;
     }
-    free(r); free(z); free(p); free(q); free(dinv);
+    free(r); free(z); free(p); free(q); free(dinv); free(fl); free(nb);
     return it;
 }
 
@@ -811,6 +886,12 @@ static double nat_sample(const orc_nat_params* P, const double* f, int c, double
 
 int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const orc_nat_params* P,
                  double* u_p2g, double* v_p2g, double* w_p2g, double* phi, orc_nat_info* info) {
+    return orc_nat_step_ex(n, pos, vel, solid, P, u_p2g, v_p2g, w_p2g, phi, NULL, NULL, NULL, info);
+}
+
+int orc_nat_step_ex(int64_t n, float* pos, float* vel, const uint8_t* solid, const orc_nat_params* P,
+                    double* u_p2g, double* v_p2g, double* w_p2g, double* phi, double* u_proj, double* v_proj,
+                    double* w_proj, orc_nat_info* info) {
     int64_t nc = (int64_t)P->nx * P->ny * P->nz;
     double* U[3];
     double* Uo[3];
@@ -833,6 +914,7 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
      * touching fluid get gravity */
     const double us[3] = {P->solid_u, P->solid_v, P->solid_w};
     for (int c = 0; c < 3; ++c)
+#pragma omp parallel for schedule(static)
         for (int k = 0; k < P->nz; ++k)
             for (int j = 0; j < P->ny; ++j)
                 for (int i = 0; i < P->nx; ++i) {
@@ -847,6 +929,7 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
                     if (c == 1 && (ta == NAT_FLUID || tb == NAT_FLUID)) U[c][id] += P->gravity_y * P->dt;
                 }
     /* divergence -> b = -div on fluid cells */
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < P->nz; ++k)
         for (int j = 0; j < P->ny; ++j)
             for (int i = 0; i < P->nx; ++i) {
@@ -863,6 +946,7 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
     if (phi) memcpy(phi, x, 8 * (size_t)nc);
     /* projection of fluid-adjacent faces */
     for (int c = 0; c < 3; ++c)
+#pragma omp parallel for schedule(static)
         for (int k = 0; k < P->nz; ++k)
             for (int j = 0; j < P->ny; ++j)
                 for (int i = 0; i < P->nx; ++i) {
@@ -875,10 +959,14 @@ int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const 
                     double pa = (ta == NAT_FLUID) ? x[nat_idx(P, ia, ja, ka)] : 0.0;
                     U[c][id] -= pb - pa;
                 }
+    if (u_proj) memcpy(u_proj, U[0], 8 * (size_t)nc);
+    if (v_proj) memcpy(v_proj, U[1], 8 * (size_t)nc);
+    if (w_proj) memcpy(w_proj, U[2], 8 * (size_t)nc);
     /* G2P: FLIP blend, then RK2 through the grid velocity; clamp into the box */
     double lo[3] = {P->ox, P->oy, P->oz};
     double hi[3] = {P->ox + P->nx * P->h, P->oy + P->ny * P->h, P->oz + P->nz * P->h};
     double eps = 1e-3 * P->h;
+#pragma omp parallel for schedule(static)
     for (int64_t p = 0; p < n; ++p) {
         double g0[3] = {((double)pos[3 * p] - P->ox) / P->h, ((double)pos[3 * p + 1] - P->oy) / P->h, ((double)pos[3 * p + 2] - P->oz) / P->h};
         double un[3];

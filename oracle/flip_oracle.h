@@ -155,6 +155,11 @@ typedef struct {
 } orc_nat_info;
 int orc_nat_step(int64_t n, float* pos, float* vel, const uint8_t* solid, const orc_nat_params* P,
                  double* u_p2g, double* v_p2g, double* w_p2g, double* phi, orc_nat_info* info);
+/* The same step, also writing the face grids after the projection (u_proj,
+ * v_proj, w_proj; any may be NULL): the grid velocity G2P samples. */
+int orc_nat_step_ex(int64_t n, float* pos, float* vel, const uint8_t* solid, const orc_nat_params* P,
+                    double* u_p2g, double* v_p2g, double* w_p2g, double* phi, double* u_proj, double* v_proj,
+                    double* w_proj, orc_nat_info* info);
 /* Individual pieces, for stage-level checks. */
 void orc_nat_p2g(int64_t n, const float* pos, const float* vel, const orc_nat_params* P,
                  double* u, double* v, double* w, uint8_t* fluid);

@@ -75,6 +75,8 @@ def lib():
             "orc_ref_substep": (I, [I64, f64p, f64p, f64p, f64p, f64p, f64p, Grid, D, D, I, C.POINTER(RefStepInfo)]),
             "orc_nat_keys": (None, [I64, f32p, C.POINTER(NatParams), u32p]),
             "orc_nat_step": (I, [I64, f32p, f32p, C.c_void_p, C.POINTER(NatParams), f64p, f64p, f64p, f64p, C.POINTER(NatInfo)]),
+            "orc_nat_step_ex": (I, [I64, f32p, f32p, C.c_void_p, C.POINTER(NatParams), f64p, f64p, f64p, f64p, f64p, f64p,
+                                    f64p, C.POINTER(NatInfo)]),
             "orc_nat_p2g": (None, [I64, f32p, f32p, C.POINTER(NatParams), f64p, f64p, f64p, u8p]),
             "orc_nat_pcg": (I, [u8p, f64p, f64p, C.POINTER(NatParams), C.POINTER(D)]),
             "orc_nat_apply_A": (None, [u8p, f64p, f64p, C.POINTER(NatParams)]),
@@ -236,19 +238,21 @@ def nat_keys(pos, P):
 
 
 def nat_step(pos, vel, P, solid=None):
-    """One native-mode step in FP64.  pos/vel: (n,3) float32, updated copies returned."""
+    """One native-mode step in FP64.  pos/vel: (n,3) float32, updated copies
+    returned, with the face grids after P2G (u, v, w) and after the projection
+    (u_proj, v_proj, w_proj), x fastest."""
     pos = np.ascontiguousarray(pos, np.float32).copy()
     vel = np.ascontiguousarray(vel, np.float32).copy()
     nc = P.nx * P.ny * P.nz
-    u, v, w, phi = (np.empty(nc, np.float64) for _ in range(4))
+    u, v, w, phi, uq, vq, wq = (np.empty(nc, np.float64) for _ in range(7))
     info = NatInfo()
     sp = None
     if solid is not None:
         solid = np.ascontiguousarray(solid, np.uint8)
         sp = solid.ctypes.data
-    lib().orc_nat_step(pos.shape[0], pos, vel, sp, C.byref(P), u, v, w, phi, C.byref(info))
-    return dict(pos=pos, vel=vel, u=u, v=v, w=w, phi=phi, iters=info.iters, rel_residual=info.rel_residual,
-                fluid_cells=info.fluid_cells)
+    lib().orc_nat_step_ex(pos.shape[0], pos, vel, sp, C.byref(P), u, v, w, phi, uq, vq, wq, C.byref(info))
+    return dict(pos=pos, vel=vel, u=u, v=v, w=w, phi=phi, u_proj=uq, v_proj=vq, w_proj=wq, iters=info.iters,
+                rel_residual=info.rel_residual, fluid_cells=info.fluid_cells)
 
 
 def nat_pcg(type_, b, P):

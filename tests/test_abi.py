@@ -30,13 +30,21 @@ def test_library_loads_and_binds():
         assert hasattr(L, s)
 
 
-def test_sm100a_code_only():
-    """The library carries sm_100a SASS (and no other architecture)."""
-    out = subprocess.run(["cuobjdump", "--list-elf", F.LIB_PATH], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    arches = set(re.findall(r"sm_(\d+a?)", out.stdout))
-    assert arches == {"100a"}, arches
+def test_sm100a_build_flags():
+    """Every object of the library is compiled for sm_100a and nothing else."""
+    from flip2_b200 import build as B
+    assert B.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert "-gencode" not in " ".join(B.NVCC_FLAGS).replace(" ".join(B.ARCH), "")
+
+
+@pytest.mark.gpu
+def test_sm100a_code_loaded():
+    """The runtime loads sm_100 device code for the library's kernels
+    (cudaFuncAttributes::binaryVersion through the C ABI)."""
+    L = F.lib()
+    v = C.c_int(0)
+    assert L.flip_binary_version(C.byref(v)) == 0
+    assert v.value == 100, v.value
 
 
 def test_scratch_size_queries():

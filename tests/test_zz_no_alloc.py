@@ -51,3 +51,34 @@ def test_noalloc_scan_rejects_sizes_beyond_its_static_scratch():
     dummy = C.c_void_p(16)  # never dereferenced: the size check comes first
     assert L.flip_inclusive_scan_u32_noalloc(dummy, dummy, (1 << 28) + 1, None) == 1
     assert b"2^28" in L.flip_last_error(None)
+
+
+def test_noalloc_scan_status_reports_no_timeout_after_good_calls():
+    import torch
+    L = F.lib()
+    x = np.arange(50_000, dtype=np.uint32)
+    _scan_both(torch, x)
+    flags = C.c_uint32(0xFFFFFFFF)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.flip_inclusive_scan_u32_noalloc_status(stream, C.byref(flags)) == 0
+    assert flags.value == 0
+
+
+@pytest.mark.parametrize("n", [(1 << 28) - 4096, (1 << 28) - 4095, 1 << 28])
+def test_noalloc_scan_at_its_size_limit(n):
+    """2^28 elements fill every status word of the static array (65,536 tiles
+    of 4096); 2^28 - 4095 reaches the last word with a one-element tile, and
+    2^28 - 4096 stops one tile short of it.  All-ones input: the scan is
+    1, 2, ..., n."""
+    import torch
+    L = F.lib()
+    d_in = torch.ones(n, dtype=torch.int32, device="cuda")
+    out = torch.empty_like(d_in)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.flip_inclusive_scan_u32_noalloc(C.c_void_p(d_in.data_ptr()), C.c_void_p(out.data_ptr()), n, stream) == 0
+    flags = C.c_uint32(0)
+    assert L.flip_inclusive_scan_u32_noalloc_status(stream, C.byref(flags)) == 0 and flags.value == 0
+    expect = torch.arange(1, n + 1, dtype=torch.int32, device="cuda")
+    assert torch.equal(out, expect)
+    del d_in, out, expect
+    torch.cuda.empty_cache()

@@ -90,3 +90,35 @@ def zapron_race_voxels(b, g):
         v = ids[vs:ve].astype(np.int64)
         aff[vs:ve] = [(a in T) or (a + 1 in T) or (a + 8 in T) or (a + 64 in T) for a in v]
     return aff
+
+
+def native_step_errors(P, ref, nc, F):
+    """Errors of a native step run on the engine P against the FP64 oracle
+    run `ref` (oracle.nat_step of the same input) on an nc^3 grid of cell
+    1/nc.  Every quantity is measured in the norm the parity tests bound:
+      pressure_rel_err_max   max |phi - phi64| / max |phi64| (fluid cells);
+      p2g_face_rel_err       max over u, v, w of max |U - U64| / max |U64|
+                             (the face grids right after P2G);
+      proj_face_rel_err      the same for the faces after the projection, the
+                             grid velocity that G2P samples;
+      velocity_rel_err_max   max |v - v64| / max |v64| over the particles;
+      position_err_max_in_h  max |x - x64| / h."""
+    import numpy as np
+    perm = P.read(F.BUF_PERM)
+    phi = tiled_to_linear(P.read(F.BUF_PRESSURE), nc, nc, nc).astype(np.float64)
+    out = {}
+    fl = np.abs(ref["phi"]) > 0
+    out["pressure_rel_err_max"] = rel_err(phi, ref["phi"])
+    out["pressure_rel_err_l2"] = float(np.linalg.norm(phi[fl] - ref["phi"][fl]) / max(np.linalg.norm(ref["phi"][fl]), 1e-300))
+    p2g, proj = 0.0, 0.0
+    for (bp, bq, kp, kq) in ((F.BUF_GRID_U_P2G, F.BUF_GRID_U, "u", "u_proj"), (F.BUF_GRID_V_P2G, F.BUF_GRID_V, "v", "v_proj"),
+                             (F.BUF_GRID_W_P2G, F.BUF_GRID_W, "w", "w_proj")):
+        p2g = max(p2g, rel_err(tiled_to_linear(P.read(bp, np.float32), nc, nc, nc), ref[kp]))
+        proj = max(proj, rel_err(tiled_to_linear(P.read(bq, np.float32), nc, nc, nc), ref[kq]))
+    out["p2g_face_rel_err"] = p2g
+    out["proj_face_rel_err"] = proj
+    pg, vg = P.download()
+    po, vo = ref["pos"][perm], ref["vel"][perm]
+    out["velocity_rel_err_max"] = rel_err(vg, vo)
+    out["position_err_max_in_h"] = float(np.max(np.abs(pg.astype(np.float64) - po)) * nc)
+    return out
