@@ -146,27 +146,41 @@ def cpu_sample(cells, max_particles):
     return pos[m].astype(np.float64), vel[m].astype(np.float64), s
 
 
-def ref_substeps(pos, vel, cells, steps):
+# Host cost of one reference sub-step, measured on the GPU box's 16 cores:
+# 262,084 particles took 22 s a step once the fluid moves (the first step from
+# rest is about 40x cheaper, so samples warm up before they are timed).
+REF_PARTICLES_PER_STEP_SECOND = 12_000
+
+
+def ref_cpu_run(cells, steps, warm, budget_s):
+    """Time `steps` sub-steps of the reference's algorithm restated on the host
+    (oracle/flip_oracle.c orc_ref_substep: bin, tent P2G, Courant dt + red-black
+    SOR pressure loop, projection, G2P, Euler advect; FP64, OpenMP on every
+    host core) after `warm` untimed ones, on a corner sample of the workload
+    sized so that the steps take about budget_s.  Returns (particles per
+    second of a timed step, particles, seconds timed, sample description)."""
     from oracle import oracle as O
+    target = int(max(5_000, min(400_000, budget_s / max(1, steps + warm) * REF_PARTICLES_PER_STEP_SECOND)))
+    pos, vel, s = cpu_sample(cells, target)
+    n = pos.shape[0]
     g = O.grid(0.0, 0.0, 0.0, cells // 4, cells // 4, cells // 4, 4.0 / cells)
     arrs = [pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2]]
-    times = []
-    for _ in range(steps):
-        t = time.perf_counter()
+    for _ in range(warm):
         arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
-        times.append(time.perf_counter() - t)
-    return times
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
+    sec = time.perf_counter() - t0
+    sample = ("reference algorithm restated on the host (oracle/flip_oracle.c orc_ref_substep, FP64, OpenMP, %d "
+              "threads): %d particles of the workload inside [0,%.3f]^2x[0,%.3f], %d untimed then %d timed "
+              "sub-steps" % (os.cpu_count(), n, s, 2 * s, warm, steps))
+    return n * steps / sec, n, sec, sample
 
 
-def cpu_baseline(cells, budget_s=20.0):
-    pos, vel, s = cpu_sample(cells, 400_000)
-    t = ref_substeps(pos, vel, cells, 1)[0]
-    n = pos.shape[0]
-    return {"value": n / t, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
-            "sample": "reference algorithm (oracle/flip_oracle.c orc_ref_substep: bin, tent P2G, Courant dt + "
-                      "red-black SOR pressure loop, projection, G2P, Euler advect; FP64, OpenMP) for one sub-step "
-                      "of the %d particles of the workload inside [0,%.3f]^2x[0,%.3f]" % (n, s, 2 * s),
-            "seconds": t}
+def cpu_baseline(cells, budget_s=25.0):
+    value, n, sec, sample = ref_cpu_run(cells, 3, 3, budget_s)
+    return {"value": value, "unit": METRIC, "cores": os.cpu_count(), "kind": "port", "sample": sample,
+            "seconds": sec}
 
 
 # ------------------------------------------------------------ clocks
@@ -251,25 +265,9 @@ class Clocks:
 def run_reference(args, rank):
     if rank != 0:
         return
-    cells = args.cells
     steps, warm = max(1, args.steps), max(0, args.warmup)
-    # each sample step ~1 s of host work per 60k particles: keep the run within ~2 minutes
-    budget_particles = int(max(20_000, min(400_000, 110.0 / (steps + warm) * 60_000)))
-    pos, vel, s = cpu_sample(cells, budget_particles)
-    n = pos.shape[0]
-    from oracle import oracle as O
-    g = O.grid(0.0, 0.0, 0.0, cells // 4, cells // 4, cells // 4, 4.0 / cells)
-    arrs = [pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2]]
-    for _ in range(warm):
-        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        arrs, _ = O.ref_substep(*arrs, g, frame_dt=DT, elapsed=0.0)
-    sec = time.perf_counter() - t0
-    value = n * steps / sec
-    sample = ("reference algorithm restated on the host (oracle/flip_oracle.c orc_ref_substep, FP64, OpenMP, %d "
-              "threads): %d particles of the workload inside [0,%.3f]^2x[0,%.3f], one sub-step per step"
-              % (os.cpu_count(), n, s, 2 * s))
+    # the whole --steps/--warmup run on the host stays within about 2.5 minutes
+    value, n, sec, sample = ref_cpu_run(args.cells, steps, warm, 150.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
             "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",

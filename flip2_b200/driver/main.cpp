@@ -4,6 +4,12 @@
 // 24 fps with a CSV of positions after each frame.
 //
 //   flip2_main [particles] [frames] [native|reference] [outdir]
+//
+// With outdir, frame f is written as outdir/f (the reference's "x, y, z" CSV)
+// and outdir/f.bin (exact FP32 positions), and the initial x coordinates go
+// through a CudaVec<double> and its getMax: outdir/px0.f64 holds them (raw
+// doubles) and outdir/getmax.txt the device maximum of their absolute values
+// (%.17g).
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -29,14 +35,33 @@ int main(int argc, char** argv) {
         std::vector<double> px(n), py(n), pz(n), zero(n, 0.0);
         for (unsigned i = 0; i < n; ++i) { px[i] = dx(rng); py[i] = dy(rng); pz[i] = dz(rng); }
         particles.upload(px, py, pz, &zero, &zero, &zero);
+        if (!outdir.empty()) {
+            flip2::CudaVec<double> xs(n);
+            for (unsigned i = 0; i < n; ++i) xs[i] = px[i];
+            xs.upload();
+            double m = xs.getMax(nullptr, true);
+            FILE* f = std::fopen((outdir + "/getmax.txt").c_str(), "w");
+            FILE* g = std::fopen((outdir + "/px0.f64").c_str(), "wb");
+            if (!f || !g) throw flip2::Error(FLIP_ERR_ARG, "cannot write into " + outdir);
+            std::fprintf(f, "%.17g\n", m);
+            std::fwrite(px.data(), sizeof(double), n, g);
+            std::fclose(f);
+            std::fclose(g);
+        }
         particles.initialize();
-        if (!outdir.empty()) particles.writePositionsToFile(outdir + "/0");
+        if (!outdir.empty()) {
+            particles.writePositionsToFile(outdir + "/0");
+            particles.writePositionsToBinaryFile(outdir + "/0.bin");
+        }
         for (int f = 0; f < frames; ++f) {
             particles.solveFrame(24.0);
             flip_info i = particles.info();
             std::printf("frame %d: t=%.5f dt=%.3g pressure iters %d residual %.3g\n", f + 1, i.elapsed_time, i.dt,
                         i.pressure_iters, i.residual);
-            if (!outdir.empty()) particles.writePositionsToFile(outdir + "/" + std::to_string(f + 1));
+            if (!outdir.empty()) {
+                particles.writePositionsToFile(outdir + "/" + std::to_string(f + 1));
+                particles.writePositionsToBinaryFile(outdir + "/" + std::to_string(f + 1) + ".bin");
+            }
         }
     } catch (const flip2::Error& e) {
         std::fprintf(stderr, "flip2_main: %s\n", e.what());
