@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--cells", type=int, default=N_CELLS, help="voxels per axis (default 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the learned-vs-plain pressure comparison")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 64M-particle binning microbenchmark")
+    ap.add_argument("--no-c5", action="store_true", help="skip the 200-step learned-solve block")
     ap.add_argument("--config", default="c2", choices=["c2", "c5"],
                     help="c2: the 256^3 dam-break (default); c5: dam-break + sphere with the learned pressure solve")
     return ap.parse_args()
@@ -129,6 +131,125 @@ def c4_pressure(F, device):
             "speedup_learned_over_plain": mean("plain_ms") / mean("learned_ms"),
             "speedup_learned_over_no_network": mean("no_network_ms") / mean("learned_ms"),
             "fallback_rate": mean("learned_fell_back"), "problems": rows}
+
+
+# ------------------------------------------------ C5: full step, learned solve
+C5_STEPS = 200
+
+
+def c5_learned(F, torch, dev, cells, steps=C5_STEPS, warmup=3):
+    """The full step with the learned preconditioner at scale: the 256^3
+    dam-break plus a sphere of fluid (radius 0.15 at (0.5, 0.75, 0.5)), 8
+    particles per fluid voxel, FP32 state, dt 1/480, pressure by the learned
+    multilevel FCG (the network solving the 16^3 level of a V-cycle) with the
+    Jacobi-PCG restart, 200 steps, each one CUDA graph launch.  Device time
+    from CUDA events around the 200 steps; iterations and restarts from the
+    engine's device-side counters (read once, after the steps)."""
+    pos, vel = scene(cells, "c5")
+    n = pos.shape[0]
+    stream = torch.cuda.Stream(device=dev)
+    P = F.Particles(n, mode=F.MODE_NATIVE, params=F.default_params(F.MODE_NATIVE, device=dev.index, pressure_method=2),
+                    stream=stream.cuda_stream)
+    R = cells // 4
+    P.setDomain(0.0, 0.0, 0.0, R, R, R, 4.0 / cells)
+    P.lp_set_weights(np.load(os.path.join(ROOT, "flip2_b200", "data", "mg_weights.npy")))
+    P.upload(pos, vel)
+    del pos, vel
+    for _ in range(warmup):
+        P.step(DT)
+    i0 = P.info()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        P.step(DT)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    i1 = P.info()
+    P.close()
+    solves = i1.solves - i0.solves
+    return {"workload": "256^3 dam-break + fluid sphere r=0.15 at (0.5,0.75,0.5), %d particles, dt=1/480, learned "
+                        "multilevel FCG to 1e-6 with Jacobi-PCG restart, %d steps, one CUDA graph launch per step"
+                        % (n, steps),
+            "particles": n, "steps": steps, "ms_per_step": ms / steps,
+            "particle_steps_per_s": n * steps / (ms / 1e3),
+            "pressure_iters_mean": (i1.pressure_iters_total - i0.pressure_iters_total) / max(1, solves),
+            "fallback_rate": (i1.fallbacks - i0.fallbacks) / max(1, solves), "solves": solves,
+            "last_rel_residual": i1.residual, "converged": i1.converged, "error_flags": i1.error_flags,
+            "kernel_launches_per_step": (i1.launches - i0.launches) / steps}
+
+
+# ----------------------------------------------------- C3 binning microbenchmark
+C3_KEY_BITS = 28  # keys of a 512^3 domain of unit root cells are below 2^28
+
+
+def c3_binning(F, torch, dev, reps=3):
+    """The 64M-particle binning microbenchmark: positions in a 512^3 domain,
+    50% uniform and 50% from 16 Gaussian blobs (sigma 8 cells, seed 1), FP64
+    as the reference stores them.  Times the reference's own three methods
+    through the engine in reference mode -- alignParticlesToGrid (cell keys),
+    sortParticles (radix sort of the 28-bit keys with the index payload, then
+    the gather of the positions) and generateVoxels (segment heads, y-row
+    table, voxel activation, the scan of per-node counts, voxel compaction)
+    -- each rep from the unsorted input, and checks every output against the
+    SHA-256 of the reference engine's own output on the same input
+    (tests/golden/ref_c3_hashes.json, which also holds the reference's B200
+    times of the same methods)."""
+    import hashlib
+    from flip2_b200 import scenes
+    h = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_c3_hashes.json")))
+    n = h["n"]
+    pos = scenes.binning_mix(n, domain=512, seed=h["seed"]).astype(np.float64)
+    host = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    del pos
+    stream = torch.cuda.Stream(device=dev)
+    P = F.Particles(n, mode=F.MODE_REFERENCE, params=F.default_params(F.MODE_REFERENCE, device=dev.index),
+                    stream=stream.cuda_stream)
+    P.setDomain(0.0, 0.0, 0.0, 512, 512, 512, 1.0)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    times = {"align": [], "sort": [], "voxels": []}
+    checks = None
+    for r in range(reps + 1):
+        P.upload(tuple(host), None)
+        P.sync()
+        ev[0].record(stream)
+        P.alignParticlesToGrid()
+        ev[1].record(stream)
+        P.sortParticles()
+        ev[2].record(stream)
+        P.generateVoxels()
+        ev[3].record(stream)
+        torch.cuda.synchronize(dev)
+        if r == 0:  # the first pass also sizes the voxel buffers; check its outputs
+            sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+            info = P.info()
+            checks = {"nodes": info.nodes == h["nodes"], "voxels": info.voxels == h["voxels"],
+                      "keys": sha(P.read(F.BUF_KEYS)) == h["sha256_keys"],
+                      "perm": sha(P.read(F.BUF_PERM)) == h["sha256_perm"],
+                      "flags": sha(P.read(F.BUF_FLAGS)) == h["sha256_flags"],
+                      "starts": sha(P.read(F.BUF_STARTS)) == h["sha256_starts"],
+                      "node_voxels": sha(P.read(F.BUF_NODE_VOXELS)) == h["sha256_node_voxels"],
+                      "voxel_ids": sha(P.read(F.BUF_VOXEL_IDS)) == h["sha256_voxel_ids"],
+                      "solids": sha(P.read(F.BUF_SOLIDS)) == h["sha256_solids"]}
+            continue
+        times["align"].append(ev[0].elapsed_time(ev[1]))
+        times["sort"].append(ev[1].elapsed_time(ev[2]))
+        times["voxels"].append(ev[2].elapsed_time(ev[3]))
+    P.close()
+    ms = {k: statistics.median(v) for k, v in times.items()}
+    ref_ms = {k: 1e3 * v for k, v in h["seconds"].items()}
+    # algorithmic bytes: keys 24 B (FP64 x, y, z) + 4 B out; sort 4 B histogram +
+    # 4 passes x 16 B (28-bit keys, 8-bit digits) + the gather of x, y, z by the
+    # permutation (4 + 24 + 24 B)
+    key_bytes, sort_bytes = 28.0 * n, (4 + 4 * 16 + 52) * n
+    return {"workload": "64M particles (%d) in a 512^3 domain, 50%% uniform + 50%% in 16 Gaussian blobs (sigma 8, "
+                        "seed %d), FP64 positions, 28-bit keys + index payload" % (n, h["seed"]),
+            "ms": ms, "reference_b200_ms": ref_ms,
+            "speedup_vs_reference_b200": {k: ref_ms[k] / ms[k] for k in ms},
+            "keys_gbs": key_bytes / (ms["align"] / 1e3) / 1e9,
+            "sort_gbs": sort_bytes / (ms["sort"] / 1e3) / 1e9,
+            "sort_algorithmic_bytes": "120 B per key: histogram 4 + 4 onesweep passes x 16 + gather of x,y,z 52",
+            "hash_check": checks, "bit_exact": bool(checks) and all(checks.values()), "reps": reps}
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -363,20 +484,19 @@ def main():
     barrier()
     torch.cuda.synchronize(dev)
     clocks.begin()
+    fb0 = P.info().fallbacks
     ev0.record(stream)
-    fell_back = 0
     for _ in range(args.steps):
         P.step(DT)
-        if c5:
-            fell_back += P.solve_info().fell_back
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     clocks.end()
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    launches = P.info().launches - l0
     info = P.info()
+    launches = info.launches - l0
+    fell_back = info.fallbacks - fb0
     ms_max = max_over_ranks(ms)
     value = n * world * args.steps / (ms_max / 1e3)
 
@@ -449,6 +569,12 @@ def main():
     c4 = None
     if rank == 0 and world == 1 and not args.no_c4 and not c5:
         c4 = c4_pressure(F, local)
+    c3 = None
+    if rank == 0 and world == 1 and not args.no_c3 and not c5:
+        c3 = c3_binning(F, torch, dev)
+    c5_block = None
+    if rank == 0 and world == 1 and not args.no_c5 and not c5:
+        c5_block = c5_learned(F, torch, dev, args.cells)
     if rank == 0:
         workload = WORKLOAD
         if c5:
@@ -461,7 +587,7 @@ def main():
                 "config": {"workload": workload, "particles": n, "grid": "%d^3" % args.cells, "dt": DT,
                            "parallelism": "replicas x%d" % world,
                            "l2": "inputs larger than L2: %.0f MB particle state per replica" % (24 * n / 1e6)},
-                "particle_stages": particle_stages, "c4_pressure": c4,
+                "particle_stages": particle_stages, "c4_pressure": c4, "c3_binning": c3, "c5_learned": c5_block,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
                 "pcg_iters_per_step": iters, "pressure_solve_ms": stages["pcg_setup"] + stages["pcg_iterations"],
                 "stages_ms": stages, "fluid_tiles": fluid_tiles,

@@ -13,6 +13,7 @@ enum : uint32_t {
     DEVERR_LOOKBACK_TIMEOUT = 1u << 0,  // a decoupled look-back wait gave up
     DEVERR_TILE_OVERFLOW = 1u << 1,     // more particles in a tile than staged
     DEVERR_BAD_KEY = 1u << 2,           // a key outside the declared key range
+    DEVERR_TMA_TIMEOUT = 1u << 3,       // a TMA copy's mbarrier wait gave up
 };
 
 // Upper bound on polls of a look-back status word before giving up.  The

@@ -69,6 +69,32 @@ struct flip_engine {
     float* fp[6] = {};
     float* fq[6] = {};
     float *m[3] = {}, *w[3] = {}, *o[3] = {};
+    // x-fastest copies of the projected (ulin) and P2G (olin) face velocities:
+    // the grids G2P stages by TMA, through the descriptors in g2p_maps
+    float *ulin[3] = {}, *olin[3] = {};
+    NatG2PMaps g2p_maps{};
+    PcgMaps pcg_maps{};  // TMA descriptors of the Jacobi-PCG vectors (pcg_tma.cu)
+    // keys[p] holds the tile key of particle p's current position (G2P writes
+    // them for the next step; uploads invalidate them)
+    bool keys_valid = false;
+    uint32_t* head_dense = nullptr;  // first particle of each tile key (segment heads of the native binning)
+    // captured steps and frames (native mode): the device keeps the solve's
+    // outcome (d_rec) and the sub-step control (d_frame); step_graph and
+    // frame_graph are rebuilt when the domain, the solids or the solve
+    // configuration change
+    SolveRecord* d_rec = nullptr;
+    FrameState* d_frame = nullptr;
+    SolveRecord* h_rec = nullptr;        // pinned readback of d_rec
+    FrameState* h_frame = nullptr;       // pinned readback of d_frame
+    bool rec_pending = false;            // d_rec is newer than the host's copy of the last solve
+    uint64_t rec_chunks_counted[2] = {0, 0};
+    uint64_t rec_fallbacks_counted = 0;
+    cudaGraphExec_t step_graph = nullptr, frame_graph = nullptr;
+    uint32_t step_graph_launches = 0;   // kernels of one captured step outside its loops
+    float* cap_fp0 = nullptr;           // fp[0] when the graphs were captured (eager steps swap fp and fq)
+    static constexpr int kCapStreams = 4;
+    cudaStream_t cap_streams[kCapStreams] = {};
+    int cap_depth = 0;
     uint8_t *type = nullptr, *solid_tiled = nullptr, *tile_flags = nullptr;
     bool has_solid = false;
     float usolid[3] = {0.0f, 0.0f, 0.0f};  // velocity of the interior solid cells (native)
@@ -181,8 +207,10 @@ static int dev_err_eval(flip_engine* e) {
     e->h_small[4] = 0;
     e->err_seen |= w;
     E_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream));
-    return e->fail(FLIP_ERR_TIMEOUT, "a decoupled look-back wait of the sort or scan timed out; the binning of this "
-                                     "step is invalid");
+    return e->fail(FLIP_ERR_TIMEOUT, (w & DEVERR_TMA_TIMEOUT)
+                                         ? "a TMA copy of G2P timed out; the particles of this step are invalid"
+                                         : "a decoupled look-back wait of the sort or scan timed out; the binning of "
+                                           "this step is invalid");
 }
 static int dev_err_check(flip_engine* e) {
     E_TRY(dev_err_fetch(e));
@@ -239,6 +267,8 @@ extern "C" int flip_create(uint64_t n, const flip_params* params, void* stream, 
     rc = e->cuda(cudaMallocHost((void**)&e->h_small, 4096), "cudaMallocHost");
     if (rc) { flip_destroy(e); return rc; }
     rc = e->cuda(cudaMallocHost((void**)&e->h_state, sizeof(PcgState)), "cudaMallocHost");
+    e->h_rec = reinterpret_cast<SolveRecord*>(reinterpret_cast<char*>(e->h_small) + 256);
+    e->h_frame = reinterpret_cast<FrameState*>(reinterpret_cast<char*>(e->h_small) + 512);
     if (rc) { flip_destroy(e); return rc; }
     for (auto& v : e->solve_ev) {
         rc = e->cuda(cudaEventCreate(&v), "cudaEventCreate");
@@ -269,7 +299,12 @@ static void free_mg(flip_engine* e) {
     e->mg_arena = nullptr;
     e->mg = MgHierarchy{};
 }
+static void free_step_graphs(flip_engine* e) {
+    if (e->step_graph) { cudaGraphExecDestroy(e->step_graph); e->step_graph = nullptr; }
+    if (e->frame_graph) { cudaGraphExecDestroy(e->frame_graph); e->frame_graph = nullptr; }
+}
 static void free_arena(flip_engine* e) {
+    free_step_graphs(e);
     free_mg(e);
     free_lp_activations(e);
     e->poisson_ready = false;
@@ -344,6 +379,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         if (e->nslots >= (1ull << 32)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: grid above 2^32 voxels");
         e->key_bits = bits_for(e->ntiles_total - 1);
         add((void**)&e->node_keys, 4 * e->ntiles_total);  // occupied tiles, or fluid tiles of a pressure problem
+        add((void**)&e->head_dense, 4 * e->ntiles_total);
         add((void**)&e->gen_sph, sizeof(float4) * kGenMaxSpheres);
         add((void**)&e->gen_imp, sizeof(float) * 7 * kGenMaxImpulses);
         for (int a = 0; a < 6; ++a) { add((void**)&e->fp[a], 4 * n); add((void**)&e->fq[a], 4 * n); }
@@ -351,6 +387,8 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
             add((void**)&e->m[c], 4 * e->nslots);
             add((void**)&e->w[c], 4 * e->nslots);
             add((void**)&e->o[c], 4 * e->nslots);
+            add((void**)&e->ulin[c], 4 * e->nslots);
+            add((void**)&e->olin[c], 4 * e->nslots);
         }
         add((void**)&e->type, e->nslots);
         add((void**)&e->tile_flags, e->ntiles_total);
@@ -362,6 +400,8 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         add((void**)&e->cell_prev, e->nslots);
         add((void**)&e->pcg.tcoord, 4 * e->ntiles_total);
         add((void**)&e->pcg.st, sizeof(PcgState));
+        add((void**)&e->d_rec, sizeof(SolveRecord));
+        add((void**)&e->d_frame, sizeof(FrameState));
         add((void**)&e->pcg.partials, sizeof(double) * 4 * kPcgBlocks);
     }
     size_t total = 0;
@@ -377,7 +417,11 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         // zero everything once so that stale tiles read as zero
         E_CUDA(cudaMemsetAsync(e->arena, 0, total, e->stream));
         E_CUDA(cudaStreamSynchronize(e->stream));
+        E_TRY(nat_make_g2p_maps(e->g2p_maps, e->ulin, e->olin, e->D));
+        E_TRY(nat_make_pcg_maps(e->pcg_maps, e->pcg, e->ntiles_total));
+        e->pcg.warm_ok = &e->d_rec->warm_ok;
     }
+    e->keys_valid = false;
     return FLIP_OK;
 }
 
@@ -407,6 +451,7 @@ extern "C" int flip_upload_particles_f64(flip_engine* e, const double* px, const
         }
     }
     e->binned = e->have_voxels = false;
+    e->keys_valid = false;
     return FLIP_OK;
 }
 
@@ -435,6 +480,7 @@ extern "C" int flip_upload_particles_f32(flip_engine* e, const float* px, const 
         }
     }
     e->binned = e->have_voxels = false;
+    e->keys_valid = false;
     return FLIP_OK;
 }
 
@@ -488,9 +534,12 @@ extern "C" int flip_set_solid_velocity(flip_engine* e, double ux, double uy, dou
     if (!e) return FLIP_ERR_ARG;
     if (!std::isfinite(ux) || !std::isfinite(uy) || !std::isfinite(uz))
         return e->fail(FLIP_ERR_ARG, "flip_set_solid_velocity: non-finite velocity");
+    E_TRY(rt_join(e));
+    if (e->stream) E_CUDA(cudaStreamSynchronize(e->stream));  // a captured launch in flight uses the old value
     e->usolid[0] = (float)ux;
     e->usolid[1] = (float)uy;
     e->usolid[2] = (float)uz;
+    free_step_graphs(e);  // the captured steps hold the velocity as a kernel argument
     return FLIP_OK;
 }
 
@@ -509,6 +558,7 @@ extern "C" int flip_set_solid_mask(flip_engine* e, const uint8_t* mask_host, uin
     cudaFree(lin);
     if (rc) return rc;
     e->has_solid = true;
+    free_step_graphs(e);
     return FLIP_OK;
 }
 
@@ -702,7 +752,11 @@ static int nat_grid(flip_engine* e, int per_sm) { return e->sms * per_sm; }
 
 static int nat_bin(flip_engine* e) {
     E_TRY(e->mark(0));
-    E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
+    if (!e->keys_valid) {  // else the last G2P wrote them
+        E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
+        e->launches += 1;
+        e->keys_valid = true;
+    }
     E_TRY(e->mark(1));
     E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
                         e->stream, e->d_err, kSpinLimit, 0));
@@ -710,14 +764,10 @@ static int nat_bin(flip_engine* e) {
     E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
     for (int a = 0; a < 6; ++a) std::swap(e->fp[a], e->fq[a]);
     E_TRY(e->mark(3));
-    if (e->n == 0) {
-        E_CUDA(cudaMemsetAsync(e->d_counts, 0, sizeof(uint32_t), e->stream));
-    } else {
-        E_TRY(launch_scan(1, e->keys, nullptr, e->n, e->scan_scratch, e->scan_scratch_bytes, e->stream, e->starts,
-                          e->node_keys, e->d_counts, e->d_err, kSpinLimit, 0));
-    }
+    E_TRY(nat_launch_segment_heads(e->keys, e->n, (uint32_t)e->ntiles_total, e->head_dense, e->node_keys, e->starts,
+                                   e->d_counts, nat_grid(e, 8), e->stream));
     E_TRY(e->mark(4));
-    e->launches += 1 + 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 1;
+    e->launches += 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 2;
     e->binned = true;
     return FLIP_OK;
 }
@@ -746,7 +796,8 @@ static int nat_p2g_stage(flip_engine* e, double dt) {
     E_TRY(e->mark(7));
     E_TRY(nat_launch_normalize(e->grid_tiles, e->d_counts + 1, e->D, (float)(e->P.gravity_y * dt), e->m,
                                (const float* const*)e->w, e->o, e->type,
-                               make_float3(e->usolid[0], e->usolid[1], e->usolid[2]), nat_grid(e, 4), e->stream));
+                               make_float3(e->usolid[0], e->usolid[1], e->usolid[2]), nat_grid(e, 4), e->stream, e->ulin,
+                               e->olin));
     E_TRY(e->mark(8));
     e->launches += 1 + (e->has_solid ? 1 : 0) + 3 + 1;
     e->have_voxels = true;
@@ -803,8 +854,9 @@ static int nat_pcg_graph(flip_engine* e, int iters, int max_iter) {
     E_TRY(build_loop_graph(e, [&]() {
         int rc = FLIP_OK;
         for (int k = 0; k < iters && rc == FLIP_OK; ++k)
-            rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-        if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            rc = nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err,
+                                           nat_grid(e, 4), e->stream);
+        if (rc == FLIP_OK) rc = nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
         return rc;
     }, limit, &e->pcg_graph));
     e->pcg_graph_iters = iters;
@@ -1137,6 +1189,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(e->mark(9));
         E_TRY(nat_mgpcg_graph(e, chunk, max_learned, network));
         E_TRY(run_loop(e, e->mg_graph, (2u + mg_cycle_launches(e, network, true)) * (uint32_t)chunk + 1u));
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
@@ -1163,6 +1216,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(e->mark(9));
         E_TRY(nat_fpcg_graph(e, chunk, max_learned));
         E_TRY(run_loop(e, e->fpcg_graph, 7u * (uint32_t)chunk + 1u));
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
@@ -1176,12 +1230,13 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         pcg_state_host(e, tol, max_plain, 0);
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
         const bool w = warm && method == 0;
-        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
-                                  w ? e->cell_prev : nullptr));
+        E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU,
+                                   e->type, e->pcg, e->stream, w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
         if (method == 0) E_TRY(e->mark(9));
         E_TRY(nat_pcg_graph(e, chunk, max_plain));
         E_TRY(run_loop(e, e->pcg_graph, 2u * (uint32_t)chunk + 1u));
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 0, method == 0 ? 0 : 1, e->stream));
         const PcgState& s = *e->h_state;
         if (method != 0) info.plain_iters = s.iter;
         else info.iters = s.iter;
@@ -1217,14 +1272,37 @@ static int nat_pressure(flip_engine* e) {
     return FLIP_OK;
 }
 
+static int nat_project_stage(flip_engine* e) {
+    return nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->pcg.xg, e->type, e->m, nat_grid(e, 4),
+                              e->stream, e->ulin);
+}
+// G2P + advection on the tiles of this step's binning; also writes the tile
+// key of every new position for the next step's sort
+// in and out: the particle state G2P reads (the binning's gathered order)
+// and writes; nullptrs mean fp in place.  dt_p: dt from the device.
+static int nat_g2p_stage(flip_engine* e, double dt, float* const* in = nullptr, float* const* out = nullptr,
+                         const float* dt_p = nullptr) {
+    float* const* I = in ? in : e->fp;
+    float* const* Q = out ? out : e->fp;
+    E_TRY(nat_launch_g2p(e->g2p_maps, e->node_keys, e->starts, e->d_counts, e->n, e->D, (float)dt, e->P.flip_ratio,
+                         (const float* const*)e->m, (const float* const*)e->o, (const float* const*)I,
+                         (const float* const*)(I + 3), Q, Q + 3, e->keys, e->has_solid ? e->type : nullptr,
+                         make_float3(e->usolid[0], e->usolid[1], e->usolid[2]), dt_p, e->d_err, nat_grid(e, 4),
+                         e->stream));
+    e->keys_valid = true;
+    e->binned = false;
+    return FLIP_OK;
+}
+
+static int rec_refresh(flip_engine* e);
 static int nat_step(flip_engine* e, double dt) {
+    E_TRY(rec_refresh(e));  // the warm-start flag of a captured step before this one
     E_TRY(nat_bin(e));
     E_TRY(nat_p2g_stage(e, dt));
     E_TRY(nat_pressure(e));
-    E_TRY(nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->pcg.xg, e->type, e->m, nat_grid(e, 4), e->stream));
+    E_TRY(nat_project_stage(e));
     E_TRY(e->mark(11));
-    E_TRY(nat_launch_g2p(e->n, e->D, (float)dt, e->P.flip_ratio, (const float* const*)e->m, (const float* const*)e->o,
-                         e->fp, e->fp + 3, e->stream));
+    E_TRY(nat_g2p_stage(e, dt));
     E_TRY(e->mark(12));
     e->launches += 2;
     if (e->timing) {
@@ -1241,6 +1319,312 @@ static int nat_step(flip_engine* e, double dt) {
     return FLIP_OK;
 }
 
+// ==================================================== captured steps
+// A native step, or a whole native frame, as one CUDA graph.  The host
+// launches it and reads nothing back: the solve's outcome stays in d_rec
+// (read when the caller asks), the warm start follows the device flag
+// d_rec->warm_ok, dt and gravity * dt come from d_frame, and conditional
+// nodes carry every data-dependent branch -- the solve's iteration loop
+// (WHILE), the Jacobi-PCG restart of a flexible solve that missed tol (IF),
+// and, for a frame, the loop over Courant-limited sub-steps (WHILE).
+// Conditional nodes are added while the stream is being captured; their
+// bodies are captured on side streams.
+//
+// In a captured step the gather writes the sorted state into fq and G2P
+// writes the new state back into fp, so that the state always sits in fp
+// between launches (the eager path swaps fp and fq instead).
+
+// a conditional handle of the graph being captured on e->stream
+static int cap_handle(flip_engine* e, unsigned int dflt, cudaGraphConditionalHandle* h) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    E_CUDA(cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &g, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive) return e->fail(FLIP_ERR_STATE, "conditional handle outside a capture");
+    E_CUDA(cudaGraphConditionalHandleCreate(h, g, dflt, cudaGraphCondAssignDefault));
+    return FLIP_OK;
+}
+// add a conditional node on handle h at the capture point of e->stream.  A
+// handle's default applies at graph launch only, so a node inside another
+// loop's body has its condition set by a kernel before it (cap_loop does).
+static int cap_cond_node(flip_engine* e, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h,
+                         cudaGraph_t* body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    E_CUDA(cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return e->fail(FLIP_ERR_STATE, "conditional node outside a capture");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    E_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    E_CUDA(cudaStreamUpdateCaptureDependencies(e->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    return FLIP_OK;
+}
+// capture fn() into a conditional body on the next side stream (e->stream
+// points at that stream meanwhile, so the launchers record into the body)
+template <class Fn>
+static int cap_body(flip_engine* e, cudaGraph_t body, Fn fn) {
+    if (e->cap_depth >= flip_engine::kCapStreams) return e->fail(FLIP_ERR_STATE, "conditional nodes nested too deep");
+    cudaStream_t& side = e->cap_streams[e->cap_depth];
+    if (!side) E_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    E_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    cudaStream_t outer = e->stream;
+    e->stream = side;
+    e->cap_depth++;
+    int rc = fn();
+    e->cap_depth--;
+    e->stream = outer;
+    cudaGraph_t done = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(side, &done);
+    if (rc != FLIP_OK) return rc;
+    E_CUDA(ce);
+    return FLIP_OK;
+}
+// a WHILE loop of chunks: body() then the loop control kernel; the
+// condition is set to 1 by a kernel before the node, so the loop also runs
+// when it sits inside another loop's body
+template <class Fn>
+static int cap_loop(flip_engine* e, int limit, Fn body) {
+    cudaGraphConditionalHandle h;
+    cudaGraph_t g = nullptr;
+    E_TRY(cap_handle(e, 1u, &h));
+    E_TRY(nat_launch_cond_set(h, 1u, e->stream));
+    E_TRY(cap_cond_node(e, cudaGraphCondTypeWhile, h, &g));
+    return cap_body(e, g, [&]() {
+        E_TRY(body());
+        return nat_launch_loop_ctl(h, e->pcg.st, limit, e->stream);
+    });
+}
+static int cap_plain_chunk(flip_engine* e, int chunk) {
+    for (int k = 0; k < chunk; ++k)
+        E_TRY(nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err, nat_grid(e, 4),
+                                        e->stream));
+    return nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+}
+static int cap_mg_chunk(flip_engine* e, int chunk, bool network) {
+    const int* halt = &e->pcg.st->halt;
+    for (int k = 0; k < chunk; ++k) {
+        E_TRY(nat_launch_fpcg_direction_update(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        if (k == chunk - 1) E_TRY(nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_TRY(mg_cycle(e, network, halt, 0));
+    }
+    return FLIP_OK;
+}
+// Jacobi-PCG from a fresh state: b from U (nullptr: already in pcg.b),
+// warm: from the previous solution where the device flag allows
+static int cap_plain_solve(flip_engine* e, const float* const* U, bool warm, int stage) {
+    const int chunk = e->P.pcg_check_every;
+    const float* const nullU[3] = {nullptr, nullptr, nullptr};
+    E_TRY(nat_launch_state_init(e->pcg.st, e->P.pcg_tol, e->P.pcg_max_iter, e->P.true_residual_every, 0, e->stream));
+    E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU, e->type,
+                               e->pcg, e->stream, warm ? e->cell_prev : nullptr));
+    E_TRY(cap_loop(e, loop_limit(e->P.pcg_max_iter, chunk), [&]() { return cap_plain_chunk(e, chunk); }));
+    return nat_launch_solve_record(e->d_rec, e->pcg.st, 0, stage, e->stream);
+}
+// the pressure solve of a captured step (pressure_method 0 or 2)
+static int cap_solve(flip_engine* e) {
+    const float* const* U = (const float* const*)e->m;
+    const bool warm = e->P.pcg_warm_start != 0;
+    if (e->P.pressure_method == 0) return cap_plain_solve(e, U, warm, 0);
+    const int chunk = e->P.pcg_check_every;
+    const int max_learned = e->P.learned_max_iter > 0 ? e->P.learned_max_iter : e->P.pcg_max_iter;
+    const bool network = e->P.mg_coarse == 0;
+    E_TRY(nat_launch_state_init(e->pcg.st, e->P.pcg_tol, max_learned, chunk, 1, e->stream));
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U, e->type, e->pcg, e->stream,
+                              warm ? e->cell_prev : nullptr));
+    E_TRY(mg_setup_problem(e, network));
+    E_TRY(mg_cycle(e, network, &e->pcg.st->halt, 1));
+    E_TRY(cap_loop(e, loop_limit(max_learned, chunk), [&]() { return cap_mg_chunk(e, chunk, network); }));
+    E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
+    // the flexible solve missed tol: Jacobi-PCG restarts from x = 0 on the same b
+    cudaGraphConditionalHandle h;
+    cudaGraph_t g = nullptr;
+    E_TRY(cap_handle(e, 0u, &h));
+    E_TRY(nat_launch_fallback_cond(h, e->pcg.st, e->stream));
+    E_TRY(cap_cond_node(e, cudaGraphCondTypeIf, h, &g));
+    return cap_body(e, g, [&]() { return cap_plain_solve(e, nullptr, false, 1); });
+}
+
+static int cap_step(flip_engine* e) {
+    const float* dtp = &e->d_frame->dt;
+    const float* gdtp = &e->d_frame->gdt;
+    // binning (the keys come from the previous G2P or from the launch)
+    E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
+                        e->stream, e->d_err, kSpinLimit, 0));
+    E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
+    E_TRY(nat_launch_segment_heads(e->keys, e->n, (uint32_t)e->ntiles_total, e->head_dense, e->node_keys, e->starts,
+                                   e->d_counts, nat_grid(e, 8), e->stream));
+    // P2G and the face grids
+    const size_t fb = 4 * e->nslots;
+    for (int c = 0; c < 3; ++c) {
+        E_CUDA(cudaMemsetAsync(e->m[c], 0, fb, e->stream));
+        E_CUDA(cudaMemsetAsync(e->w[c], 0, fb, e->stream));
+    }
+    E_CUDA(cudaMemsetAsync(e->type, 0, e->nslots, e->stream));
+    if (e->P.pcg_warm_start)
+        E_CUDA(cudaMemcpyAsync(e->cell_prev, e->pcg.cell, e->nslots, cudaMemcpyDeviceToDevice, e->stream));
+    E_CUDA(cudaMemsetAsync(e->pcg.cell, 0, e->nslots, e->stream));
+    E_CUDA(cudaMemsetAsync(e->tile_flags, 0, e->ntiles_total, e->stream));
+    E_TRY(nat_launch_p2g(e->node_keys, e->starts, e->d_counts, e->n, (const float* const*)e->fq,
+                         (const float* const*)(e->fq + 3), e->D, e->m, e->w, e->type, nat_grid(e, 8), e->stream));
+    if (e->has_solid) E_TRY(nat_launch_apply_solids(e->solid_tiled, e->type, e->nslots, e->stream));
+    E_TRY(nat_launch_dilate_compact(e->node_keys, e->d_counts, e->D, e->tile_flags, e->grid_tiles, e->d_counts + 1,
+                                    nat_grid(e, 2), e->stream));
+    E_TRY(nat_launch_tile_coords(e->node_keys, e->d_counts, e->D, e->pcg.tcoord, nat_grid(e, 2), e->stream));
+    E_TRY(nat_launch_normalize(e->grid_tiles, e->d_counts + 1, e->D, 0.0f, e->m, (const float* const*)e->w, e->o,
+                               e->type, make_float3(e->usolid[0], e->usolid[1], e->usolid[2]), nat_grid(e, 4),
+                               e->stream, e->ulin, e->olin, gdtp));
+    E_TRY(cap_solve(e));
+    E_TRY(nat_project_stage(e));
+    return nat_g2p_stage(e, 0.0, e->fq, e->fp, dtp);
+}
+// kernels of one captured step outside its loops and its restart branch
+static uint32_t cap_step_launches(flip_engine* e) {
+    uint32_t k = 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 2;  // sort, gather, heads
+    k += 1 + (e->has_solid ? 1 : 0) + 3 + 1;                       // P2G .. normalise
+    k += 2 + (e->P.pcg_warm_start ? 1 : 0) + 1 + 1;                // state, init (+ warm), loop condition, record
+    if (e->P.pressure_method == 2) {
+        const bool network = e->P.mg_coarse == 0;
+        k += 2u * (uint32_t)(e->mg.levels - 1) + 2u * (uint32_t)std::max(0, e->mg.levels - 2) + (network ? 4u : 0u);
+        k += mg_cycle_launches(e, network, true) + 1;              // first V-cycle, fallback condition
+    }
+    return k + 2;                                                  // projection, G2P
+}
+
+// builds e->step_graph, or e->frame_graph (frame: a WHILE over sub-steps,
+// each taking its dt from the device-side Courant rule)
+static int cap_build(flip_engine* e, bool frame) {
+    if (e->P.pressure_method == 2) E_TRY(mg_ready(e, e->P.mg_coarse == 0));
+    const uint32_t launches = e->launches;  // the launchers count at capture time: restored below
+    cudaGraph_t g = nullptr;
+    E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
+    int rc = FLIP_OK;
+    if (!frame) {
+        rc = cap_step(e);
+    } else {
+        cudaGraphConditionalHandle h;
+        cudaGraph_t body = nullptr;
+        rc = cap_handle(e, 1u, &h);
+        if (rc == FLIP_OK) rc = cap_cond_node(e, cudaGraphCondTypeWhile, h, &body);
+        if (rc == FLIP_OK)
+            rc = cap_body(e, body, [&]() {
+                E_TRY(nat_launch_vmax(e->n, (const float* const*)(e->fp + 3), e->d_counts + 2, nat_grid(e, 4), e->stream));
+                E_TRY(nat_launch_frame_ctl(h, e->d_frame, e->d_counts + 2, e->P.gravity_y, e->stream));
+                return cap_step(e);
+            });
+    }
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    e->launches = launches;
+    if (rc != FLIP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    E_CUDA(ce);
+    e->cap_fp0 = e->fp[0];
+    cudaGraphExec_t* out = frame ? &e->frame_graph : &e->step_graph;
+    ce = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    E_CUDA(ce);
+    e->step_graph_launches = cap_step_launches(e);
+    return FLIP_OK;
+}
+static bool cap_supported(flip_engine* e) {
+    return e->P.mode == FLIP_MODE_NATIVE && !e->timing && (e->P.pressure_method == 0 || e->P.pressure_method == 2) &&
+           e->n > 0;
+}
+// before a captured launch: the keys of the current positions, if the last
+// G2P did not write them
+static int cap_keys(flip_engine* e) {
+    if (e->keys_valid) return FLIP_OK;
+    E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
+    e->launches += 1;
+    e->keys_valid = true;
+    return FLIP_OK;
+}
+static int cap_launched(flip_engine* e, uint32_t steps) {
+    e->launches += steps * e->step_graph_launches;
+    e->rec_pending = true;
+    e->binned = false;
+    e->have_voxels = true;
+    e->poisson_ready = true;
+    e->xstar_ready = false;
+    e->solution_fresh = false;
+    return FLIP_OK;
+}
+// one step as a graph launch (no host round trip)
+static int cap_step_launch(flip_engine* e, double dt) {
+    if (e->fp[0] != e->cap_fp0) free_step_graphs(e);
+    if (!e->step_graph) E_TRY(cap_build(e, false));
+    E_TRY(cap_keys(e));
+    E_TRY(nat_launch_step_dt(e->d_frame, dt, e->P.gravity_y, e->stream));
+    E_CUDA(cudaGraphLaunch(e->step_graph, e->stream));
+    e->launches += 1;
+    E_TRY(cap_launched(e, 1));
+    e->dt = dt;
+    e->elapsed += dt;
+    return FLIP_OK;
+}
+// the host's copy of the last solve from d_rec (synchronises); also counts
+// the loop kernels the captured launches ran
+static int rec_refresh(flip_engine* e) {
+    if (!e->rec_pending) return FLIP_OK;
+    E_CUDA(cudaMemcpyAsync(e->h_rec, e->d_rec, sizeof(SolveRecord), cudaMemcpyDeviceToHost, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    const SolveRecord r = *e->h_rec;
+    flip_solve_info info{};
+    info.iters = r.iters;
+    info.plain_iters = r.plain_iters;
+    info.converged = r.converged;
+    info.fell_back = r.fell_back;
+    info.rel_residual = r.rel_residual;
+    e->last_solve = info;
+    e->last_iters = r.iters + r.plain_iters;
+    e->last_converged = r.converged;
+    e->last_rel = r.rel_residual;
+    e->warm_ok = r.warm_ok != 0;
+    e->solution_fresh = r.converged != 0;
+    const int chunk = e->P.pcg_check_every;
+    const uint32_t per_plain = 2u * (uint32_t)chunk + 2u;
+    uint32_t per_primary = per_plain;
+    if (e->P.pressure_method == 2) per_primary = (2u + mg_cycle_launches(e, e->P.mg_coarse == 0, true)) * (uint32_t)chunk + 2u;
+    e->launches += (uint32_t)((r.chunks_primary - e->rec_chunks_counted[0]) * per_primary +
+                              (r.chunks_plain - e->rec_chunks_counted[1]) * per_plain);
+    // a restart runs the state, init, loop-condition and record kernels of its branch
+    e->launches += (uint32_t)(4u * (r.fallbacks - e->rec_fallbacks_counted));
+    e->rec_chunks_counted[0] = r.chunks_primary;
+    e->rec_chunks_counted[1] = r.chunks_plain;
+    e->rec_fallbacks_counted = r.fallbacks;
+    e->rec_pending = false;
+    return FLIP_OK;
+}
+
+// a whole frame as one graph launch: the device takes sub-steps of
+// min(max_substep_dt, 0.7 h / max |v component|, the rest of the frame)
+static int cap_frame_launch(flip_engine* e, double frame_dt) {
+    if (e->fp[0] != e->cap_fp0) free_step_graphs(e);
+    if (!e->frame_graph) E_TRY(cap_build(e, true));
+    E_TRY(cap_keys(e));
+    E_TRY(nat_launch_frame_init(e->d_frame, frame_dt, e->P.max_substep_dt, (double)e->D.h, e->stream));
+    E_CUDA(cudaGraphLaunch(e->frame_graph, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->h_frame, e->d_frame, sizeof(FrameState), cudaMemcpyDeviceToHost, e->stream));
+    E_TRY(dev_err_fetch(e));
+    E_CUDA(cudaStreamSynchronize(e->stream));
+    const FrameState f = *e->h_frame;
+    e->launches += 2;  // frame init, graph
+    E_TRY(cap_launched(e, (uint32_t)f.substeps));
+    e->launches += 2u * (uint32_t)f.substeps;  // the speed reduction and the sub-step control
+    E_TRY(dev_err_eval(e));
+    if (f.error) return e->fail(FLIP_ERR_STATE, "solveFrame: dt collapsed");
+    e->dt = f.dt;
+    e->elapsed += f.t;
+    return FLIP_OK;
+}
+
 // ============================================================ public API
 #define CHECK_E()                                                             \
     do {                                                                      \
@@ -1254,7 +1638,9 @@ static int nat_step(flip_engine* e, double dt) {
 extern "C" int flip_align_particles_to_grid(flip_engine* e) {
     CHECK_E();
     if (e->P.mode == FLIP_MODE_REFERENCE) return ref_align(e);
-    return nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream);
+    E_TRY(nat_launch_keys(e->fp[0], e->fp[1], e->fp[2], e->n, e->D, e->keys, e->stream));
+    e->keys_valid = true;
+    return FLIP_OK;
 }
 extern "C" int flip_sort_particles(flip_engine* e) {
     CHECK_E();
@@ -1282,14 +1668,15 @@ extern "C" int flip_pressure_solve(flip_engine* e) {
 extern "C" int flip_update_voxel_velocities(flip_engine* e) {
     CHECK_E();
     if (e->P.mode == FLIP_MODE_REFERENCE) return ref_update_vel(e);
-    return nat_launch_project(e->grid_tiles, e->d_counts + 1, e->D, e->pcg.x, e->pcg.xg, e->type, e->m, nat_grid(e, 4), e->stream);
+    return nat_project_stage(e);
 }
 extern "C" int flip_voxel_vels_to_particles(flip_engine* e) {
     CHECK_E();
     if (e->P.mode == FLIP_MODE_REFERENCE) return ref_g2p_stage(e);
-    // native G2P moves the particles as well (advection is fused)
-    return nat_launch_g2p(e->n, e->D, (float)e->P.max_substep_dt, e->P.flip_ratio, (const float* const*)e->m,
-                          (const float* const*)e->o, e->fp, e->fp + 3, e->stream);
+    // native G2P moves the particles as well (advection is fused); it works
+    // on the tiles of the current binning
+    if (!e->have_voxels) return e->fail(FLIP_ERR_STATE, "voxelVelsToParticles before particleVelToVoxels");
+    return nat_g2p_stage(e, e->P.max_substep_dt);
 }
 extern "C" int flip_advect_particles(flip_engine* e) {
     CHECK_E();
@@ -1299,7 +1686,7 @@ extern "C" int flip_advect_particles(flip_engine* e) {
 extern "C" int flip_move_solid_particles(flip_engine* e) {
     CHECK_E();
     if (e->P.mode == FLIP_MODE_REFERENCE) return ref_move_solids_stage(e);
-    return FLIP_OK;  // native positions are clamped inside the box by G2P
+    return FLIP_OK;  // native mode: G2P clamps into the box and moves particles out of solid cells
 }
 extern "C" int flip_initialize(flip_engine* e) {
     CHECK_E();
@@ -1361,8 +1748,9 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
         }
         return dev_err_check(e);
     }
-    // sub-steps of min(max_substep_dt, the Courant limit, what is left of the frame)
     const double frameDt = 1.0 / fps;
+    if (cap_supported(e)) return cap_frame_launch(e, frameDt);
+    // sub-steps of min(max_substep_dt, the Courant limit, what is left of the frame)
     double t = 0.0;
     int guard = 0;
     while (frameDt - t > 1e-12 * frameDt) {
@@ -1379,7 +1767,7 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
 extern "C" int flip_step(flip_engine* e, double dt) {
     CHECK_E();
     if (!(dt > 0.0)) return e->fail(FLIP_ERR_ARG, "dt must be positive");
-    if (e->P.mode == FLIP_MODE_NATIVE) return nat_step(e, dt);
+    if (e->P.mode == FLIP_MODE_NATIVE) return cap_supported(e) ? cap_step_launch(e, dt) : nat_step(e, dt);
     // reference math with a fixed dt: bin, P2G, gravity + divergence, SOR,
     // projection, G2P, advection (no Courant clamp, no dt halving)
     E_TRY(ref_align(e));
@@ -1456,7 +1844,8 @@ extern "C" int flip_step_streamed_f32(flip_engine* e, float* px, float* py, floa
     E_CUDA(cudaStreamWaitEvent(e->stream, e->ev_up, 0));
     e->rt_down_pending = false;
     e->binned = e->have_voxels = false;
-    E_TRY(nat_step(e, dt));
+    e->keys_valid = false;
+    E_TRY(cap_supported(e) ? cap_step_launch(e, dt) : nat_step(e, dt));
     // downloads of the new state (the step leaves it in fp)
     E_CUDA(cudaEventRecord(e->ev_step, e->stream));
     E_CUDA(cudaStreamWaitEvent(e->down_stream, e->ev_step, 0));
@@ -1586,6 +1975,7 @@ extern "C" int flip_read_buffer(flip_engine* e, int which, void* host_dst, uint6
 extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
     if (!e || !out) return FLIP_ERR_ARG;
     E_TRY(rt_join(e));
+    if (e->have_domain) E_TRY(rec_refresh(e));
     memset(out, 0, sizeof(*out));
     if (e->have_domain) {
         E_CUDA(cudaStreamSynchronize(e->stream));
@@ -1616,6 +2006,13 @@ extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
     out->elapsed_time = e->elapsed;
     out->n = e->n;
     out->launches = e->launches;
+    if (e->have_domain && e->P.mode == FLIP_MODE_NATIVE && e->d_rec) {
+        SolveRecord r{};
+        E_CUDA(cudaMemcpy(&r, e->d_rec, sizeof(r), cudaMemcpyDeviceToHost));
+        out->solves = r.solves;
+        out->fallbacks = r.fallbacks;
+        out->pressure_iters_total = r.iters_total;
+    }
     return FLIP_OK;
 }
 
@@ -1979,6 +2376,10 @@ extern "C" int flip_mg_train_step(flip_engine* e, int sample, float lr, double* 
 
 extern "C" int flip_get_solve_info(flip_engine* e, flip_solve_info* out) {
     if (!e || !out) return FLIP_ERR_ARG;
+    if (e->have_domain) {
+        E_CUDA(cudaSetDevice(e->P.device));
+        E_TRY(rec_refresh(e));
+    }
     *out = e->last_solve;
     return FLIP_OK;
 }
@@ -2022,6 +2423,7 @@ extern "C" int flip_destroy(flip_engine* e) {
     for (auto v : evs) if (v) cudaEventDestroy(v);
     if (e->up_stream) cudaStreamDestroy(e->up_stream);
     if (e->down_stream) cudaStreamDestroy(e->down_stream);
+    for (auto& c : e->cap_streams) if (c) cudaStreamDestroy(c);
     if (e->lp_warena) cudaFree(e->lp_warena);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;

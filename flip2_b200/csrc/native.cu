@@ -11,8 +11,11 @@
 //
 // Particles are SoA float arrays sorted by tile every step (sort.cu), so a
 // CTA working on one tile reads one contiguous particle range.
+#include <cudaTypedefs.h>
+#include <mutex>
 #include "common.cuh"
 #include "native.cuh"
+#include "tma.cuh"
 
 namespace flip {
 
@@ -102,22 +105,60 @@ __global__ void nat_gather_kernel(const uint32_t* __restrict__ perm, uint64_t n,
 // trilinear weights into a shared-memory box of 10^3 nodes per component
 // (the tile plus the one-node halo its stencils reach); the box is then
 // added to the global grids.  Also marks the cells that hold particles.
+//
+// The box accumulates in one of two forms (P2GAcc):
+//   kAccF32: FP32 sums, updated with shared-memory float atomics;
+//   kAccFix64: 64-bit fixed point with 32 fraction bits, updated with
+//     shared-memory integer atomics.  A particle adds at most 1 to a weight
+//     sum and at most |v| to a momentum sum, so the sums stay far inside the
+//     signed 64-bit range; each term is rounded once (to 2^-33), the sums are
+//     exact and independent of the order of the atomics.
+enum P2GAcc { kAccF32 = 0, kAccFix64 = 1 };
 constexpr int kP2GThreads = 256;
 constexpr int kBox = 10;
 constexpr int kBoxN = kBox * kBox * kBox;
+constexpr float kFix = 4294967296.0f;          // 2^32
+constexpr double kInvFix = 1.0 / 4294967296.0;
 
+template <int ACC>
+struct P2GBox;
+template <>
+struct P2GBox<kAccF32> {
+    float v[3][2][kBoxN];
+    __device__ __forceinline__ void add(int c, int l, float w, float wv) {
+        atomicAdd(&v[c][0][l], wv);
+        atomicAdd(&v[c][1][l], w);
+    }
+    __device__ __forceinline__ float mom(int c, int l) const { return v[c][0][l]; }
+    __device__ __forceinline__ float wt(int c, int l) const { return v[c][1][l]; }
+    __device__ __forceinline__ void clear(int l) { (&v[0][0][0])[l] = 0.0f; }
+};
+template <>
+struct P2GBox<kAccFix64> {
+    unsigned long long v[3][2][kBoxN];
+    __device__ __forceinline__ void add(int c, int l, float w, float wv) {
+        atomicAdd(&v[c][0][l], (unsigned long long)__float2ll_rn(wv * kFix));
+        atomicAdd(&v[c][1][l], (unsigned long long)__float2ll_rn(w * kFix));
+    }
+    __device__ __forceinline__ float mom(int c, int l) const { return (float)((double)(long long)v[c][0][l] * kInvFix); }
+    __device__ __forceinline__ float wt(int c, int l) const { return (float)((double)(long long)v[c][1][l] * kInvFix); }
+    __device__ __forceinline__ void clear(int l) { (&v[0][0][0])[l] = 0ull; }
+};
+
+template <int ACC>
 __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
     const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
     uint64_t n, const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
     const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, NatDims D,
     float* __restrict__ mu, float* __restrict__ mv, float* __restrict__ mw, float* __restrict__ wu,
     float* __restrict__ wv, float* __restrict__ ww, uint8_t* __restrict__ type) {
-    __shared__ float sm[3][2][kBoxN];
+    extern __shared__ __align__(16) unsigned char p2g_smem[];
+    P2GBox<ACC>& sm = *reinterpret_cast<P2GBox<ACC>*>(p2g_smem);
     const uint32_t ntiles = *d_ntiles;
     float* gm[3] = {mu, mv, mw};
     float* gw[3] = {wu, wv, ww};
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        for (int l = threadIdx.x; l < 3 * 2 * kBoxN; l += kP2GThreads) (&sm[0][0][0])[l] = 0.0f;
+        for (int l = threadIdx.x; l < 3 * 2 * kBoxN; l += kP2GThreads) sm.clear(l);
         __syncthreads();
         const uint32_t key = tile_keys[t];
         const int tx = key % D.tx, ty = (key / D.tx) % D.ty, tz = key / (D.tx * D.ty);
@@ -155,9 +196,7 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
                             // a zero weight (a wall face) changes no sum
                             const float w = wx[di] * wy[dj] * wz[dk];
                             if (w == 0.0f) continue;
-                            const int l = l0 + di + kBox * (dj + kBox * dk);
-                            atomicAdd(&sm[c][0][l], w * v[c]);
-                            atomicAdd(&sm[c][1][l], w);
+                            sm.add(c, l0 + di + kBox * (dj + kBox * dk), w, w * v[c]);
                         }
             }
         }
@@ -169,10 +208,10 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
             const uint32_t s = nslot(i, j, k, D);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                float w = sm[c][1][l];
+                const float w = sm.wt(c, l);
                 if (w != 0.0f) {
                     atomicAdd(gw[c] + s, w);
-                    atomicAdd(gm[c] + s, sm[c][0][l]);
+                    atomicAdd(gm[c] + s, sm.mom(c, l));
                 }
             }
         }
@@ -315,6 +354,41 @@ __global__ void __launch_bounds__(kCompactThreads) nat_compact_kernel(const uint
     if (threadIdx.x == 0) *d_count = total;
 }
 
+// Segment heads of the sorted tile keys through a dense per-tile table
+// (replaces a scan of head flags: no look-back chain).  dense[key] = index of
+// the first particle with that tile key (kNoHead if the tile is empty); the
+// compaction then lists the occupied tiles in key order -- the order of the
+// sorted segments -- with their starts.
+constexpr uint32_t kNoHead = 0xFFFFFFFFu;
+__global__ void nat_heads_kernel(const uint32_t* __restrict__ keys, uint64_t n, uint32_t ntotal,
+                                 uint32_t* __restrict__ dense) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if ((i == 0 || keys[i - 1] != k) && k < ntotal) dense[k] = (uint32_t)i;
+    }
+}
+__global__ void __launch_bounds__(kCompactThreads) nat_heads_compact_kernel(const uint32_t* __restrict__ dense,
+                                                                            uint32_t ntotal, uint32_t* __restrict__ list,
+                                                                            uint32_t* __restrict__ starts,
+                                                                            uint32_t* __restrict__ d_count) {
+    __shared__ uint32_t sh[kCompactThreads / 32 + 1];
+    const uint32_t per = (ntotal + kCompactThreads - 1) / kCompactThreads;
+    const uint32_t b0 = min(ntotal, threadIdx.x * per), b1 = min(ntotal, b0 + per);
+    uint32_t c = 0;
+    for (uint32_t i = b0; i < b1; ++i) c += dense[i] != kNoHead ? 1u : 0u;
+    uint32_t total;
+    uint32_t o = block_exclusive_scan<kCompactThreads>(c, sh, &total);
+    for (uint32_t i = b0; i < b1; ++i) {
+        const uint32_t st = dense[i];
+        if (st != kNoHead) {
+            list[o] = i;
+            starts[o] = st;
+            ++o;
+        }
+    }
+    if (threadIdx.x == 0) *d_count = total;
+}
+
 // solid mask (tile-blocked) onto the cell types
 __global__ void nat_apply_solids_kernel(const uint8_t* __restrict__ solid, uint8_t* __restrict__ type, uint64_t nslots) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -340,23 +414,31 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
                                                              const float* __restrict__ wv, const float* __restrict__ ww,
                                                              float* __restrict__ ou, float* __restrict__ ov,
                                                              float* __restrict__ ow, const uint8_t* __restrict__ type,
-                                                             float3 usolid) {
+                                                             float3 usolid, float* __restrict__ lu, float* __restrict__ lv,
+                                                             float* __restrict__ lw, float* __restrict__ lou,
+                                                             float* __restrict__ lov, float* __restrict__ low,
+                                                             const float* __restrict__ gdt_p) {
     const uint32_t cnt = *d_count;
+    if (gdt_p) gdt = *gdt_p;
     const float us[3] = {usolid.x, usolid.y, usolid.z};
     float* m[3] = {mu, mv, mw};
     const float* w[3] = {wu, wv, ww};
     float* o[3] = {ou, ov, ow};
+    float* L[3] = {lu, lv, lw};
+    float* LO[3] = {lou, lov, low};
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
     for (uint32_t t = blockIdx.x; t < cnt; t += gridDim.x) {
         const uint32_t key = tiles[t];
         const int i = 8 * (key % D.tx) + li, j = 8 * ((key / D.tx) % D.ty) + lj, k = 8 * (key / (D.tx * D.ty)) + lk;
         const uint32_t s = (key << 9) | threadIdx.x;
+        const uint32_t lin = (uint32_t)i + (uint32_t)D.nx * ((uint32_t)j + (uint32_t)D.ny * (uint32_t)k);
         const uint8_t tb = type[s];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             float wt = w[c][s];
             float val = wt > 0.0f ? __fdiv_rn(m[c][s], wt) : 0.0f;
             o[c][s] = val;
+            if (LO[c]) LO[c][lin] = val;
             uint8_t ta = nat_type(type, i - (c == 0), j - (c == 1), k - (c == 2), D);
             // wall faces and faces between two solids 0; a face between a
             // solid and a non-solid cell moves with the solid
@@ -364,6 +446,7 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
             if (ta == kSolid || tb == kSolid) val = (!wall && ((ta == kSolid) != (tb == kSolid))) ? us[c] : 0.0f;
             else if (c == 1 && (ta == kFluid || tb == kFluid)) val += gdt;
             m[c][s] = val;
+            if (L[c]) L[c][lin] = val;
         }
     }
 }
@@ -373,31 +456,6 @@ __global__ void __launch_bounds__(512) nat_normalize_kernel(const uint32_t* __re
 // number of non-solid neighbours on the diagonal and -1 for each fluid
 // neighbour (air neighbours are Dirichlet zero, solid ones Neumann).
 
-// last CTA to finish sums the per-CTA partials (fixed order: deterministic)
-template <int NV, int NT>
-__device__ __forceinline__ bool last_block_reduce_n(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
-                                                    double (&out)[NV]) {
-    __shared__ bool s_last;
-#pragma unroll
-    for (int q = 0; q < NV; ++q) {
-        double r = block_sum_f64<NT>(v[q], sh);
-        if (threadIdx.x == 0) partials[q * kPcgBlocks + blockIdx.x] = r;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-    __syncthreads();
-    if (!s_last) return false;
-    __threadfence();
-#pragma unroll
-    for (int q = 0; q < NV; ++q) {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) a += ((volatile double*)partials)[q * kPcgBlocks + b];
-        out[q] = block_sum_f64<NT>(a, sh);
-    }
-    if (threadIdx.x == 0) *ticket = 0u;
-    return true;  // out[] valid in thread 0
-}
 template <int NV>
 __device__ __forceinline__ bool last_block_reduce(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
                                                   double (&out)[NV]) {
@@ -428,12 +486,18 @@ __device__ __forceinline__ float jacobi_inv_s(const float* tab, uint8_t c) { ret
 // cell_prev (warm start): the previous solve's cell codes; x starts from the
 // previous solution (x + xg) on cells that are fluid in both solves, 0
 // elsewhere, and pcg_warm_kernel then replaces r = b by b - A x
+// W (the TMA Jacobi-PCG of pcg_tma.cu): the residual is kept Jacobi-scaled,
+// w = D^-1 r, and the tiles walked are the dilated list, so that w and both
+// direction buffers are also zero on the non-fluid cells around the fluid
+// (the halo reads of that solver take no cell codes)
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
                                                         const uint8_t* __restrict__ cell_prev, PcgBuffers B) {
     __shared__ double sh[32];
     const uint32_t ntiles = *d_ntiles;
+    const bool warm = cell_prev && (!B.warm_ok || *B.warm_ok);
     double bb = 0.0, rz = 0.0, nf = 0.0;
     NAT_TILE_LOOP_BEGIN
     float b = 0.0f;
@@ -461,12 +525,13 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     B.cell[s] = code;
     B.b[s] = b;
     double x0 = 0.0;
-    if (cell_prev && (code & kCellFluid) && (cell_prev[s] & kCellFluid)) x0 = B.x[s] + (double)B.xg[s];
+    if (warm && (code & kCellFluid) && (cell_prev[s] & kCellFluid)) x0 = B.x[s] + (double)B.xg[s];
     B.x[s] = x0;
     B.xg[s] = 0.0f;
-    B.r[s] = b;
-    B.p0[s] = 0.0f;
     const float z = b * jacobi_inv(code);
+    B.r[s] = W ? ((code & kCellFluid) ? __fdiv_rn(b, (float)(code & 7u)) : 0.0f) : b;
+    B.p0[s] = 0.0f;
+    if (W) B.p1[s] = 0.0f;
     bb += (double)b * (double)b;
     rz += (double)b * (double)z;
     NAT_TILE_LOOP_END
@@ -808,6 +873,7 @@ __global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32
 // iterations.  Replaces r, decides convergence on the true value and asks
 // the next direction kernel to fold xg into x.  The FP64 solution of the tile
 // and its halo is staged in shared memory like the matvec.
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __restrict__ tiles,
                                                             const uint32_t* __restrict__ tcoord,
                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -842,10 +908,16 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
         if (c & kCellFluid) {
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
-            const float rs = (float)res;
-            r[s] = rs;
             rr += res * res;
-            rz += (double)rs * (double)(rs * jacobi_inv(c));
+            if (W) {
+                const float ws = (float)(res / (double)(c & 7u));
+                r[s] = ws;
+                rz += (double)(c & 7u) * (double)ws * (double)ws;
+            } else {
+                const float rs = (float)res;
+                r[s] = rs;
+                rz += (double)rs * (double)(rs * jacobi_inv(c));
+            }
         }
         __syncthreads();
     }
@@ -878,6 +950,7 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
 // warm start: r = b - A x in FP64 for the initial guess, r.r and r.z, and
 // the state for the first iteration (converged already if |r| <= tol |b|;
 // b = 0 gives x = 0)
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __restrict__ tiles,
                                                            const uint32_t* __restrict__ tcoord,
                                                            const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -914,10 +987,16 @@ __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __rest
         if (c & kCellFluid) {
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
-            const float rs = (float)res;
-            r[s] = rs;
             rr += res * res;
-            rz += (double)rs * (double)(rs * jacobi_inv(c));
+            if (W) {
+                const float ws = (float)(res / (double)(c & 7u));
+                r[s] = ws;
+                rz += (double)(c & 7u) * (double)ws * (double)ws;
+            } else {
+                const float rs = (float)res;
+                r[s] = rs;
+                rz += (double)rs * (double)(rs * jacobi_inv(c));
+            }
         }
         __syncthreads();
     }
@@ -987,9 +1066,12 @@ __global__ void __launch_bounds__(512, 4) fpcg_dot_kernel(const uint32_t* __rest
 __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_count,
                                                            NatDims D, const double* __restrict__ phi, const float* __restrict__ phig,
                                                            const uint8_t* __restrict__ type, float* __restrict__ u,
-                                                           float* __restrict__ v, float* __restrict__ w) {
+                                                           float* __restrict__ v, float* __restrict__ w,
+                                                           float* __restrict__ lu, float* __restrict__ lv,
+                                                           float* __restrict__ lw) {
     const uint32_t ntiles = *d_count;
     float* U[3] = {u, v, w};
+    float* L[3] = {lu, lv, lw};
     NAT_TILE_LOOP_BEGIN
     const uint8_t tb = type[s];
 #pragma unroll
@@ -1001,52 +1083,153 @@ __global__ void __launch_bounds__(512) nat_project_kernel(const uint32_t* __rest
         double pb = (tb == kFluid) ? phi[s] + (double)phig[s] : 0.0;
         const uint32_t sa = (ta == kFluid) ? nslot(ia, ja, ka, D) : 0u;
         double pa = (ta == kFluid) ? phi[sa] + (double)phig[sa] : 0.0;
-        U[c][s] -= (float)(pb - pa);
+        const float nu = U[c][s] - (float)(pb - pa);
+        U[c][s] = nu;
+        if (L[c]) L[c][(uint32_t)i + (uint32_t)D.nx * ((uint32_t)j + (uint32_t)D.ny * (uint32_t)k)] = nu;
     }
     NAT_TILE_LOOP_END
 }
 
 // ------------------------------------------------------- G2P + advect
-// FLIP/PIC blend of the grid velocity change, then RK2 (midpoint) through the
-// projected grid velocity; positions clamped inside the box.
-__global__ void __launch_bounds__(256) nat_g2p_kernel(uint64_t n, NatDims D, float dt, float flip,
-                                                       const float* __restrict__ u, const float* __restrict__ v,
-                                                       const float* __restrict__ w, const float* __restrict__ ou,
-                                                       const float* __restrict__ ov, const float* __restrict__ ow,
-                                                       float* __restrict__ px, float* __restrict__ py, float* __restrict__ pz,
-                                                       float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz) {
-    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const float* U[3] = {u, v, w};
-    const float* O[3] = {ou, ov, ow};
-    float X[3] = {px[p], py[p], pz[p]};
-    float V[3] = {vx[p], vy[p], vz[p]};
+// One CTA per occupied tile (persistent loop).  The new and old face
+// velocities around the tile come into shared memory by TMA: for each of the
+// six fields one 16 x 12 x 12 box of its linear (x-fastest) copy, from
+// (8tx - 4, 8ty - 2, 8tz - 2) -- x starts on a 16-byte boundary, and the
+// two-cell margin in y and z (four and four in x) covers the stencils of
+// every particle of the tile and of RK2 midpoints that move less than a cell
+// (zero fill outside the grid is the wall value).  The tile's particles then
+// sample the boxes: the FLIP/PIC blend of the grid velocity change, the RK2
+// midpoint through the new grid (from global memory in the rare case that
+// the midpoint's stencil leaves the box), the clamp into the box, the
+// reseed of particles that entered an interior solid cell (the native form of
+// the reference's moveSolids, engine/particles.cu:674-740: the particle
+// returns to its position at the start of the step, which lay outside every
+// solid, and takes the solid's velocity), and the tile key of the new
+// position for the next step's sort.
+constexpr int kG2PThreads = 256;
+constexpr int kGBx = 16, kGBy = 12, kGBz = 12;
+constexpr int kGBoxN = kGBx * kGBy * kGBz;                    // 2304 floats
+constexpr uint32_t kGBoxBytes = kGBoxN * sizeof(float);        // 9216 B
+constexpr uint32_t kG2PSmem = 6 * kGBoxBytes + 128;            // six boxes + the mbarrier
+constexpr uint32_t kG2PSpinLimit = 1u << 24;
+
+// trilinear sample of component c's box (origin bx0, by0, bz0) at grid
+// coordinates g; false when the stencil leaves the box
+__device__ __forceinline__ bool box_sample(const float* __restrict__ B, int c, float gx, float gy, float gz,
+                                           const NatDims& D, int bx0, int by0, int bz0, float& out) {
+    int i0, j0, k0;
+    float fx, fy, fz;
+    nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
+    const int li = i0 - bx0, lj = j0 - by0, lk = k0 - bz0;
+    if ((unsigned)li >= (unsigned)(kGBx - 1) || (unsigned)lj >= (unsigned)(kGBy - 1) || (unsigned)lk >= (unsigned)(kGBz - 1))
+        return false;
+    const float* b = B + li + kGBx * (lj + kGBy * lk);
+    const float c00 = fmaf(fx, b[1] - b[0], b[0]);
+    const float c10 = fmaf(fx, b[kGBx + 1] - b[kGBx], b[kGBx]);
+    const float c01 = fmaf(fx, b[kGBx * kGBy + 1] - b[kGBx * kGBy], b[kGBx * kGBy]);
+    const float c11 = fmaf(fx, b[kGBx * kGBy + kGBx + 1] - b[kGBx * kGBy + kGBx], b[kGBx * kGBy + kGBx]);
+    const float c0 = fmaf(fy, c10 - c00, c00), c1 = fmaf(fy, c11 - c01, c01);
+    out = fmaf(fz, c1 - c0, c0);
+    return true;
+}
+
+__global__ void __launch_bounds__(kG2PThreads) nat_g2p_tile_kernel(
+    const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv, const __grid_constant__ CUtensorMap mw,
+    const __grid_constant__ CUtensorMap mou, const __grid_constant__ CUtensorMap mov, const __grid_constant__ CUtensorMap mow,
+    const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
+    uint64_t n, NatDims D, float dt, float flip, const float* __restrict__ gu, const float* __restrict__ gv,
+    const float* __restrict__ gw, const float* __restrict__ gou, const float* __restrict__ gov,
+    const float* __restrict__ gow, const float* px, const float* py, const float* pz, const float* vx,
+    const float* vy, const float* vz, float* qx, float* qy, float* qz, float* wx, float* wy, float* wz,
+    uint32_t* __restrict__ keys_out, const uint8_t* __restrict__ solid_type, float3 usolid, const float* __restrict__ dt_p,
+    uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char g2p_smem[];
+    float* box = reinterpret_cast<float*>(g2p_smem);  // U u, v, w then O u, v, w
+    uint64_t* bar = reinterpret_cast<uint64_t*>(g2p_smem + 6 * kGBoxBytes);
+    const CUtensorMap* maps[6] = {&mu, &mv, &mw, &mou, &mov, &mow};
+    const float* G[3] = {gu, gv, gw};
+    const float* GO[3] = {gou, gov, gow};
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    const uint32_t ntiles = *d_ntiles;
+    if (dt_p) dt = *dt_p;
     const float o[3] = {D.ox, D.oy, D.oz};
     const int nn[3] = {D.nx, D.ny, D.nz};
-    float g[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) g[c] = __fdiv_rn(__fsub_rn(X[c], o[c]), D.h);
-    float un[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        un[c] = nat_sample(U[c], c, g[0], g[1], g[2], D);
-        float uo = nat_sample(O[c], c, g[0], g[1], g[2], D);
-        float vf = V[c] + (un[c] - uo);
-        V[c] = flip * vf + (1.0f - flip) * un[c];
-    }
-    float gm[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gm[c] = __fdiv_rn(__fsub_rn(fmaf(0.5f * dt, un[c], X[c]), o[c]), D.h);
     const float eps = 1e-3f * D.h;
+    uint32_t parity = 0;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t key = tile_keys[t];
+        const int tx = (int)(key % D.tx), ty = (int)((key / D.tx) % D.ty), tz = (int)(key / (D.tx * D.ty));
+        const int bx0 = 8 * tx - 4, by0 = 8 * ty - 2, bz0 = 8 * tz - 2;
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();  // the previous tile's reads of the boxes come first
+            mbar_expect_tx(bar, 6 * kGBoxBytes);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float um = nat_sample(U[c], c, gm[0], gm[1], gm[2], D);
-        float xn = fmaf(dt, um, X[c]);
-        float lo = o[c] + eps, hi = o[c] + (float)nn[c] * D.h - eps;
-        X[c] = fminf(fmaxf(xn, lo), hi);
+            for (int f = 0; f < 6; ++f) tma_load_3d(box + f * kGBoxN, maps[f], bx0, by0, bz0, bar);
+        }
+        const uint32_t start = starts[t];
+        const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
+        // every thread waits on the copies; the CTA decides together
+        if (!__syncthreads_and(mbar_wait_bounded(bar, parity, kG2PSpinLimit))) {
+            // the copies never completed: report, wait (bounded) once more so
+            // that no copy lands after the CTA has left, and stop
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_TMA_TIMEOUT);
+            mbar_wait_bounded(bar, parity, kG2PSpinLimit);
+            return;
+        }
+        parity ^= 1u;
+        for (uint64_t p = start + threadIdx.x; p < end; p += kG2PThreads) {
+            float X[3] = {px[p], py[p], pz[p]};
+            float V[3] = {vx[p], vy[p], vz[p]};
+            float g[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) g[c] = __fdiv_rn(__fsub_rn(X[c], o[c]), D.h);
+            float un[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                // the stencils of a particle of this tile lie inside the box;
+                // the global reads only guard against a position the binning
+                // did not see
+                float uo;
+                if (!box_sample(box + c * kGBoxN, c, g[0], g[1], g[2], D, bx0, by0, bz0, un[c]))
+                    un[c] = nat_sample(G[c], c, g[0], g[1], g[2], D);
+                if (!box_sample(box + (3 + c) * kGBoxN, c, g[0], g[1], g[2], D, bx0, by0, bz0, uo))
+                    uo = nat_sample(GO[c], c, g[0], g[1], g[2], D);
+                const float vf = V[c] + (un[c] - uo);
+                V[c] = flip * vf + (1.0f - flip) * un[c];
+            }
+            float gm[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) gm[c] = __fdiv_rn(__fsub_rn(fmaf(0.5f * dt, un[c], X[c]), o[c]), D.h);
+            float Xn[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float um;
+                if (!box_sample(box + c * kGBoxN, c, gm[0], gm[1], gm[2], D, bx0, by0, bz0, um))
+                    um = nat_sample(G[c], c, gm[0], gm[1], gm[2], D);
+                const float xn = fmaf(dt, um, X[c]);
+                const float lo = o[c] + eps, hi = o[c] + (float)nn[c] * D.h - eps;
+                Xn[c] = fminf(fmaxf(xn, lo), hi);
+            }
+            // a particle moved into an interior solid cell goes back to where
+            // it started the step (a non-solid cell) and moves with the solid
+            if (solid_type &&
+                solid_type[nslot(nat_cell(Xn[0], D.ox, D.h, D.nx), nat_cell(Xn[1], D.oy, D.h, D.ny),
+                                 nat_cell(Xn[2], D.oz, D.h, D.nz), D)] == kSolid) {
+                V[0] = usolid.x; V[1] = usolid.y; V[2] = usolid.z;
+            } else {
+                X[0] = Xn[0]; X[1] = Xn[1]; X[2] = Xn[2];
+            }
+            qx[p] = X[0]; qy[p] = X[1]; qz[p] = X[2];
+            wx[p] = V[0]; wy[p] = V[1]; wz[p] = V[2];
+            if (keys_out) {
+                const int ci = nat_cell(X[0], D.ox, D.h, D.nx), cj = nat_cell(X[1], D.oy, D.h, D.ny),
+                          ck = nat_cell(X[2], D.oz, D.h, D.nz);
+                keys_out[p] = (uint32_t)((ci >> 3) + D.tx * ((cj >> 3) + D.ty * (ck >> 3)));
+            }
+        }
+        __syncthreads();  // every thread is done with the boxes before the next copy
     }
-    px[p] = X[0]; py[p] = X[1]; pz[p] = X[2];
-    vx[p] = V[0]; vy[p] = V[1]; vz[p] = V[2];
 }
 
 // ----------------------------------------------------------- launchers
@@ -1065,11 +1248,19 @@ int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src,
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+// the accumulator form of the P2G box
+constexpr int kP2GAcc = kAccFix64;
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s) {
-    nat_p2g_kernel<<<grid, kP2GThreads, 0, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0], vs[1], vs[2], D,
-                                                m[0], m[1], m[2], w[0], w[1], w[2], type);
+    constexpr size_t smem = sizeof(P2GBox<kP2GAcc>);
+    static bool attr_done = false;
+    if (!attr_done) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_p2g_kernel<kP2GAcc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_done = true;
+    }
+    nat_p2g_kernel<kP2GAcc><<<grid, kP2GThreads, smem, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
+                                                             vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1090,6 +1281,14 @@ int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_
     FLIP_CUDA_TRY(cudaMemsetAsync(flags, 0, ntiles_total, s));
     nat_mark_fluid_tiles_kernel<<<nb(nslots, 256), 256, 0, s>>>(type, flags, nslots);
     nat_compact_kernel<<<1, kCompactThreads, 0, s>>>(flags, ntiles_total, list, d_count);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_segment_heads(const uint32_t* keys, uint64_t n, uint32_t ntiles_total, uint32_t* dense, uint32_t* list,
+                             uint32_t* starts, uint32_t* d_count, int grid, cudaStream_t s) {
+    FLIP_CUDA_TRY(cudaMemsetAsync(dense, 0xFF, sizeof(uint32_t) * ntiles_total, s));
+    if (n) nat_heads_kernel<<<grid, 256, 0, s>>>(keys, n, ntiles_total, dense);
+    nat_heads_compact_kernel<<<1, kCompactThreads, 0, s>>>(dense, ntiles_total, list, starts, d_count);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1131,16 +1330,21 @@ int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tile
 }
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
                          const float* const* w, float* const* o, const uint8_t* type, float3 usolid, int grid,
-                         cudaStream_t s) {
-    nat_normalize_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, gdt, m[0], m[1], m[2], w[0], w[1], w[2], o[0], o[1], o[2], type, usolid);
+                         cudaStream_t s, float* const* lin, float* const* lin_old, const float* gdt_p) {
+    float* const nl[3] = {nullptr, nullptr, nullptr};
+    float* const* L = lin ? lin : nl;
+    float* const* LO = lin_old ? lin_old : nl;
+    nat_normalize_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, gdt, m[0], m[1], m[2], w[0], w[1], w[2], o[0], o[1], o[2],
+                                              type, usolid, L[0], L[1], L[2], LO[0], LO[1], LO[2], gdt_p);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
-    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
+    pcg_init_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
     if (cell_prev)
-        pcg_warm_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st, B.partials);
+        pcg_warm_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
+                                                          B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1181,7 +1385,27 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
 }
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s) {
-    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st, B.partials);
+    pcg_check_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
+                                                       B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+// the Jacobi-scaled form (pcg_tma.cu): init over the dilated tile list, warm
+// start and true-residual check over the occupied tiles
+int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
+                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
+                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
+    pcg_init_kernel<true><<<kPcgBlocks, 512, 0, s>>>(dil_tiles, d_ndil, D, U[0], U[1], U[2], type, cell_prev, B);
+    if (cell_prev)
+        pcg_warm_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
+                                                         B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                          cudaStream_t s) {
+    pcg_check_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
+                                                      B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1194,6 +1418,106 @@ int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, c
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
+// ------------------------------------------------ solve and frame control
+__global__ void pcg_state_init_kernel(PcgState* st, double tol2, int max_iter, int true_every, int flexible) {
+    PcgState init{};
+    init.tol2 = tol2;
+    init.max_iter = max_iter;
+    init.true_every = true_every;
+    init.next_check = true_every;
+    init.flexible = flexible;
+    *st = init;
+}
+int nat_launch_state_init(PcgState* st, double tol, int max_iter, int true_every, int flexible, cudaStream_t s) {
+    pcg_state_init_kernel<<<1, 1, 0, s>>>(st, tol * tol, max_iter, true_every, flexible);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+__global__ void solve_record_kernel(SolveRecord* rec, PcgState* st, int flexible, int stage) {
+    const double rr = st->true_checks ? st->rr_true : st->rr;
+    const double rel = st->bb > 0.0 ? sqrt(rr / st->bb) : 0.0;
+    const int conv = st->done == 1;
+    rec->iters_total += (unsigned long long)st->iter;
+    if (stage == 0) {
+        rec->iters = st->iter;
+        rec->plain_iters = 0;
+        rec->fell_back = flexible && !conv;
+        rec->solves += 1;
+        rec->fallbacks += (unsigned long long)(flexible && !conv);
+        if (flexible) rec->chunks_primary += (unsigned long long)st->chunks;
+        else rec->chunks_plain += (unsigned long long)st->chunks;
+    } else {
+        rec->plain_iters = st->iter;
+        rec->chunks_plain += (unsigned long long)st->chunks;
+    }
+    rec->converged = conv;
+    rec->rel_residual = rel;
+    rec->warm_ok = conv;
+}
+int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, cudaStream_t s) {
+    solve_record_kernel<<<1, 1, 0, s>>>(rec, st, flexible, stage);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+__global__ void cond_set_kernel(cudaGraphConditionalHandle h, unsigned int v) { cudaGraphSetConditional(h, v); }
+int nat_launch_cond_set(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t s) {
+    cond_set_kernel<<<1, 1, 0, s>>>(h, v);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+__global__ void fallback_cond_kernel(cudaGraphConditionalHandle h, const PcgState* st) {
+    cudaGraphSetConditional(h, st->done != 1 ? 1u : 0u);
+}
+int nat_launch_fallback_cond(cudaGraphConditionalHandle h, const PcgState* st, cudaStream_t s) {
+    fallback_cond_kernel<<<1, 1, 0, s>>>(h, st);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+// the rules of the host loop of flip_solve_frame, on the device: sub-steps
+// of min(max_dt, 0.7 h / max |v component|, the rest of the frame); a
+// collapsed dt or 100,000 sub-steps stop the frame with fs->error set
+__global__ void frame_ctl_kernel(cudaGraphConditionalHandle h, FrameState* fs, const uint32_t* vmax_bits, float gravity_y) {
+    const float vmax = __uint_as_float(*vmax_bits);
+    double dt = fmin(fs->max_dt, fs->frame_dt - fs->t);
+    if (vmax > 0.0f) dt = fmin(dt, 0.7 * fs->h / (double)vmax);
+    if (!(dt > 1e-9 * fs->frame_dt) || fs->substeps >= 100000) {
+        fs->error = 1;
+        dt = 0.0;
+    }
+    fs->t += dt;
+    fs->dt = (float)dt;
+    fs->gdt = (float)((double)gravity_y * dt);
+    fs->substeps += 1;
+    cudaGraphSetConditional(h, (!fs->error && fs->frame_dt - fs->t > 1e-12 * fs->frame_dt) ? 1u : 0u);
+}
+int nat_launch_frame_ctl(cudaGraphConditionalHandle h, FrameState* fs, const uint32_t* vmax_bits, float gravity_y,
+                         cudaStream_t s) {
+    frame_ctl_kernel<<<1, 1, 0, s>>>(h, fs, vmax_bits, gravity_y);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+__global__ void frame_init_kernel(FrameState* fs, double frame_dt, double max_dt, double h) {
+    FrameState f{};
+    f.frame_dt = frame_dt;
+    f.max_dt = max_dt;
+    f.h = h;
+    *fs = f;
+}
+int nat_launch_frame_init(FrameState* fs, double frame_dt, double max_dt, double h, cudaStream_t s) {
+    frame_init_kernel<<<1, 1, 0, s>>>(fs, frame_dt, max_dt, h);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+__global__ void step_dt_kernel(FrameState* fs, double dt, float gravity_y) {
+    fs->dt = (float)dt;
+    fs->gdt = (float)((double)gravity_y * dt);
+}
+int nat_launch_step_dt(FrameState* fs, double dt, float gravity_y, cudaStream_t s) {
+    step_dt_kernel<<<1, 1, 0, s>>>(fs, dt, gravity_y);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
 // largest |velocity component| over the particles, as the bits of a
 // non-negative float (their unsigned order is the float order); *out must be 0
 __global__ void __launch_bounds__(256) nat_vmax_kernel(uint64_t n, const float* __restrict__ vx,
@@ -1213,17 +1537,113 @@ int nat_launch_vmax(uint64_t n, const float* const* V, uint32_t* d_out, int grid
     return FLIP_OK;
 }
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
-                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s) {
-    nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, phig, type, U[0], U[1], U[2]);
+                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s,
+                       float* const* lin) {
+    float* const nl[3] = {nullptr, nullptr, nullptr};
+    float* const* L = lin ? lin : nl;
+    nat_project_kernel<<<grid, 512, 0, s>>>(tiles, d_count, D, phi, phig, type, U[0], U[1], U[2], L[0], L[1], L[2]);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
-                   float* const* P, float* const* V, cudaStream_t s) {
+int nat_launch_g2p(const NatG2PMaps& M, const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles,
+                   uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
+                   const float* const* P, const float* const* V, float* const* Pout, float* const* Vout,
+                   uint32_t* keys_out, const uint8_t* solid_type, float3 usolid, const float* dt_p, uint32_t* err,
+                   int grid, cudaStream_t s) {
+    static bool attr_done = false;
+    if (!attr_done) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_g2p_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kG2PSmem));
+        attr_done = true;
+    }
     if (n)
-        nat_g2p_kernel<<<nb(n, 256), 256, 0, s>>>(n, D, dt, flip, U[0], U[1], U[2], O[0], O[1], O[2], P[0], P[1], P[2], V[0],
-                                                  V[1], V[2]);
+        nat_g2p_tile_kernel<<<grid, kG2PThreads, kG2PSmem, s>>>(M.u[0], M.u[1], M.u[2], M.o[0], M.o[1], M.o[2], tile_keys,
+                                                               starts, d_ntiles, n, D, dt, flip, U[0], U[1], U[2], O[0],
+                                                               O[1], O[2], P[0], P[1], P[2], V[0], V[1], V[2], Pout[0],
+                                                               Pout[1], Pout[2], Vout[0], Vout[1], Vout[2], keys_out,
+                                                               solid_type, usolid, dt_p, err);
     FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+
+// ------------------------------------------------------- tensor maps
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::mutex mu;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!fn) {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }
+    return fn;
+}
+
+int encode_tensor_map(CUtensorMap* map, CUtensorMapDataType dtype, int rank, const void* base, const uint64_t* dims,
+                      const uint64_t* strides_bytes, const uint32_t* box) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn) {
+        set_error_text("cuTensorMapEncodeTiled is not available from the driver");
+        return FLIP_ERR_CUDA;
+    }
+    if (reinterpret_cast<uintptr_t>(base) & 255) {
+        set_error_text("tensor map: base not 256-byte aligned");
+        return FLIP_ERR_ARG;
+    }
+    cuuint64_t d[5];
+    cuuint64_t st[4];
+    cuuint32_t b[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = dims[i];
+        b[i] = box[i];
+        es[i] = 1;
+        if (i + 1 < rank) {
+            st[i] = strides_bytes[i];
+            if (st[i] % 16) {
+                set_error_text("tensor map: stride not a multiple of 16 bytes");
+                return FLIP_ERR_ARG;
+            }
+        }
+    }
+    CUresult r = fn(map, dtype, (cuuint32_t)rank, const_cast<void*>(base), d, st, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error_text("cuTensorMapEncodeTiled failed");
+        return FLIP_ERR_CUDA;
+    }
+    return FLIP_OK;
+}
+
+int encode_grid_map_f32(CUtensorMap* map, const float* base, int nx, int ny, int nz, int bx, int by, int bz) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn) {
+        set_error_text("cuTensorMapEncodeTiled is not available from the driver");
+        return FLIP_ERR_CUDA;
+    }
+    if ((bx * 4) % 16 || (nx * 4) % 16 || (reinterpret_cast<uintptr_t>(base) & 255)) {
+        set_error_text("tensor map: box or row not a multiple of 16 bytes, or base not 256-byte aligned");
+        return FLIP_ERR_ARG;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error_text("cuTensorMapEncodeTiled failed");
+        return FLIP_ERR_CUDA;
+    }
+    return FLIP_OK;
+}
+
+int nat_make_g2p_maps(NatG2PMaps& M, float* const* ulin, float* const* olin, const NatDims& D) {
+    for (int c = 0; c < 3; ++c) {
+        if (int rc = encode_grid_map_f32(&M.u[c], ulin[c], D.nx, D.ny, D.nz, kGBx, kGBy, kGBz)) return rc;
+        if (int rc = encode_grid_map_f32(&M.o[c], olin[c], D.nx, D.ny, D.nz, kGBx, kGBy, kGBz)) return rc;
+    }
     return FLIP_OK;
 }
 

@@ -1,5 +1,6 @@
 // native.cuh -- declarations shared by native.cu and the engine.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -54,12 +55,104 @@ struct PcgBuffers {
     uint32_t* tcoord;  // packed tile coordinates of the occupied tiles
     PcgState* st;
     double* partials;  // [4][kPcgBlocks]
+    // device flag of the warm start (optional): the previous solve converged,
+    // so its solution may start this one; 0 makes a warm-start launch cold
+    const int* warm_ok;
+};
+
+// Outcome of the last pressure solve, kept on the device so that steps and
+// frames captured in a CUDA graph need no host round trip; the host reads
+// it when asked (flip_get_info, flip_get_solve_info).
+struct SolveRecord {
+    int iters;          // iterations of the method asked for
+    int plain_iters;    // iterations of a Jacobi-PCG restart (0 if none)
+    int converged;      // the true relative residual met tol
+    int fell_back;      // the flexible solve missed tol and Jacobi-PCG restarted
+    double rel_residual;
+    int warm_ok;        // converged: the next step may start from this pressure
+    int pad;
+    unsigned long long solves, fallbacks;        // since the counters were last cleared
+    unsigned long long iters_total;              // iterations of every solve, restarts included
+    unsigned long long chunks_primary, chunks_plain;  // loop chunks run (the launch count)
+};
+
+// Sub-step control of a captured frame: the device picks each sub-step's dt.
+struct FrameState {
+    double t;           // time already taken in this frame
+    double frame_dt;    // length of the frame
+    double max_dt;      // largest sub-step
+    double h;           // voxel size (the Courant limit is 0.7 h / max |v|)
+    float dt, gdt;      // this sub-step's dt and gravity * dt, read by the step's kernels
+    int substeps;
+    int error;          // 1: dt collapsed (the frame stopped)
 };
 constexpr uint8_t kCellFluid = 0x80;
+
+// The last CTA to finish sums the per-CTA partials, in CTA order (deterministic
+// for a given grid of at most kPcgBlocks CTAs of NT threads); out[] valid in
+// thread 0 of that CTA.
+template <int NV, int NT>
+__device__ __forceinline__ bool last_block_reduce_n(double (&v)[NV], double* partials, unsigned int* ticket, double* sh,
+                                                    double (&out)[NV]) {
+    __shared__ bool s_last;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double r = block_sum_f64<NT>(v[q], sh);
+        if (threadIdx.x == 0) partials[q * kPcgBlocks + blockIdx.x] = r;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) a += ((volatile double*)partials)[q * kPcgBlocks + b];
+        out[q] = block_sum_f64<NT>(a, sh);
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;  // out[] valid in thread 0
+}
+
+// TMA descriptors of the Jacobi-scaled PCG (pcg_tma.cu): the residual w and
+// both direction buffers as 4-D tile tensors (8 x 8 x 8 x tiles) with boxes of
+// a whole tile (c) and of the x (4 x 8 x 8), y (8 x 1 x 8) and z (8 x 8 x 1)
+// faces, q and xg with tile boxes, and the cell codes (512 bytes a tile)
+struct PcgMaps {
+    CUtensorMap wc, wx, wy, wz;
+    CUtensorMap p0c, p0x, p0y, p0z;
+    CUtensorMap p1c, p1x, p1y, p1z;
+    CUtensorMap qc, xgc, cellc;
+};
+int nat_make_pcg_maps(PcgMaps& M, const PcgBuffers& B, uint64_t ntiles_total);
+// one Jacobi-PCG iteration with TMA-staged tiles on the Jacobi-scaled
+// residual kept in B.r (w = D^-1 r); a TMA wait that gives up sets
+// DEVERR_TMA_TIMEOUT in *err
+int nat_launch_pcgw_iteration(const PcgMaps& M, const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D,
+                              PcgBuffers& B, uint32_t* err, int grid, cudaStream_t s);
+// initial state of that solve (B.r = D^-1 b; w and both directions zero on
+// the non-fluid cells of the dilated tiles dil_tiles), with the warm start as
+// nat_launch_pcg_init's; and its true-residual check (B.r = D^-1 (b - A x))
+int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
+                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
+                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev = nullptr);
+int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                          cudaStream_t s);
+// TMA descriptor of an arbitrary dense tensor (rank <= 5, strides in bytes of
+// dims 1 .. rank-1), zero fill outside it
+int encode_tensor_map(CUtensorMap* map, CUtensorMapDataType dtype, int rank, const void* base, const uint64_t* dims,
+                      const uint64_t* strides_bytes, const uint32_t* box);
 
 int nat_launch_keys(const float* px, const float* py, const float* pz, uint64_t n, const NatDims& D, uint32_t* keys,
                     cudaStream_t s);
 int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src, float* const* dst, cudaStream_t s);
+// occupied tiles of sorted tile keys, in key order: list[c] the tile key,
+// starts[c] its first particle, *d_count their number (dense: a scratch
+// table of ntiles_total words)
+int nat_launch_segment_heads(const uint32_t* keys, uint64_t n, uint32_t ntiles_total, uint32_t* dense, uint32_t* list,
+                             uint32_t* starts, uint32_t* d_count, int grid, cudaStream_t s);
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s);
@@ -80,9 +173,13 @@ int nat_launch_apply_solids(const uint8_t* solid, uint8_t* type, uint64_t nslots
 int nat_launch_mask_to_tiles(const uint8_t* lin, const NatDims& D, uint8_t* tiled, cudaStream_t s);
 // P2G sums -> face velocities; gravity on faces touching fluid; wall faces
 // 0; faces between a solid and a non-solid cell take usolid
+// lin / lin_old (optional): x-fastest copies of the face velocities and of
+// the P2G ("old") velocities, for the TMA boxes of G2P; gdt_p (optional)
+// replaces gdt by a device value
 int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, float gdt, float* const* m,
                          const float* const* w, float* const* o, const uint8_t* type, float3 usolid, int grid,
-                         cudaStream_t s);
+                         cudaStream_t s, float* const* lin = nullptr, float* const* lin_old = nullptr,
+                         const float* gdt_p = nullptr);
 // U == nullptr: the right-hand side is already in B.b (standalone Poisson problems).
 // cell_prev != nullptr: warm start from the previous solution (x + xg) on the
 // cells that were fluid in the previous solve (cell_prev: its cell codes)
@@ -106,11 +203,50 @@ int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const 
 // end of a loop chunk inside a conditional WHILE graph node: continue while
 // the solve is not done and fewer than limit chunks have run
 int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, cudaStream_t s);
+// PcgState for a new solve: tolerance tol^2 of the relative residual,
+// iteration cap, FP64 true-residual period, flexible (FCG) or Jacobi-PCG
+int nat_launch_state_init(PcgState* st, double tol, int max_iter, int true_every, int flexible, cudaStream_t s);
+// the solve's outcome into rec: stage 0 after the method asked for (method 0:
+// Jacobi-PCG; else the flexible solve, whose miss of tol is a fallback),
+// stage 1 after the Jacobi-PCG restart
+int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, cudaStream_t s);
+// sets a conditional node's condition value
+int nat_launch_cond_set(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t s);
+// condition of a conditional IF node: the flexible solve did not converge
+int nat_launch_fallback_cond(cudaGraphConditionalHandle h, const PcgState* st, cudaStream_t s);
+// one sub-step of a captured frame: dt = min(max_dt, Courant limit from
+// *vmax_bits, the rest of the frame) into fs, and the WHILE condition of the
+// sub-step loop (more of the frame left after this sub-step)
+int nat_launch_frame_ctl(cudaGraphConditionalHandle h, FrameState* fs, const uint32_t* vmax_bits, float gravity_y,
+                         cudaStream_t s);
+// a new frame of length frame_dt in fs (t = 0, no sub-steps yet)
+int nat_launch_frame_init(FrameState* fs, double frame_dt, double max_dt, double h, cudaStream_t s);
+// fs->dt and fs->gdt of a fixed-dt step
+int nat_launch_step_dt(FrameState* fs, double dt, float gravity_y, cudaStream_t s);
 // *d_out = bits of max over particles of max(|vx|, |vy|, |vz|) (the Courant limit's speed)
 int nat_launch_vmax(uint64_t n, const float* const* V, uint32_t* d_out, int grid, cudaStream_t s);
+// lin (optional): the x-fastest copy of U, updated alike
 int nat_launch_project(const uint32_t* tiles, const uint32_t* d_count, const NatDims& D, const double* phi,
-                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s);
-int nat_launch_g2p(uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
-                   float* const* P, float* const* V, cudaStream_t s);
+                       const float* phig, const uint8_t* type, float* const* U, int grid, cudaStream_t s,
+                       float* const* lin = nullptr);
+// TMA descriptors of the x-fastest copies of the new (u) and old (o) face
+// velocities, encoded once per domain
+struct NatG2PMaps {
+    CUtensorMap u[3], o[3];
+};
+int nat_make_g2p_maps(NatG2PMaps& M, float* const* ulin, float* const* olin, const NatDims& D);
+// G2P + FLIP blend + RK2 advection per occupied tile (tile_keys/starts of this
+// step's binning), grids staged by TMA; particle state read from P, V and
+// written to Pout, Vout (the same arrays, or the pre-gather ones); dt_p
+// (optional) replaces dt by a device value; keys_out (optional) receives each
+// particle's tile key at its new position; solid_type (optional, the cell
+// types of this step, tile-blocked): a particle whose new position lies in a
+// solid cell keeps its old position and takes the velocity usolid; a TMA
+// wait that gives up sets DEVERR_TMA_TIMEOUT in *err
+int nat_launch_g2p(const NatG2PMaps& M, const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles,
+                   uint64_t n, const NatDims& D, float dt, float flip, const float* const* U, const float* const* O,
+                   const float* const* P, const float* const* V, float* const* Pout, float* const* Vout,
+                   uint32_t* keys_out, const uint8_t* solid_type, float3 usolid, const float* dt_p, uint32_t* err,
+                   int grid, cudaStream_t s);
 
 }  // namespace flip

@@ -254,7 +254,10 @@ double flip_get_courant_dt(flip_engine* e);         /* getCourantDt, particles.c
 /* In native mode solveFrame takes sub-steps of min(max_substep_dt, the
  * Courant limit 0.7 h / max |v component|, the rest of the frame), with the
  * speed reduced on the device; flip_get_courant_dt returns that limit (0 at
- * rest). */
+ * rest).  With pressure_method 0 or 2 and stage timing off the whole frame is
+ * one CUDA graph launch: a conditional loop over sub-steps whose dt the
+ * device picks, each sub-step the graph of flip_step; the call synchronises
+ * once, at the end of the frame. */
 /* writePositionsToFile (particles.cu:817-828): "x, y, z" per line. */
 int flip_write_positions_csv(flip_engine* e, const char* path);
 /* Binary variant of the same frame (no reference counterpart): a 16-byte
@@ -264,8 +267,12 @@ int flip_write_positions_csv(flip_engine* e, const char* path);
 int flip_write_positions_bin(flip_engine* e, const char* path);
 
 /* One fixed-dt step of the whole path (bin, P2G, pressure, projection,
- * G2P + advection), asynchronous on the engine stream except for the
- * convergence reads of the pressure solve. */
+ * G2P + advection), asynchronous on the engine stream.  NATIVE with
+ * pressure_method 0 or 2 and stage timing off: one CUDA graph launch (captured
+ * on first use, with the solve's iteration loop and the Jacobi-PCG restart as
+ * conditional nodes); the host reads nothing back -- flip_get_info and
+ * flip_get_solve_info fetch the solve's outcome when called.  Otherwise the
+ * stages are launched one by one and the pressure solve synchronises. */
 int flip_step(flip_engine* e, double dt);
 int flip_sync(flip_engine* e);
 /* NATIVE, no reference counterpart: a host round trip per step.  Uploads
@@ -400,6 +407,10 @@ typedef struct {
                                 FLIP_ERR_TIMEOUT; bit 2: a tensor-core wait of the
                                 learned preconditioner timed out)                */
     uint32_t launches;       /* kernels this engine launched since creation      */
+    uint64_t solves;         /* NATIVE: pressure solves since setDomain           */
+    uint64_t fallbacks;      /* NATIVE: of those, flexible solves that missed tol
+                                and restarted Jacobi-PCG                          */
+    uint64_t pressure_iters_total; /* NATIVE: their iterations, restarts included */
 } flip_info;
 int flip_get_info(flip_engine* e, flip_info* out);
 /* Per-stage device times of flip_step (CUDA events on the engine stream).

@@ -978,12 +978,22 @@ int orc_nat_step_ex(int64_t n, float* pos, float* vel, const uint8_t* solid, con
         }
         double xm[3], gm[3];
         for (int c = 0; c < 3; ++c) { xm[c] = (double)pos[3 * p + c] + 0.5 * P->dt * un[c]; gm[c] = (xm[c] - lo[c]) / P->h; }
+        float xf[3];
         for (int c = 0; c < 3; ++c) {
             double um = nat_sample(P, U[c], c, gm[0], gm[1], gm[2]);
             double xn = (double)pos[3 * p + c] + P->dt * um;
             if (xn < lo[c] + eps) xn = lo[c] + eps;
             if (xn > hi[c] - eps) xn = hi[c] - eps;
-            pos[3 * p + c] = (float)xn;
+            xf[c] = (float)xn;
+        }
+        /* a particle that moved into an interior solid cell stays where it
+         * started the step and takes the solid's velocity */
+        if (solid && solid[nat_idx(P, nat_cell(xf[0], (float)P->ox, (float)P->h, P->nx),
+                                   nat_cell(xf[1], (float)P->oy, (float)P->h, P->ny),
+                                   nat_cell(xf[2], (float)P->oz, (float)P->h, P->nz))]) {
+            for (int c = 0; c < 3; ++c) vel[3 * p + c] = (float)us[c];
+        } else {
+            for (int c = 0; c < 3; ++c) pos[3 * p + c] = xf[c];
         }
     }
     if (info) { info->iters = it; info->rel_residual = rel; info->fluid_cells = nfluid; }
