@@ -176,7 +176,8 @@ def c5_learned(F, torch, dev, cells, steps=C5_STEPS, warmup=3):
             "pressure_iters_mean": (i1.pressure_iters_total - i0.pressure_iters_total) / max(1, solves),
             "fallback_rate": (i1.fallbacks - i0.fallbacks) / max(1, solves), "solves": solves,
             "last_rel_residual": i1.residual, "converged": i1.converged, "error_flags": i1.error_flags,
-            "kernel_launches_per_step": (i1.launches - i0.launches) / steps}
+            "kernel_launches_per_step": (i1.launches - i0.launches) / steps,
+            "graph_launched_steps": i1.graph_steps - i0.graph_steps}
 
 
 # ----------------------------------------------------- C3 binning microbenchmark
@@ -591,7 +592,8 @@ def main():
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
                 "pcg_iters_per_step": iters, "pressure_solve_ms": stages["pcg_setup"] + stages["pcg_iterations"],
                 "stages_ms": stages, "fluid_tiles": fluid_tiles,
-                "pcg_rel_residual": info.residual, "error_flags": info.error_flags}
+                "pcg_rel_residual": info.residual, "error_flags": info.error_flags,
+                "graph_steps": info.graph_steps}
         if c5:
             line["fallback_rate"] = fell_back / args.steps
         print(json.dumps(line), flush=True)

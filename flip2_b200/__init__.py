@@ -75,7 +75,7 @@ class Info(C.Structure):
     _fields_ = [("nodes", C.c_uint32), ("voxels", C.c_uint32), ("pressure_iters", C.c_int32), ("converged", C.c_int32),
                 ("dt", C.c_double), ("residual", C.c_double), ("elapsed_time", C.c_double), ("n", C.c_uint64),
                 ("error_flags", C.c_uint32), ("launches", C.c_uint32), ("solves", C.c_uint64),
-                ("fallbacks", C.c_uint64), ("pressure_iters_total", C.c_uint64)]
+                ("fallbacks", C.c_uint64), ("pressure_iters_total", C.c_uint64), ("graph_steps", C.c_uint64)]
 
 
 def lib():

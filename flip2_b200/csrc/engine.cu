@@ -9,6 +9,7 @@
 // native mode.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -92,6 +93,8 @@ struct flip_engine {
     cudaGraphExec_t step_graph = nullptr, frame_graph = nullptr;
     uint32_t step_graph_launches = 0;   // kernels of one captured step outside its loops
     float* cap_fp0 = nullptr;           // fp[0] when the graphs were captured (eager steps swap fp and fq)
+    bool cap_off = false;               // capturing failed here: steps run launch by launch
+    uint64_t graph_steps = 0;           // steps run as graph launches (flip_info)
     static constexpr int kCapStreams = 4;
     cudaStream_t cap_streams[kCapStreams] = {};
     int cap_depth = 0;
@@ -1161,6 +1164,34 @@ static int run_loop(flip_engine* e, cudaGraphExec_t g, uint32_t launches_per_chu
     return dev_err_eval(e);
 }
 
+// The Jacobi-PCG loop driven from the host, a chunk per launch sequence with
+// a state read after each: the same kernels as the loop graph, for profilers
+// that do not look inside conditional graph nodes (environment variable
+// FLIP2_HOST_SOLVE_LOOP=1; stage timing or the per-stage API only).
+static bool host_solve_loop() {
+    static const bool on = [] {
+        const char* v = std::getenv("FLIP2_HOST_SOLVE_LOOP");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+static int run_plain_host(flip_engine* e, int chunk, int max_iter) {
+    const int limit = loop_limit(max_iter, chunk);
+    for (int c = 0; c < limit; ++c) {
+        for (int k = 0; k < chunk; ++k)
+            E_TRY(nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err,
+                                            nat_grid(e, 4), e->stream));
+        E_TRY(nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
+        E_TRY(dev_err_fetch(e));
+        E_CUDA(cudaStreamSynchronize(e->stream));
+        e->launches += 2u * (uint32_t)chunk + 1u;
+        E_TRY(dev_err_eval(e));
+        if (e->h_state->done) break;
+    }
+    return FLIP_OK;
+}
+
 // Solve A x = b on the occupied tiles.  U: face velocities giving b = -div U,
 // or nullptr when b is already in pcg.b.  method 1 runs learned FPCG first and,
 // if it stops without meeting tol (iteration cap or a non-positive r.z),
@@ -1189,7 +1220,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(e->mark(9));
         E_TRY(nat_mgpcg_graph(e, chunk, max_learned, network));
         E_TRY(run_loop(e, e->mg_graph, (2u + mg_cycle_launches(e, network, true)) * (uint32_t)chunk + 1u));
-        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, 0, e->stream));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
@@ -1216,7 +1247,7 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         E_TRY(e->mark(9));
         E_TRY(nat_fpcg_graph(e, chunk, max_learned));
         E_TRY(run_loop(e, e->fpcg_graph, 7u * (uint32_t)chunk + 1u));
-        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, 0, e->stream));
         E_TRY(lp_check_err(e));
         const PcgState& s = *e->h_state;
         info.iters = s.iter;
@@ -1234,9 +1265,13 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
                                    e->type, e->pcg, e->stream, w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
         if (method == 0) E_TRY(e->mark(9));
-        E_TRY(nat_pcg_graph(e, chunk, max_plain));
-        E_TRY(run_loop(e, e->pcg_graph, 2u * (uint32_t)chunk + 1u));
-        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 0, method == 0 ? 0 : 1, e->stream));
+        if (host_solve_loop()) {
+            E_TRY(run_plain_host(e, chunk, max_plain));
+        } else {
+            E_TRY(nat_pcg_graph(e, chunk, max_plain));
+            E_TRY(run_loop(e, e->pcg_graph, 2u * (uint32_t)chunk + 1u));
+        }
+        E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 0, method == 0 ? 0 : 1, 0, e->stream));
         const PcgState& s = *e->h_state;
         if (method != 0) info.plain_iters = s.iter;
         else info.iters = s.iter;
@@ -1424,7 +1459,7 @@ static int cap_plain_solve(flip_engine* e, const float* const* U, bool warm, int
     E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU, e->type,
                                e->pcg, e->stream, warm ? e->cell_prev : nullptr));
     E_TRY(cap_loop(e, loop_limit(e->P.pcg_max_iter, chunk), [&]() { return cap_plain_chunk(e, chunk); }));
-    return nat_launch_solve_record(e->d_rec, e->pcg.st, 0, stage, e->stream);
+    return nat_launch_solve_record(e->d_rec, e->pcg.st, 0, stage, 1, e->stream);
 }
 // the pressure solve of a captured step (pressure_method 0 or 2)
 static int cap_solve(flip_engine* e) {
@@ -1440,7 +1475,7 @@ static int cap_solve(flip_engine* e) {
     E_TRY(mg_setup_problem(e, network));
     E_TRY(mg_cycle(e, network, &e->pcg.st->halt, 1));
     E_TRY(cap_loop(e, loop_limit(max_learned, chunk), [&]() { return cap_mg_chunk(e, chunk, network); }));
-    E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, e->stream));
+    E_TRY(nat_launch_solve_record(e->d_rec, e->pcg.st, 1, 0, 1, e->stream));
     // the flexible solve missed tol: Jacobi-PCG restarts from x = 0 on the same b
     cudaGraphConditionalHandle h;
     cudaGraph_t g = nullptr;
@@ -1534,8 +1569,21 @@ static int cap_build(flip_engine* e, bool frame) {
     return FLIP_OK;
 }
 static bool cap_supported(flip_engine* e) {
-    return e->P.mode == FLIP_MODE_NATIVE && !e->timing && (e->P.pressure_method == 0 || e->P.pressure_method == 2) &&
-           e->n > 0;
+    return e->P.mode == FLIP_MODE_NATIVE && !e->timing && !e->cap_off &&
+           (e->P.pressure_method == 0 || e->P.pressure_method == 2) && e->n > 0;
+}
+// a graph that cannot be captured or instantiated here (a driver without
+// some node type inside conditional bodies, a caller stream that cannot be
+// captured) is not an error of the step: the engine keeps stepping launch by
+// launch, with the same results
+static int cap_build_or_off(flip_engine* e, bool frame) {
+    const int rc = cap_build(e, frame);
+    if (rc == FLIP_OK) return FLIP_OK;
+    free_step_graphs(e);
+    e->cap_off = true;
+    e->err.clear();
+    (void)cudaGetLastError();
+    return rc;
 }
 // before a captured launch: the keys of the current positions, if the last
 // G2P did not write them
@@ -1557,13 +1605,15 @@ static int cap_launched(flip_engine* e, uint32_t steps) {
     return FLIP_OK;
 }
 // one step as a graph launch (no host round trip)
+static int nat_step(flip_engine* e, double dt);
 static int cap_step_launch(flip_engine* e, double dt) {
     if (e->fp[0] != e->cap_fp0) free_step_graphs(e);
-    if (!e->step_graph) E_TRY(cap_build(e, false));
+    if (!e->step_graph && cap_build_or_off(e, false) != FLIP_OK) return nat_step(e, dt);
     E_TRY(cap_keys(e));
     E_TRY(nat_launch_step_dt(e->d_frame, dt, e->P.gravity_y, e->stream));
     E_CUDA(cudaGraphLaunch(e->step_graph, e->stream));
     e->launches += 1;
+    e->graph_steps += 1;
     E_TRY(cap_launched(e, 1));
     e->dt = dt;
     e->elapsed += dt;
@@ -1595,19 +1645,20 @@ static int rec_refresh(flip_engine* e) {
     e->launches += (uint32_t)((r.chunks_primary - e->rec_chunks_counted[0]) * per_primary +
                               (r.chunks_plain - e->rec_chunks_counted[1]) * per_plain);
     // a restart runs the state, init, loop-condition and record kernels of its branch
-    e->launches += (uint32_t)(4u * (r.fallbacks - e->rec_fallbacks_counted));
+    e->launches += (uint32_t)(4u * (r.fallbacks_captured - e->rec_fallbacks_counted));
     e->rec_chunks_counted[0] = r.chunks_primary;
     e->rec_chunks_counted[1] = r.chunks_plain;
-    e->rec_fallbacks_counted = r.fallbacks;
+    e->rec_fallbacks_counted = r.fallbacks_captured;
     e->rec_pending = false;
     return FLIP_OK;
 }
 
 // a whole frame as one graph launch: the device takes sub-steps of
 // min(max_substep_dt, 0.7 h / max |v component|, the rest of the frame)
+static int eager_frame(flip_engine* e, double frameDt);
 static int cap_frame_launch(flip_engine* e, double frame_dt) {
     if (e->fp[0] != e->cap_fp0) free_step_graphs(e);
-    if (!e->frame_graph) E_TRY(cap_build(e, true));
+    if (!e->frame_graph && cap_build_or_off(e, true) != FLIP_OK) return eager_frame(e, frame_dt);
     E_TRY(cap_keys(e));
     E_TRY(nat_launch_frame_init(e->d_frame, frame_dt, e->P.max_substep_dt, (double)e->D.h, e->stream));
     E_CUDA(cudaGraphLaunch(e->frame_graph, e->stream));
@@ -1616,6 +1667,7 @@ static int cap_frame_launch(flip_engine* e, double frame_dt) {
     E_CUDA(cudaStreamSynchronize(e->stream));
     const FrameState f = *e->h_frame;
     e->launches += 2;  // frame init, graph
+    e->graph_steps += (uint64_t)f.substeps;
     E_TRY(cap_launched(e, (uint32_t)f.substeps));
     e->launches += 2u * (uint32_t)f.substeps;  // the speed reduction and the sub-step control
     E_TRY(dev_err_eval(e));
@@ -1750,7 +1802,12 @@ extern "C" int flip_solve_frame(flip_engine* e, double fps) {
     }
     const double frameDt = 1.0 / fps;
     if (cap_supported(e)) return cap_frame_launch(e, frameDt);
-    // sub-steps of min(max_substep_dt, the Courant limit, what is left of the frame)
+    return eager_frame(e, frameDt);
+}
+
+// a native frame launch by launch: sub-steps of min(max_substep_dt, the
+// Courant limit, what is left of the frame), the speed read back per sub-step
+static int eager_frame(flip_engine* e, double frameDt) {
     double t = 0.0;
     int guard = 0;
     while (frameDt - t > 1e-12 * frameDt) {
@@ -2011,6 +2068,7 @@ extern "C" int flip_get_info(flip_engine* e, flip_info* out) {
         E_CUDA(cudaMemcpy(&r, e->d_rec, sizeof(r), cudaMemcpyDeviceToHost));
         out->solves = r.solves;
         out->fallbacks = r.fallbacks;
+        out->graph_steps = e->graph_steps;
         out->pressure_iters_total = r.iters_total;
     }
     return FLIP_OK;

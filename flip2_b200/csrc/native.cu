@@ -101,29 +101,32 @@ __global__ void nat_gather_kernel(const uint32_t* __restrict__ perm, uint64_t n,
 }
 
 // ------------------------------------------------------------------ P2G
-// One CTA per occupied tile (persistent loop).  The tile's particles scatter
-// trilinear weights into a shared-memory box of 10^3 nodes per component
-// (the tile plus the one-node halo its stencils reach); the box is then
-// added to the global grids.  Also marks the cells that hold particles.
+// One CTA per occupied tile (persistent loop) accumulates the trilinear
+// weights (and weighted velocities) of the tile's particles into a
+// shared-memory box of 10^3 nodes per component -- the tile plus the
+// one-node halo its stencils reach -- and adds the box to the global grids;
+// it also marks the cells that hold particles.  Two forms:
 //
-// The box accumulates in one of two forms (P2GAcc):
-//   kAccF32: FP32 sums, updated with shared-memory float atomics;
-//   kAccFix64: 64-bit fixed point with 32 fraction bits, updated with
-//     shared-memory integer atomics.  A particle adds at most 1 to a weight
-//     sum and at most |v| to a momentum sum, so the sums stay far inside the
-//     signed 64-bit range; each term is rounded once (to 2^-33), the sums are
-//     exact and independent of the order of the atomics.
-enum P2GAcc { kAccF32 = 0, kAccFix64 = 1 };
+//   nat_p2g_cells_kernel (the one the step uses): a thread owns one cell of
+//   the tile.  The tile's particles are first sorted by cell inside the CTA
+//   (a counting sort in shared memory: one integer atomic per particle).
+//   Then each thread walks its cell's particles and keeps, per velocity
+//   component, the 2 x 3 x 3 node sums that any particle of that cell can
+//   reach in registers (36 floats: two nodes along the component's own axis,
+//   three along each staggered axis, where the stencil's base is the cell or
+//   the one below).  The sums go into the box in 18 phases, one node offset
+//   per phase, so that within a phase no two threads touch one node: plain
+//   shared-memory adds, no atomics.  FP32 sums, as the oracle's comparison
+//   assumes (relative precision even for the tiny weights of a node that only
+//   one far particle reaches; a fixed-point accumulator loses exactly those).
+//
+//   nat_p2g_scatter_kernel: a thread owns particles and adds each of their
+//   48 weighted terms with a shared-memory float atomic.
 constexpr int kP2GThreads = 256;
 constexpr int kBox = 10;
 constexpr int kBoxN = kBox * kBox * kBox;
-constexpr float kFix = 4294967296.0f;          // 2^32
-constexpr double kInvFix = 1.0 / 4294967296.0;
 
-template <int ACC>
-struct P2GBox;
-template <>
-struct P2GBox<kAccF32> {
+struct P2GScatterBox {
     float v[3][2][kBoxN];
     __device__ __forceinline__ void add(int c, int l, float w, float wv) {
         atomicAdd(&v[c][0][l], wv);
@@ -133,27 +136,14 @@ struct P2GBox<kAccF32> {
     __device__ __forceinline__ float wt(int c, int l) const { return v[c][1][l]; }
     __device__ __forceinline__ void clear(int l) { (&v[0][0][0])[l] = 0.0f; }
 };
-template <>
-struct P2GBox<kAccFix64> {
-    unsigned long long v[3][2][kBoxN];
-    __device__ __forceinline__ void add(int c, int l, float w, float wv) {
-        atomicAdd(&v[c][0][l], (unsigned long long)__float2ll_rn(wv * kFix));
-        atomicAdd(&v[c][1][l], (unsigned long long)__float2ll_rn(w * kFix));
-    }
-    __device__ __forceinline__ float mom(int c, int l) const { return (float)((double)(long long)v[c][0][l] * kInvFix); }
-    __device__ __forceinline__ float wt(int c, int l) const { return (float)((double)(long long)v[c][1][l] * kInvFix); }
-    __device__ __forceinline__ void clear(int l) { (&v[0][0][0])[l] = 0ull; }
-};
 
-template <int ACC>
-__global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
+__global__ void __launch_bounds__(kP2GThreads) nat_p2g_scatter_kernel(
     const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
     uint64_t n, const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
     const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, NatDims D,
     float* __restrict__ mu, float* __restrict__ mv, float* __restrict__ mw, float* __restrict__ wu,
     float* __restrict__ wv, float* __restrict__ ww, uint8_t* __restrict__ type) {
-    extern __shared__ __align__(16) unsigned char p2g_smem[];
-    P2GBox<ACC>& sm = *reinterpret_cast<P2GBox<ACC>*>(p2g_smem);
+    __shared__ P2GScatterBox sm;
     const uint32_t ntiles = *d_ntiles;
     float* gm[3] = {mu, mv, mw};
     float* gw[3] = {wu, wv, ww};
@@ -212,6 +202,173 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_kernel(
                 if (w != 0.0f) {
                     atomicAdd(gw[c] + s, w);
                     atomicAdd(gm[c] + s, sm.mom(c, l));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+constexpr int kPcThreads = 512;         // one thread per cell of the tile
+constexpr int kPcChunk = 8192;          // particles sorted per round (a denser tile takes several)
+constexpr int kPcPer = kPcChunk / kPcThreads;
+struct P2GCellSmem {
+    float m[3][kBoxN], w[3][kBoxN];     // the box: momentum and weight sums per component
+    uint32_t cnt[kPcThreads], off[kPcThreads];
+    uint16_t order[kPcChunk];           // particle (within the round) of each sorted slot
+    uint32_t scan[kPcThreads / 32 + 1];
+};
+
+__global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
+    const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
+    uint64_t n, const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
+    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, NatDims D,
+    float* __restrict__ mu, float* __restrict__ mv, float* __restrict__ mw, float* __restrict__ wu,
+    float* __restrict__ wv, float* __restrict__ ww, uint8_t* __restrict__ type) {
+    extern __shared__ __align__(16) unsigned char pc_smem[];
+    P2GCellSmem& S = *reinterpret_cast<P2GCellSmem*>(pc_smem);
+    const int tid = threadIdx.x;
+    const uint32_t ntiles = *d_ntiles;
+    const float* P[3] = {px, py, pz};
+    float* gm[3] = {mu, mv, mw};
+    float* gw[3] = {wu, wv, ww};
+    const float o[3] = {D.ox, D.oy, D.oz};
+    const int nn[3] = {D.nx, D.ny, D.nz};
+    const int lc[3] = {tid & 7, (tid >> 3) & 7, tid >> 6};  // this thread's cell in the tile
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        for (int l = tid; l < 3 * kBoxN; l += kPcThreads) {
+            (&S.m[0][0])[l] = 0.0f;
+            (&S.w[0][0])[l] = 0.0f;
+        }
+        const uint32_t key = tile_keys[t];
+        const int tc[3] = {(int)(key % D.tx), (int)((key / D.tx) % D.ty), (int)(key / (D.tx * D.ty))};
+        const int cell[3] = {8 * tc[0] + lc[0], 8 * tc[1] + lc[1], 8 * tc[2] + lc[2]};
+        const uint64_t start = starts[t];
+        const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
+        for (uint64_t r0 = start; r0 < end; r0 += kPcChunk) {
+            const uint32_t m = (uint32_t)min((uint64_t)kPcChunk, end - r0);
+            S.cnt[tid] = 0u;
+            __syncthreads();
+            // counting sort of the round's particles by cell
+            uint32_t slot[kPcPer];
+#pragma unroll
+            for (int i = 0; i < kPcPer; ++i) {
+                const uint32_t q = (uint32_t)(tid + kPcThreads * i);
+                slot[i] = 0xFFFFFFFFu;
+                if (q < m) {
+                    const uint64_t p = r0 + q;
+                    int c[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) c[a] = nat_cell(P[a][p], o[a], D.h, nn[a]);
+                    type[nslot(c[0], c[1], c[2], D)] = kFluid;
+                    // a particle of this tile's segment lies in one of its cells
+                    const int l0 = c[0] - 8 * tc[0], l1 = c[1] - 8 * tc[1], l2 = c[2] - 8 * tc[2];
+                    if ((unsigned)l0 < 8u && (unsigned)l1 < 8u && (unsigned)l2 < 8u) {
+                        const uint32_t cl = (uint32_t)(l0 + 8 * l1 + 64 * l2);
+                        slot[i] = cl | (atomicAdd(&S.cnt[cl], 1u) << 9);
+                    }
+                }
+            }
+            __syncthreads();
+            uint32_t total;
+            S.off[tid] = block_exclusive_scan<kPcThreads>(S.cnt[tid], S.scan, &total);
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < kPcPer; ++i)
+                if (slot[i] != 0xFFFFFFFFu)
+                    S.order[S.off[slot[i] & 511u] + (slot[i] >> 9)] = (uint16_t)(tid + kPcThreads * i);
+            __syncthreads();
+            const uint32_t b0 = S.off[tid], b1 = b0 + S.cnt[tid];
+#pragma unroll 1
+            for (int comp = 0; comp < 3; ++comp) {
+                // the component's own axis and the two others in order (a1 < a2)
+                const int no = comp == 0 ? D.nx : (comp == 1 ? D.ny : D.nz);
+                const int n1 = comp == 0 ? D.ny : D.nx, n2 = comp == 2 ? D.ny : D.nz;
+                const int c1 = comp == 0 ? cell[1] : cell[0], c2 = comp == 2 ? cell[1] : cell[2];
+                const float* __restrict__ vc = comp == 0 ? vx : (comp == 1 ? vy : vz);
+                float am[18], aw[18];
+#pragma unroll
+                for (int k = 0; k < 18; ++k) am[k] = aw[k] = 0.0f;
+                for (uint32_t j = b0; j < b1; ++j) {
+                    const uint64_t p = r0 + S.order[j];
+                    const float gx = __fdiv_rn(__fsub_rn(px[p], o[0]), D.h), gy = __fdiv_rn(__fsub_rn(py[p], o[1]), D.h),
+                                gz = __fdiv_rn(__fsub_rn(pz[p], o[2]), D.h);
+                    const float go = comp == 0 ? gx : (comp == 1 ? gy : gz);
+                    const float g1 = comp == 0 ? gy : gx, g2 = comp == 2 ? gy : gz;
+                    int b;
+                    float f;
+                    // own axis: the stencil's base is the cell itself; the wall
+                    // faces of this component take no weight
+                    nat_axis(go, no, b, f);
+                    const float wo0 = (b == 0) ? 0.0f : 1.0f - f, wo1 = (b + 1 == no) ? 0.0f : f;
+                    // staggered axes: the base is the cell or the one below
+                    float w1[3], w2[3];
+                    nat_axis(g1 - 0.5f, n1 - 1, b, f);
+                    {
+                        const bool below = b < c1;
+                        w1[0] = below ? 1.0f - f : 0.0f;
+                        w1[1] = below ? f : 1.0f - f;
+                        w1[2] = below ? 0.0f : f;
+                    }
+                    nat_axis(g2 - 0.5f, n2 - 1, b, f);
+                    {
+                        const bool below = b < c2;
+                        w2[0] = below ? 1.0f - f : 0.0f;
+                        w2[1] = below ? f : 1.0f - f;
+                        w2[2] = below ? 0.0f : f;
+                    }
+                    const float v = vc[p];
+#pragma unroll
+                    for (int d2 = 0; d2 < 3; ++d2)
+#pragma unroll
+                        for (int d1 = 0; d1 < 3; ++d1) {
+                            const float w12 = w1[d1] * w2[d2];
+                            const int k = 2 * (d1 + 3 * d2);
+                            const float wa = wo0 * w12, wb = wo1 * w12;
+                            aw[k] += wa;
+                            am[k] = fmaf(wa, v, am[k]);
+                            aw[k + 1] += wb;
+                            am[k + 1] = fmaf(wb, v, am[k + 1]);
+                        }
+                }
+                // 18 phases: in phase k every thread adds its node k; at one
+                // offset no two cells share a node.  Box origin: tile origin - 1.
+                const int lo = lc[comp == 0 ? 0 : (comp == 1 ? 1 : 2)] + 1;
+                const int l1 = comp == 0 ? lc[1] : lc[0], l2 = comp == 2 ? lc[1] : lc[2];
+                float* __restrict__ bm = S.m[comp];
+                float* __restrict__ bw = S.w[comp];
+#pragma unroll
+                for (int d2 = 0; d2 < 3; ++d2)
+#pragma unroll
+                    for (int d1 = 0; d1 < 3; ++d1)
+#pragma unroll
+                        for (int d0 = 0; d0 < 2; ++d0) {
+                            const int k = d0 + 2 * (d1 + 3 * d2);
+                            const int io = lo + d0, i1 = l1 + d1, i2 = l2 + d2;
+                            const int l = comp == 0 ? io + kBox * (i1 + kBox * i2)
+                                                    : (comp == 1 ? i1 + kBox * (io + kBox * i2) : i1 + kBox * (i2 + kBox * io));
+                            if (aw[k] != 0.0f) {
+                                bm[l] += am[k];
+                                bw[l] += aw[k];
+                            }
+                            __syncthreads();
+                        }
+            }
+        }
+        // the box onto the global grids (halo nodes are shared with the
+        // neighbouring tiles: atomics)
+        for (int l = tid; l < kBoxN; l += kPcThreads) {
+            const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
+            const int i = 8 * tc[0] - 1 + li, j = 8 * tc[1] - 1 + lj, k = 8 * tc[2] - 1 + lk;
+            if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) continue;
+            const uint32_t s = nslot(i, j, k, D);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float w = S.w[c][l];
+                if (w != 0.0f) {
+                    atomicAdd(gw[c] + s, w);
+                    atomicAdd(gm[c] + s, S.m[c][l]);
                 }
             }
         }
@@ -1248,19 +1405,25 @@ int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src,
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-// the accumulator form of the P2G box
-constexpr int kP2GAcc = kAccFix64;
+// the form of P2G the step uses: true = the cell-owned kernel (no atomics
+// in the accumulation), false = the float-atomic scatter
+constexpr bool kP2GCells = true;
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s) {
-    constexpr size_t smem = sizeof(P2GBox<kP2GAcc>);
-    static bool attr_done = false;
-    if (!attr_done) {
-        FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_p2g_kernel<kP2GAcc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_done = true;
+    if (kP2GCells) {
+        constexpr size_t smem = sizeof(P2GCellSmem);
+        static bool attr_done = false;
+        if (!attr_done) {
+            FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_p2g_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_done = true;
+        }
+        nat_p2g_cells_kernel<<<grid, kPcThreads, smem, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
+                                                            vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
+    } else {
+        nat_p2g_scatter_kernel<<<grid, kP2GThreads, 0, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
+                                                            vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
     }
-    nat_p2g_kernel<kP2GAcc><<<grid, kP2GThreads, smem, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
-                                                             vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1433,7 +1596,7 @@ int nat_launch_state_init(PcgState* st, double tol, int max_iter, int true_every
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-__global__ void solve_record_kernel(SolveRecord* rec, PcgState* st, int flexible, int stage) {
+__global__ void solve_record_kernel(SolveRecord* rec, PcgState* st, int flexible, int stage, int captured) {
     const double rr = st->true_checks ? st->rr_true : st->rr;
     const double rel = st->bb > 0.0 ? sqrt(rr / st->bb) : 0.0;
     const int conv = st->done == 1;
@@ -1444,18 +1607,21 @@ __global__ void solve_record_kernel(SolveRecord* rec, PcgState* st, int flexible
         rec->fell_back = flexible && !conv;
         rec->solves += 1;
         rec->fallbacks += (unsigned long long)(flexible && !conv);
-        if (flexible) rec->chunks_primary += (unsigned long long)st->chunks;
-        else rec->chunks_plain += (unsigned long long)st->chunks;
+        if (captured) {
+            if (flexible) rec->chunks_primary += (unsigned long long)st->chunks;
+            else rec->chunks_plain += (unsigned long long)st->chunks;
+            rec->fallbacks_captured += (unsigned long long)(flexible && !conv);
+        }
     } else {
         rec->plain_iters = st->iter;
-        rec->chunks_plain += (unsigned long long)st->chunks;
+        if (captured) rec->chunks_plain += (unsigned long long)st->chunks;
     }
     rec->converged = conv;
     rec->rel_residual = rel;
     rec->warm_ok = conv;
 }
-int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, cudaStream_t s) {
-    solve_record_kernel<<<1, 1, 0, s>>>(rec, st, flexible, stage);
+int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, int captured, cudaStream_t s) {
+    solve_record_kernel<<<1, 1, 0, s>>>(rec, st, flexible, stage, captured);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -73,7 +73,8 @@ struct SolveRecord {
     int pad;
     unsigned long long solves, fallbacks;        // since the counters were last cleared
     unsigned long long iters_total;              // iterations of every solve, restarts included
-    unsigned long long chunks_primary, chunks_plain;  // loop chunks run (the launch count)
+    unsigned long long chunks_primary, chunks_plain;  // loop chunks run in captured solves (the launch count)
+    unsigned long long fallbacks_captured;           // restarts inside captured solves (the launch count)
 };
 
 // Sub-step control of a captured frame: the device picks each sub-step's dt.
@@ -208,8 +209,9 @@ int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, c
 int nat_launch_state_init(PcgState* st, double tol, int max_iter, int true_every, int flexible, cudaStream_t s);
 // the solve's outcome into rec: stage 0 after the method asked for (method 0:
 // Jacobi-PCG; else the flexible solve, whose miss of tol is a fallback),
-// stage 1 after the Jacobi-PCG restart
-int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, cudaStream_t s);
+// stage 1 after the Jacobi-PCG restart; captured: the solve ran inside a
+// captured step (its loop chunks count towards the step's launches)
+int nat_launch_solve_record(SolveRecord* rec, PcgState* st, int flexible, int stage, int captured, cudaStream_t s);
 // sets a conditional node's condition value
 int nat_launch_cond_set(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t s);
 // condition of a conditional IF node: the flexible solve did not converge

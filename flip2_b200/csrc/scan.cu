@@ -43,33 +43,46 @@ static ScanLayout scan_layout(uint64_t n) {
 
 __device__ __forceinline__ int pad_idx(int j) { return j + (j >> 5); }
 
-// Decoupled look-back by one thread: publishes the tile aggregate, walks the
-// predecessors and returns the tile's exclusive prefix (u32, wrapping).
-__device__ __forceinline__ uint32_t lookback_u32(unsigned long long* status, uint32_t tile, uint32_t agg, uint32_t* err,
-                                                 uint32_t spin_limit) {
+// Decoupled look-back by one warp: publishes the tile's aggregate, then lane
+// l reads predecessor tile - 1 - l of a 32-tile window; the window is summed
+// once every tile up to the nearest inclusive prefix has published, and
+// slides back 32 tiles while it holds none.  Publishes and returns the tile's
+// exclusive prefix (u32, wrapping) on every lane.  A window reload counts as
+// one poll against spin_limit.
+__device__ __forceinline__ uint32_t lookback_warp_u32(unsigned long long* status, uint32_t tile, uint32_t agg,
+                                                      uint32_t* err, uint32_t spin_limit) {
+    const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        st_relaxed_u64(status, kStPrefix | agg);
+        if (lane == 0) st_relaxed_u64(status, kStPrefix | agg);
         return 0u;
     }
-    st_relaxed_u64(status + tile, kStAgg | agg);
-    uint32_t excl = 0;
-    int64_t t = (int64_t)tile - 1;
-    uint32_t spins = 0;
-    while (t >= 0) {
-        unsigned long long s = ld_relaxed_u64(status + t);
-        unsigned long long f = s & kStFlags;
-        if (f == 0ull) {
+    if (lane == 0) st_relaxed_u64(status + tile, kStAgg | agg);
+    uint32_t excl = 0, spins = 0;
+    bool timed_out = false;
+    int64_t end = (int64_t)tile - 1;
+    while (true) {
+        const int64_t t = end - lane;
+        const unsigned long long s = t >= 0 ? ld_relaxed_u64(status + t) : kStPrefix;
+        const unsigned long long f = s & kStFlags;
+        const uint32_t pre = __ballot_sync(0xffffffffu, f == kStPrefix);
+        const uint32_t unset = __ballot_sync(0xffffffffu, f == 0ull);
+        const int first = pre ? __ffs(pre) - 1 : 31;  // lanes 0 .. first are summed
+        const uint32_t need = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if (unset & need) {
             if (++spins > spin_limit) {
-                atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
+                timed_out = true;
                 break;
             }
             continue;
         }
-        excl += (uint32_t)s;
-        if (f == kStPrefix) break;
-        --t;
+        excl += warp_sum<uint32_t>(lane <= first ? (uint32_t)s : 0u);
+        if (pre) break;
+        end -= 32;
     }
-    st_relaxed_u64(status + tile, kStPrefix | (uint32_t)(excl + agg));
+    if (lane == 0) {
+        if (timed_out) atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
+        st_relaxed_u64(status + tile, kStPrefix | (uint32_t)(excl + agg));
+    }
     return excl;
 }
 
@@ -116,7 +129,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const uint32_t* __re
     }
     uint32_t agg;
     uint32_t texcl = block_exclusive_scan<kScanThreads>(sum, s_scan, &agg);
-    if (tid == 0) s_excl = lookback_u32(status, tile, agg, err, spin_limit);
+    if (tid < 32) {
+        const uint32_t e = lookback_warp_u32(status, tile, agg, err, spin_limit);
+        if (tid == 0) s_excl = e;
+    }
     __syncthreads();
     const uint32_t pre = s_excl + texcl;
     if (MODE == 0) {

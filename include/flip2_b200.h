@@ -411,6 +411,7 @@ typedef struct {
     uint64_t fallbacks;      /* NATIVE: of those, flexible solves that missed tol
                                 and restarted Jacobi-PCG                          */
     uint64_t pressure_iters_total; /* NATIVE: their iterations, restarts included */
+    uint64_t graph_steps;    /* NATIVE: steps that ran as CUDA graph launches     */
 } flip_info;
 int flip_get_info(flip_engine* e, flip_info* out);
 /* Per-stage device times of flip_step (CUDA events on the engine stream).

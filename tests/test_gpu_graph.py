@@ -55,6 +55,7 @@ def test_captured_steps_match_stage_by_stage(torch, method):
     (pe, ve), ie, _ = run(pos, vel, nc, 6, True, pressure_method=method)
     (pg, vg), ig, info = run(pos, vel, nc, 6, False, pressure_method=method)
     assert info.solves == 6
+    assert info.graph_steps == 6  # every step ran as one graph launch
     # the same kernels on the same data: iteration counts agree (float
     # atomics may reorder sums, so allow one chunk of slack) and the particles
     # agree far inside the parity tolerance against the FP64 oracle
@@ -77,7 +78,7 @@ def test_captured_restart_branch(torch):
     s = P.solve_info()
     info = P.info()
     assert s.fell_back == 1 and s.plain_iters > 0 and s.converged == 1 and s.rel_residual <= 1e-6
-    assert info.solves == 3 and info.fallbacks == 3
+    assert info.solves == 3 and info.fallbacks == 3 and info.graph_steps == 3
     P.close()
 
 
@@ -105,5 +106,6 @@ def test_captured_frame_matches_stage_by_stage(torch):
     (pg, vg), ig = res[False]
     assert abs(ie.elapsed_time - 2.0 / 24.0) < 1e-12 and abs(ig.elapsed_time - 2.0 / 24.0) < 1e-12
     assert ie.solves == ig.solves >= 20  # at least max_substep_dt's ten sub-steps per frame
+    assert ie.graph_steps == 0 and ig.graph_steps == ig.solves  # the captured frames ran every sub-step
     assert np.max(np.abs(pe - pg)) < 1e-4 / nc
     assert pg[:, 1].mean() < pos[:, 1].mean()
