@@ -74,7 +74,6 @@ struct flip_engine {
     // the grids G2P stages by TMA, through the descriptors in g2p_maps
     float *ulin[3] = {}, *olin[3] = {};
     NatG2PMaps g2p_maps{};
-    PcgMaps pcg_maps{};  // TMA descriptors of the Jacobi-PCG vectors (pcg_tma.cu)
     // keys[p] holds the tile key of particle p's current position (G2P writes
     // them for the next step; uploads invalidate them)
     bool keys_valid = false;
@@ -377,6 +376,7 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         D.tx = D.nx / 8; D.ty = D.ny / 8; D.tz = D.nz / 8;
         D.ox = e->grid.negX; D.oy = e->grid.negY; D.oz = e->grid.negZ;
         D.h = e->grid.cellSize / 4.0f;
+        D.inv_h = 1.0f / D.h;
         e->ntiles_total = (uint64_t)D.tx * D.ty * D.tz;
         e->nslots = e->ntiles_total * 512;
         if (e->nslots >= (1ull << 32)) return e->fail(FLIP_ERR_ARG, "flip_set_domain: grid above 2^32 voxels");
@@ -421,7 +421,6 @@ extern "C" int flip_set_domain(flip_engine* e, double nx, double ny, double nz, 
         E_CUDA(cudaMemsetAsync(e->arena, 0, total, e->stream));
         E_CUDA(cudaStreamSynchronize(e->stream));
         E_TRY(nat_make_g2p_maps(e->g2p_maps, e->ulin, e->olin, e->D));
-        E_TRY(nat_make_pcg_maps(e->pcg_maps, e->pcg, e->ntiles_total));
         e->pcg.warm_ok = &e->d_rec->warm_ok;
     }
     e->keys_valid = false;
@@ -857,9 +856,8 @@ static int nat_pcg_graph(flip_engine* e, int iters, int max_iter) {
     E_TRY(build_loop_graph(e, [&]() {
         int rc = FLIP_OK;
         for (int k = 0; k < iters && rc == FLIP_OK; ++k)
-            rc = nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err,
-                                           nat_grid(e, 4), e->stream);
-        if (rc == FLIP_OK) rc = nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
         return rc;
     }, limit, &e->pcg_graph));
     e->pcg_graph_iters = iters;
@@ -1178,10 +1176,8 @@ static bool host_solve_loop() {
 static int run_plain_host(flip_engine* e, int chunk, int max_iter) {
     const int limit = loop_limit(max_iter, chunk);
     for (int c = 0; c < limit; ++c) {
-        for (int k = 0; k < chunk; ++k)
-            E_TRY(nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err,
-                                            nat_grid(e, 4), e->stream));
-        E_TRY(nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_TRY(nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
         E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
         E_TRY(dev_err_fetch(e));
         E_CUDA(cudaStreamSynchronize(e->stream));
@@ -1261,8 +1257,8 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         pcg_state_host(e, tol, max_plain, 0);
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
         const bool w = warm && method == 0;
-        E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU,
-                                   e->type, e->pcg, e->stream, w ? e->cell_prev : nullptr));
+        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
+                                  w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
         if (method == 0) E_TRY(e->mark(9));
         if (host_solve_loop()) {
@@ -1436,10 +1432,8 @@ static int cap_loop(flip_engine* e, int limit, Fn body) {
     });
 }
 static int cap_plain_chunk(flip_engine* e, int chunk) {
-    for (int k = 0; k < chunk; ++k)
-        E_TRY(nat_launch_pcgw_iteration(e->pcg_maps, e->node_keys, e->d_counts, e->D, e->pcg, e->d_err, nat_grid(e, 4),
-                                        e->stream));
-    return nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+    for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+    return nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
 }
 static int cap_mg_chunk(flip_engine* e, int chunk, bool network) {
     const int* halt = &e->pcg.st->halt;
@@ -1456,8 +1450,8 @@ static int cap_plain_solve(flip_engine* e, const float* const* U, bool warm, int
     const int chunk = e->P.pcg_check_every;
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
     E_TRY(nat_launch_state_init(e->pcg.st, e->P.pcg_tol, e->P.pcg_max_iter, e->P.true_residual_every, 0, e->stream));
-    E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU, e->type,
-                               e->pcg, e->stream, warm ? e->cell_prev : nullptr));
+    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
+                              warm ? e->cell_prev : nullptr));
     E_TRY(cap_loop(e, loop_limit(e->P.pcg_max_iter, chunk), [&]() { return cap_plain_chunk(e, chunk); }));
     return nat_launch_solve_record(e->d_rec, e->pcg.st, 0, stage, 1, e->stream);
 }
@@ -1535,7 +1529,10 @@ static uint32_t cap_step_launches(flip_engine* e) {
 // each taking its dt from the device-side Courant rule)
 static int cap_build(flip_engine* e, bool frame) {
     if (e->P.pressure_method == 2) E_TRY(mg_ready(e, e->P.mg_coarse == 0));
-    const uint32_t launches = e->launches;  // the launchers count at capture time: restored below
+    // the launchers count, and the G2P stage marks the keys valid, at capture
+    // time: both are restored below (the first launch still needs its keys)
+    const uint32_t launches = e->launches;
+    const bool keys_valid = e->keys_valid;
     cudaGraph_t g = nullptr;
     E_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
     int rc = FLIP_OK;
@@ -1555,6 +1552,7 @@ static int cap_build(flip_engine* e, bool frame) {
     }
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
     e->launches = launches;
+    e->keys_valid = keys_valid;
     if (rc != FLIP_OK) {
         if (g) cudaGraphDestroy(g);
         return rc;

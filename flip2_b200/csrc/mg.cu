@@ -578,6 +578,7 @@ int mg_plan(int nx, int ny, int nz, float h, MgLevel* L, int max_levels) {
         l.D.tx = l.D.nx / 8; l.D.ty = l.D.ny / 8; l.D.tz = l.D.nz / 8;
         l.D.ox = l.D.oy = l.D.oz = 0.0f;
         l.D.h = hl;
+        l.D.inv_h = 1.0f / hl;
         l.ntiles = (uint32_t)(l.D.tx * l.D.ty * l.D.tz);
         ++levels;
         if (ex <= kMgCoarsest && ey <= kMgCoarsest && ez <= kMgCoarsest) break;

@@ -30,9 +30,11 @@ __device__ __forceinline__ int nat_cell_g(float g, int n) {
     if (!(t > 0.0f)) c = 0;
     return c;
 }
-__device__ __forceinline__ int nat_cell(float p, float o, float h, int n) {
-    return nat_cell_g(__fdiv_rn(__fsub_rn(p, o), h), n);
-}
+// grid coordinate of a position on one axis; the one form every kernel uses
+// for cells, keys and stencils, so that they agree on which cell holds a
+// particle (exact, like a division, when h is a power of two)
+__device__ __forceinline__ float nat_grid_coord(float p, float o, float inv_h) { return __fmul_rn(__fsub_rn(p, o), inv_h); }
+__device__ __forceinline__ int nat_cell(float p, float o, float inv_h, int n) { return nat_cell_g(nat_grid_coord(p, o, inv_h), n); }
 __device__ __forceinline__ uint8_t nat_type(const uint8_t* type, int i, int j, int k, const NatDims& D) {
     if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return kSolid;
     return type[nslot(i, j, k, D)];
@@ -57,32 +59,13 @@ __device__ __forceinline__ bool nat_wall(int c, int i, int j, int k, const NatDi
     if (c == 1) return j == 0 || j == D.ny;
     return k == 0 || k == D.nz;
 }
-__device__ __forceinline__ float nat_sample(const float* __restrict__ f, int c, float gx, float gy, float gz,
-                                            const NatDims& D) {
-    int i0, j0, k0;
-    float fx, fy, fz;
-    nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
-    float s = 0.0f;
-#pragma unroll
-    for (int dk = 0; dk < 2; ++dk)
-#pragma unroll
-        for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-            for (int di = 0; di < 2; ++di) {
-                int i = i0 + di, j = j0 + dj, k = k0 + dk;
-                if (nat_wall(c, i, j, k, D)) continue;
-                float w = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) * (dk ? fz : 1.0f - fz);
-                s = fmaf(w, __ldg(f + nslot(i, j, k, D)), s);
-            }
-    return s;
-}
 
 // ------------------------------------------------------------- binning
 __global__ void nat_keys_kernel(const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
                                 uint64_t n, NatDims D, uint32_t* __restrict__ keys) {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    int i = nat_cell(px[p], D.ox, D.h, D.nx), j = nat_cell(py[p], D.oy, D.h, D.ny), k = nat_cell(pz[p], D.oz, D.h, D.nz);
+    int i = nat_cell(px[p], D.ox, D.inv_h, D.nx), j = nat_cell(py[p], D.oy, D.inv_h, D.ny), k = nat_cell(pz[p], D.oz, D.inv_h, D.nz);
     keys[p] = (uint32_t)((i >> 3) + D.tx * ((j >> 3) + D.ty * (k >> 3)));
 }
 
@@ -156,8 +139,8 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_scatter_kernel(
         const uint32_t start = starts[t];
         const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
         for (uint64_t p = start + threadIdx.x; p < end; p += kP2GThreads) {
-            const float gx = __fdiv_rn(__fsub_rn(px[p], D.ox), D.h), gy = __fdiv_rn(__fsub_rn(py[p], D.oy), D.h),
-                        gz = __fdiv_rn(__fsub_rn(pz[p], D.oz), D.h);
+            const float gx = nat_grid_coord(px[p], D.ox, D.inv_h), gy = nat_grid_coord(py[p], D.oy, D.inv_h),
+                        gz = nat_grid_coord(pz[p], D.oz, D.inv_h);
             type[nslot(nat_cell_g(gx, D.nx), nat_cell_g(gy, D.ny), nat_cell_g(gz, D.nz), D)] = kFluid;
             const float v[3] = {vx[p], vy[p], vz[p]};
 #pragma unroll
@@ -211,10 +194,11 @@ __global__ void __launch_bounds__(kP2GThreads) nat_p2g_scatter_kernel(
 
 
 constexpr int kPcThreads = 512;         // one thread per cell of the tile
-constexpr int kPcChunk = 8192;          // particles sorted per round (a denser tile takes several)
+constexpr int kPcChunk = 4096;          // particles sorted per round (a denser tile takes several)
 constexpr int kPcPer = kPcChunk / kPcThreads;
 struct P2GCellSmem {
     float m[3][kBoxN], w[3][kBoxN];     // the box: momentum and weight sums per component
+    float g[3][kPcChunk];               // grid coordinates of each sorted slot's particle
     uint32_t cnt[kPcThreads], off[kPcThreads];
     uint16_t order[kPcChunk];           // particle (within the round) of each sorted slot
     uint32_t scan[kPcThreads / 32 + 1];
@@ -260,7 +244,7 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
                     const uint64_t p = r0 + q;
                     int c[3];
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) c[a] = nat_cell(P[a][p], o[a], D.h, nn[a]);
+                    for (int a = 0; a < 3; ++a) c[a] = nat_cell(P[a][p], o[a], D.inv_h, nn[a]);
                     type[nslot(c[0], c[1], c[2], D)] = kFluid;
                     // a particle of this tile's segment lies in one of its cells
                     const int l0 = c[0] - 8 * tc[0], l1 = c[1] - 8 * tc[1], l2 = c[2] - 8 * tc[2];
@@ -274,10 +258,17 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
             uint32_t total;
             S.off[tid] = block_exclusive_scan<kPcThreads>(S.cnt[tid], S.scan, &total);
             __syncthreads();
+            // the sorted slots: particle index and grid coordinates (the same
+            // form nat_cell used above), so that the three component passes
+            // below read them from shared memory
 #pragma unroll
             for (int i = 0; i < kPcPer; ++i)
-                if (slot[i] != 0xFFFFFFFFu)
-                    S.order[S.off[slot[i] & 511u] + (slot[i] >> 9)] = (uint16_t)(tid + kPcThreads * i);
+                if (slot[i] != 0xFFFFFFFFu) {
+                    const uint32_t q = (uint32_t)(tid + kPcThreads * i), at = S.off[slot[i] & 511u] + (slot[i] >> 9);
+                    S.order[at] = (uint16_t)q;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) S.g[a][at] = nat_grid_coord(P[a][r0 + q], o[a], D.inv_h);
+                }
             __syncthreads();
             const uint32_t b0 = S.off[tid], b1 = b0 + S.cnt[tid];
 #pragma unroll 1
@@ -292,8 +283,7 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
                 for (int k = 0; k < 18; ++k) am[k] = aw[k] = 0.0f;
                 for (uint32_t j = b0; j < b1; ++j) {
                     const uint64_t p = r0 + S.order[j];
-                    const float gx = __fdiv_rn(__fsub_rn(px[p], o[0]), D.h), gy = __fdiv_rn(__fsub_rn(py[p], o[1]), D.h),
-                                gz = __fdiv_rn(__fsub_rn(pz[p], o[2]), D.h);
+                    const float gx = S.g[0][j], gy = S.g[1][j], gz = S.g[2][j];
                     const float go = comp == 0 ? gx : (comp == 1 ? gy : gz);
                     const float g1 = comp == 0 ? gy : gx, g2 = comp == 2 ? gy : gz;
                     int b;
@@ -643,11 +633,6 @@ __device__ __forceinline__ float jacobi_inv_s(const float* tab, uint8_t c) { ret
 // cell_prev (warm start): the previous solve's cell codes; x starts from the
 // previous solution (x + xg) on cells that are fluid in both solves, 0
 // elsewhere, and pcg_warm_kernel then replaces r = b by b - A x
-// W (the TMA Jacobi-PCG of pcg_tma.cu): the residual is kept Jacobi-scaled,
-// w = D^-1 r, and the tiles walked are the dilated list, so that w and both
-// direction buffers are also zero on the non-fluid cells around the fluid
-// (the halo reads of that solver take no cell codes)
-template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
@@ -686,9 +671,8 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     B.x[s] = x0;
     B.xg[s] = 0.0f;
     const float z = b * jacobi_inv(code);
-    B.r[s] = W ? ((code & kCellFluid) ? __fdiv_rn(b, (float)(code & 7u)) : 0.0f) : b;
+    B.r[s] = b;
     B.p0[s] = 0.0f;
-    if (W) B.p1[s] = 0.0f;
     bb += (double)b * (double)b;
     rz += (double)b * (double)z;
     NAT_TILE_LOOP_END
@@ -1030,7 +1014,6 @@ __global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32
 // iterations.  Replaces r, decides convergence on the true value and asks
 // the next direction kernel to fold xg into x.  The FP64 solution of the tile
 // and its halo is staged in shared memory like the matvec.
-template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __restrict__ tiles,
                                                             const uint32_t* __restrict__ tcoord,
                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -1066,15 +1049,9 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
             rr += res * res;
-            if (W) {
-                const float ws = (float)(res / (double)(c & 7u));
-                r[s] = ws;
-                rz += (double)(c & 7u) * (double)ws * (double)ws;
-            } else {
-                const float rs = (float)res;
-                r[s] = rs;
-                rz += (double)rs * (double)(rs * jacobi_inv(c));
-            }
+            const float rs = (float)res;
+            r[s] = rs;
+            rz += (double)rs * (double)(rs * jacobi_inv(c));
         }
         __syncthreads();
     }
@@ -1107,7 +1084,6 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
 // warm start: r = b - A x in FP64 for the initial guess, r.r and r.z, and
 // the state for the first iteration (converged already if |r| <= tol |b|;
 // b = 0 gives x = 0)
-template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __restrict__ tiles,
                                                            const uint32_t* __restrict__ tcoord,
                                                            const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -1145,15 +1121,9 @@ __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __rest
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
             rr += res * res;
-            if (W) {
-                const float ws = (float)(res / (double)(c & 7u));
-                r[s] = ws;
-                rz += (double)(c & 7u) * (double)ws * (double)ws;
-            } else {
-                const float rs = (float)res;
-                r[s] = rs;
-                rz += (double)rs * (double)(rs * jacobi_inv(c));
-            }
+            const float rs = (float)res;
+            r[s] = rs;
+            rz += (double)rs * (double)(rs * jacobi_inv(c));
         }
         __syncthreads();
     }
@@ -1270,24 +1240,61 @@ constexpr uint32_t kGBoxBytes = kGBoxN * sizeof(float);        // 9216 B
 constexpr uint32_t kG2PSmem = 6 * kGBoxBytes + 128;            // six boxes + the mbarrier
 constexpr uint32_t kG2PSpinLimit = 1u << 24;
 
-// trilinear sample of component c's box (origin bx0, by0, bz0) at grid
-// coordinates g; false when the stencil leaves the box
-__device__ __forceinline__ bool box_sample(const float* __restrict__ B, int c, float gx, float gy, float gz,
-                                           const NatDims& D, int bx0, int by0, int bz0, float& out) {
-    int i0, j0, k0;
-    float fx, fy, fz;
-    nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
-    const int li = i0 - bx0, lj = j0 - by0, lk = k0 - bz0;
-    if ((unsigned)li >= (unsigned)(kGBx - 1) || (unsigned)lj >= (unsigned)(kGBy - 1) || (unsigned)lk >= (unsigned)(kGBz - 1))
-        return false;
-    const float* b = B + li + kGBx * (lj + kGBy * lk);
+// The stencils of one position: per axis the face-aligned base and weight
+// (the component's own axis) and the cell-centred ones (the two others), so
+// that the three components and both grids share six nat_axis evaluations.
+struct PosStencil {
+    int fi[3], ci[3];
+    float ff[3], cf[3];
+};
+__device__ __forceinline__ void pos_stencil(const float (&g)[3], const NatDims& D, PosStencil& S) {
+    const int nn[3] = {D.nx, D.ny, D.nz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        nat_axis(g[a], nn[a], S.fi[a], S.ff[a]);
+        nat_axis(g[a] - 0.5f, nn[a] - 1, S.ci[a], S.cf[a]);
+    }
+}
+// trilinear interpolation of a 2 x 2 x 2 block of a box (b: its lowest corner)
+__device__ __forceinline__ float box_lerp(const float* __restrict__ b, float fx, float fy, float fz) {
     const float c00 = fmaf(fx, b[1] - b[0], b[0]);
     const float c10 = fmaf(fx, b[kGBx + 1] - b[kGBx], b[kGBx]);
     const float c01 = fmaf(fx, b[kGBx * kGBy + 1] - b[kGBx * kGBy], b[kGBx * kGBy]);
     const float c11 = fmaf(fx, b[kGBx * kGBy + kGBx + 1] - b[kGBx * kGBy + kGBx], b[kGBx * kGBy + kGBx]);
     const float c0 = fmaf(fy, c10 - c00, c00), c1 = fmaf(fy, c11 - c01, c01);
-    out = fmaf(fz, c1 - c0, c0);
-    return true;
+    return fmaf(fz, c1 - c0, c0);
+}
+// component c's stencil from S: base (i0, j0, k0) and weights, and its
+// offset in a box of origin (bx0, by0, bz0); false when it leaves the box
+__device__ __forceinline__ bool comp_stencil(const PosStencil& S, int c, int bx0, int by0, int bz0, int& i0, int& j0,
+                                             int& k0, float& fx, float& fy, float& fz, int& off) {
+    i0 = c == 0 ? S.fi[0] : S.ci[0];
+    j0 = c == 1 ? S.fi[1] : S.ci[1];
+    k0 = c == 2 ? S.fi[2] : S.ci[2];
+    fx = c == 0 ? S.ff[0] : S.cf[0];
+    fy = c == 1 ? S.ff[1] : S.cf[1];
+    fz = c == 2 ? S.ff[2] : S.cf[2];
+    const int li = i0 - bx0, lj = j0 - by0, lk = k0 - bz0;
+    off = li + kGBx * (lj + kGBy * lk);
+    return (unsigned)li < (unsigned)(kGBx - 1) && (unsigned)lj < (unsigned)(kGBy - 1) && (unsigned)lk < (unsigned)(kGBz - 1);
+}
+// the same interpolation from global memory (wall faces take no weight), for
+// a stencil outside the box
+__device__ __forceinline__ float nat_sample_at(const float* __restrict__ f, int c, int i0, int j0, int k0, float fx, float fy,
+                                               float fz, const NatDims& D) {
+    float s = 0.0f;
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+            for (int di = 0; di < 2; ++di) {
+                const int i = i0 + di, j = j0 + dj, k = k0 + dk;
+                if (nat_wall(c, i, j, k, D)) continue;
+                const float w = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) * (dk ? fz : 1.0f - fz);
+                s = fmaf(w, __ldg(f + nslot(i, j, k, D)), s);
+            }
+    return s;
 }
 
 __global__ void __launch_bounds__(kG2PThreads) nat_g2p_tile_kernel(
@@ -1338,32 +1345,45 @@ __global__ void __launch_bounds__(kG2PThreads) nat_g2p_tile_kernel(
         for (uint64_t p = start + threadIdx.x; p < end; p += kG2PThreads) {
             float X[3] = {px[p], py[p], pz[p]};
             float V[3] = {vx[p], vy[p], vz[p]};
-            float g[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) g[c] = __fdiv_rn(__fsub_rn(X[c], o[c]), D.h);
+            PosStencil S;
+            {
+                const float g[3] = {nat_grid_coord(X[0], o[0], D.inv_h), nat_grid_coord(X[1], o[1], D.inv_h),
+                                    nat_grid_coord(X[2], o[2], D.inv_h)};
+                pos_stencil(g, D, S);
+            }
             float un[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 // the stencils of a particle of this tile lie inside the box;
                 // the global reads only guard against a position the binning
-                // did not see
-                float uo;
-                if (!box_sample(box + c * kGBoxN, c, g[0], g[1], g[2], D, bx0, by0, bz0, un[c]))
-                    un[c] = nat_sample(G[c], c, g[0], g[1], g[2], D);
-                if (!box_sample(box + (3 + c) * kGBoxN, c, g[0], g[1], g[2], D, bx0, by0, bz0, uo))
-                    uo = nat_sample(GO[c], c, g[0], g[1], g[2], D);
+                // did not see.  The new and the old grid share the stencil.
+                int i0, j0, k0, off;
+                float fx, fy, fz, uo;
+                if (comp_stencil(S, c, bx0, by0, bz0, i0, j0, k0, fx, fy, fz, off)) {
+                    un[c] = box_lerp(box + c * kGBoxN + off, fx, fy, fz);
+                    uo = box_lerp(box + (3 + c) * kGBoxN + off, fx, fy, fz);
+                } else {
+                    un[c] = nat_sample_at(G[c], c, i0, j0, k0, fx, fy, fz, D);
+                    uo = nat_sample_at(GO[c], c, i0, j0, k0, fx, fy, fz, D);
+                }
                 const float vf = V[c] + (un[c] - uo);
                 V[c] = flip * vf + (1.0f - flip) * un[c];
             }
-            float gm[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) gm[c] = __fdiv_rn(__fsub_rn(fmaf(0.5f * dt, un[c], X[c]), o[c]), D.h);
+            {
+                const float gm[3] = {nat_grid_coord(fmaf(0.5f * dt, un[0], X[0]), o[0], D.inv_h),
+                                     nat_grid_coord(fmaf(0.5f * dt, un[1], X[1]), o[1], D.inv_h),
+                                     nat_grid_coord(fmaf(0.5f * dt, un[2], X[2]), o[2], D.inv_h)};
+                pos_stencil(gm, D, S);
+            }
             float Xn[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                float um;
-                if (!box_sample(box + c * kGBoxN, c, gm[0], gm[1], gm[2], D, bx0, by0, bz0, um))
-                    um = nat_sample(G[c], c, gm[0], gm[1], gm[2], D);
+                int i0, j0, k0, off;
+                float fx, fy, fz, um;
+                if (comp_stencil(S, c, bx0, by0, bz0, i0, j0, k0, fx, fy, fz, off))
+                    um = box_lerp(box + c * kGBoxN + off, fx, fy, fz);
+                else
+                    um = nat_sample_at(G[c], c, i0, j0, k0, fx, fy, fz, D);
                 const float xn = fmaf(dt, um, X[c]);
                 const float lo = o[c] + eps, hi = o[c] + (float)nn[c] * D.h - eps;
                 Xn[c] = fminf(fmaxf(xn, lo), hi);
@@ -1371,8 +1391,8 @@ __global__ void __launch_bounds__(kG2PThreads) nat_g2p_tile_kernel(
             // a particle moved into an interior solid cell goes back to where
             // it started the step (a non-solid cell) and moves with the solid
             if (solid_type &&
-                solid_type[nslot(nat_cell(Xn[0], D.ox, D.h, D.nx), nat_cell(Xn[1], D.oy, D.h, D.ny),
-                                 nat_cell(Xn[2], D.oz, D.h, D.nz), D)] == kSolid) {
+                solid_type[nslot(nat_cell(Xn[0], D.ox, D.inv_h, D.nx), nat_cell(Xn[1], D.oy, D.inv_h, D.ny),
+                                 nat_cell(Xn[2], D.oz, D.inv_h, D.nz), D)] == kSolid) {
                 V[0] = usolid.x; V[1] = usolid.y; V[2] = usolid.z;
             } else {
                 X[0] = Xn[0]; X[1] = Xn[1]; X[2] = Xn[2];
@@ -1380,8 +1400,8 @@ __global__ void __launch_bounds__(kG2PThreads) nat_g2p_tile_kernel(
             qx[p] = X[0]; qy[p] = X[1]; qz[p] = X[2];
             wx[p] = V[0]; wy[p] = V[1]; wz[p] = V[2];
             if (keys_out) {
-                const int ci = nat_cell(X[0], D.ox, D.h, D.nx), cj = nat_cell(X[1], D.oy, D.h, D.ny),
-                          ck = nat_cell(X[2], D.oz, D.h, D.nz);
+                const int ci = nat_cell(X[0], D.ox, D.inv_h, D.nx), cj = nat_cell(X[1], D.oy, D.inv_h, D.ny),
+                          ck = nat_cell(X[2], D.oz, D.inv_h, D.nz);
                 keys_out[p] = (uint32_t)((ci >> 3) + D.tx * ((cj >> 3) + D.ty * (ck >> 3)));
             }
         }
@@ -1504,10 +1524,10 @@ int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const N
 }
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
-    pcg_init_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
+    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
     if (cell_prev)
-        pcg_warm_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
-                                                          B.partials);
+        pcg_warm_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
+                                                   B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1548,27 +1568,8 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
 }
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s) {
-    pcg_check_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
-                                                       B.partials);
-    FLIP_CUDA_TRY(cudaGetLastError());
-    return FLIP_OK;
-}
-// the Jacobi-scaled form (pcg_tma.cu): init over the dilated tile list, warm
-// start and true-residual check over the occupied tiles
-int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
-                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
-                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
-    pcg_init_kernel<true><<<kPcgBlocks, 512, 0, s>>>(dil_tiles, d_ndil, D, U[0], U[1], U[2], type, cell_prev, B);
-    if (cell_prev)
-        pcg_warm_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
-                                                         B.partials);
-    FLIP_CUDA_TRY(cudaGetLastError());
-    return FLIP_OK;
-}
-int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
-                          cudaStream_t s) {
-    pcg_check_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
-                                                      B.partials);
+    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
+                                                B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

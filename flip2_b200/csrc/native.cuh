@@ -15,6 +15,7 @@ struct NatDims {
     int nx, ny, nz;
     int tx, ty, tz;
     float ox, oy, oz, h;
+    float inv_h;  // 1 / h: a position maps to grid coordinates as (p - o) * inv_h wherever cells, keys and stencils are taken
 };
 
 // device-resident Jacobi-PCG state (FP64 scalars)
@@ -117,30 +118,6 @@ __device__ __forceinline__ bool last_block_reduce_n(double (&v)[NV], double* par
     return true;  // out[] valid in thread 0
 }
 
-// TMA descriptors of the Jacobi-scaled PCG (pcg_tma.cu): the residual w and
-// both direction buffers as 4-D tile tensors (8 x 8 x 8 x tiles) with boxes of
-// a whole tile (c) and of the x (4 x 8 x 8), y (8 x 1 x 8) and z (8 x 8 x 1)
-// faces, q and xg with tile boxes, and the cell codes (512 bytes a tile)
-struct PcgMaps {
-    CUtensorMap wc, wx, wy, wz;
-    CUtensorMap p0c, p0x, p0y, p0z;
-    CUtensorMap p1c, p1x, p1y, p1z;
-    CUtensorMap qc, xgc, cellc;
-};
-int nat_make_pcg_maps(PcgMaps& M, const PcgBuffers& B, uint64_t ntiles_total);
-// one Jacobi-PCG iteration with TMA-staged tiles on the Jacobi-scaled
-// residual kept in B.r (w = D^-1 r); a TMA wait that gives up sets
-// DEVERR_TMA_TIMEOUT in *err
-int nat_launch_pcgw_iteration(const PcgMaps& M, const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D,
-                              PcgBuffers& B, uint32_t* err, int grid, cudaStream_t s);
-// initial state of that solve (B.r = D^-1 b; w and both directions zero on
-// the non-fluid cells of the dilated tiles dil_tiles), with the warm start as
-// nat_launch_pcg_init's; and its true-residual check (B.r = D^-1 (b - A x))
-int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
-                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
-                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev = nullptr);
-int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
-                          cudaStream_t s);
 // TMA descriptor of an arbitrary dense tensor (rank <= 5, strides in bytes of
 // dims 1 .. rank-1), zero fill outside it
 int encode_tensor_map(CUtensorMap* map, CUtensorMapDataType dtype, int rank, const void* base, const uint64_t* dims,
