@@ -88,111 +88,24 @@ __global__ void nat_gather_kernel(const uint32_t* __restrict__ perm, uint64_t n,
 // weights (and weighted velocities) of the tile's particles into a
 // shared-memory box of 10^3 nodes per component -- the tile plus the
 // one-node halo its stencils reach -- and adds the box to the global grids;
-// it also marks the cells that hold particles.  Two forms:
+// it also marks the cells that hold particles.
 //
-//   nat_p2g_cells_kernel (the one the step uses): a thread owns one cell of
-//   the tile.  The tile's particles are first sorted by cell inside the CTA
-//   (a counting sort in shared memory: one integer atomic per particle).
-//   Then each thread walks its cell's particles and keeps, per velocity
-//   component, the 2 x 3 x 3 node sums that any particle of that cell can
-//   reach in registers (36 floats: two nodes along the component's own axis,
-//   three along each staggered axis, where the stencil's base is the cell or
-//   the one below).  The sums go into the box in 18 phases, one node offset
-//   per phase, so that within a phase no two threads touch one node: plain
-//   shared-memory adds, no atomics.  FP32 sums, as the oracle's comparison
-//   assumes (relative precision even for the tiny weights of a node that only
-//   one far particle reaches; a fixed-point accumulator loses exactly those).
-//
-//   nat_p2g_scatter_kernel: a thread owns particles and adds each of their
-//   48 weighted terms with a shared-memory float atomic.
-constexpr int kP2GThreads = 256;
+// A thread owns one cell of the tile.  The tile's particles are first sorted
+// by cell inside the CTA (a counting sort in shared memory: one integer
+// atomic per particle), with their grid coordinates kept in shared memory in
+// the sorted order.  Then each thread walks its cell's particles and keeps,
+// per velocity component, the 2 x 3 x 3 node sums that any particle of that
+// cell can reach in registers (36 floats: two nodes along the component's own
+// axis, three along each staggered axis, where the stencil's base is the cell
+// or the one below).  The sums go into the box in 18 phases, one node offset
+// per phase, so that within a phase no two threads touch one node: plain
+// shared-memory adds, no atomics.  FP32 sums, as the oracle's comparison
+// assumes (relative precision even for the tiny weights of a node that only
+// one far particle reaches; a fixed-point accumulator loses exactly those).
+// A float-atomic scatter (a thread per particle, 48 shared atomics each) ran
+// 2-2.5x slower.
 constexpr int kBox = 10;
 constexpr int kBoxN = kBox * kBox * kBox;
-
-struct P2GScatterBox {
-    float v[3][2][kBoxN];
-    __device__ __forceinline__ void add(int c, int l, float w, float wv) {
-        atomicAdd(&v[c][0][l], wv);
-        atomicAdd(&v[c][1][l], w);
-    }
-    __device__ __forceinline__ float mom(int c, int l) const { return v[c][0][l]; }
-    __device__ __forceinline__ float wt(int c, int l) const { return v[c][1][l]; }
-    __device__ __forceinline__ void clear(int l) { (&v[0][0][0])[l] = 0.0f; }
-};
-
-__global__ void __launch_bounds__(kP2GThreads) nat_p2g_scatter_kernel(
-    const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ d_ntiles,
-    uint64_t n, const float* __restrict__ px, const float* __restrict__ py, const float* __restrict__ pz,
-    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, NatDims D,
-    float* __restrict__ mu, float* __restrict__ mv, float* __restrict__ mw, float* __restrict__ wu,
-    float* __restrict__ wv, float* __restrict__ ww, uint8_t* __restrict__ type) {
-    __shared__ P2GScatterBox sm;
-    const uint32_t ntiles = *d_ntiles;
-    float* gm[3] = {mu, mv, mw};
-    float* gw[3] = {wu, wv, ww};
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        for (int l = threadIdx.x; l < 3 * 2 * kBoxN; l += kP2GThreads) sm.clear(l);
-        __syncthreads();
-        const uint32_t key = tile_keys[t];
-        const int tx = key % D.tx, ty = (key / D.tx) % D.ty, tz = key / (D.tx * D.ty);
-        const int bi = 8 * tx - 1, bj = 8 * ty - 1, bk = 8 * tz - 1;  // box origin
-        const uint32_t start = starts[t];
-        const uint64_t end = (t + 1 < ntiles) ? starts[t + 1] : n;
-        for (uint64_t p = start + threadIdx.x; p < end; p += kP2GThreads) {
-            const float gx = nat_grid_coord(px[p], D.ox, D.inv_h), gy = nat_grid_coord(py[p], D.oy, D.inv_h),
-                        gz = nat_grid_coord(pz[p], D.oz, D.inv_h);
-            type[nslot(nat_cell_g(gx, D.nx), nat_cell_g(gy, D.ny), nat_cell_g(gz, D.nz), D)] = kFluid;
-            const float v[3] = {vx[p], vy[p], vz[p]};
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                int i0, j0, k0;
-                float fx, fy, fz;
-                nat_stencil(c, gx, gy, gz, D, i0, j0, k0, fx, fy, fz);
-                const int li = i0 - bi, lj = j0 - bj, lk = k0 - bk;
-                // the 2 x 2 x 2 stencil lies inside the tile's box for every
-                // particle of the tile; the test guards the shared array
-                if ((unsigned)li >= (unsigned)(kBox - 1) || (unsigned)lj >= (unsigned)(kBox - 1) ||
-                    (unsigned)lk >= (unsigned)(kBox - 1))
-                    continue;
-                // per-axis weights, 0 on the wall faces of component c
-                float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
-                if (c == 0) { if (i0 == 0) wx[0] = 0.0f; if (i0 + 1 == D.nx) wx[1] = 0.0f; }
-                if (c == 1) { if (j0 == 0) wy[0] = 0.0f; if (j0 + 1 == D.ny) wy[1] = 0.0f; }
-                if (c == 2) { if (k0 == 0) wz[0] = 0.0f; if (k0 + 1 == D.nz) wz[1] = 0.0f; }
-                const int l0 = li + kBox * (lj + kBox * lk);
-#pragma unroll
-                for (int dk = 0; dk < 2; ++dk)
-#pragma unroll
-                    for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-                        for (int di = 0; di < 2; ++di) {
-                            // a zero weight (a wall face) changes no sum
-                            const float w = wx[di] * wy[dj] * wz[dk];
-                            if (w == 0.0f) continue;
-                            sm.add(c, l0 + di + kBox * (dj + kBox * dk), w, w * v[c]);
-                        }
-            }
-        }
-        __syncthreads();
-        for (int l = threadIdx.x; l < kBoxN; l += kP2GThreads) {
-            const int li = l % kBox, lj = (l / kBox) % kBox, lk = l / (kBox * kBox);
-            const int i = bi + li, j = bj + lj, k = bk + lk;
-            if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) continue;
-            const uint32_t s = nslot(i, j, k, D);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float w = sm.wt(c, l);
-                if (w != 0.0f) {
-                    atomicAdd(gw[c] + s, w);
-                    atomicAdd(gm[c] + s, sm.mom(c, l));
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-
 constexpr int kPcThreads = 512;         // one thread per cell of the tile
 constexpr int kPcChunk = 4096;          // particles sorted per round (a denser tile takes several)
 constexpr int kPcPer = kPcChunk / kPcThreads;
@@ -1425,25 +1338,17 @@ int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src,
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-// the form of P2G the step uses: true = the cell-owned kernel (no atomics
-// in the accumulation), false = the float-atomic scatter
-constexpr bool kP2GCells = true;
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s) {
-    if (kP2GCells) {
-        constexpr size_t smem = sizeof(P2GCellSmem);
-        static bool attr_done = false;
-        if (!attr_done) {
-            FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_p2g_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr_done = true;
-        }
-        nat_p2g_cells_kernel<<<grid, kPcThreads, smem, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
-                                                            vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
-    } else {
-        nat_p2g_scatter_kernel<<<grid, kP2GThreads, 0, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0],
-                                                            vs[1], vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
+    constexpr size_t smem = sizeof(P2GCellSmem);
+    static bool attr_done = false;
+    if (!attr_done) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(nat_p2g_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_done = true;
     }
+    nat_p2g_cells_kernel<<<grid, kPcThreads, smem, s>>>(tile_keys, starts, d_ntiles, n, ps[0], ps[1], ps[2], vs[0], vs[1],
+                                                        vs[2], D, m[0], m[1], m[2], w[0], w[1], w[2], type);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
