@@ -119,73 +119,90 @@ __device__ __forceinline__ RefLocal ref_particle_local(const double* px, const d
     return r;
 }
 
-// getNumberVoxelsUsedPerNode (particles.cu:88-190): mask + count per node
-__global__ void __launch_bounds__(kNodeThreads) ref_voxel_counts_kernel(
+// getNumberVoxelsUsedPerNode (particles.cu:88-190): mask + count per node.
+// A warp per node (kVoxWarps nodes per CTA): the 512 solid tests as 16
+// ballots, then the node's particles one after the other, the 64 points of a
+// particle's 4 x 4 x 4 stencil spread over the lanes (two each).  The tests
+// and their arithmetic are the reference's; only the work is spread.  Its
+// loops run x from sx - 2 while (unsigned) x < sx + 2, so a stencil
+// coordinate below 2 on any axis leaves a particle without marks, and points
+// outside the 8^3 tile never mark: both are tested before the distances.
+constexpr int kVoxWarps = 8;
+__global__ void __launch_bounds__(32 * kVoxWarps) ref_voxel_counts_kernel(
     const uint32_t* __restrict__ starts, const uint32_t* __restrict__ keys, uint32_t nodes, uint64_t n,
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz, flip_grid g,
     uint32_t* __restrict__ counts, uint32_t* __restrict__ masks) {
-    __shared__ uint32_t mark[512];
-    const uint32_t b = blockIdx.x;
+    __shared__ uint32_t mark[kVoxWarps][16];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t b = blockIdx.x * kVoxWarps + (uint32_t)w;
+    if (b >= nodes) return;  // a whole warp; nothing below synchronises the CTA
+    uint32_t* M = mark[w];
     uint32_t gx, gy, gz;
     ref_decompose(keys[b], g, gx, gy, gz);  // Q3: particle b's key, not the node's
-    for (int i = threadIdx.x; i < 512; i += kNodeThreads) mark[i] = ref_tile_solid(i, gx, gy, gz, g) ? 1u : 0u;
-    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < 16; ++q) {
+        const uint32_t bits = __ballot_sync(0xffffffffu, ref_tile_solid((uint32_t)(q * 32 + lane), gx, gy, gz, g));
+        if (lane == 0) M[q] = bits;
+    }
+    __syncwarp();
     const uint32_t last = (b == nodes - 1) ? (uint32_t)n : starts[b + 1];
     const double scw = ref_scw(g), hs = scw / 2.0, R = 2.0 * scw;
-    for (uint32_t idx = starts[b] + threadIdx.x; idx < last; idx += kNodeThreads) {
-        RefLocal L = ref_particle_local(px, py, pz, keys, idx, g, scw);
-        for (int x = (int)(L.sx - 2u); (uint32_t)x < L.sx + 2u; ++x)
-            for (int y = (int)(L.sy - 2u); (uint32_t)y < L.sy + 2u; ++y)
-                for (int z = (int)(L.sz - 2u); (uint32_t)z < L.sz + 2u; ++z) {
-                    double dx = L.lx - x * scw, dy = L.ly - y * scw, dz = L.lz - z * scw;
-                    double xc = ref_dist(dx, dy + hs, dz + hs);
-                    double yc = ref_dist(dx + hs, dy, dz + hs);
-                    double zc = ref_dist(dx + hs, dy + hs, dz);
-                    if (xc < R || yc < R || zc < R)
-                        if ((uint32_t)x < 8u && (uint32_t)y < 8u && (uint32_t)z < 8u) mark[x + y * 8 + z * 64] = 1u;
-                }
-    }
-    __syncthreads();
-    // 512 marks -> 16 mask words (4 warps x 4 ballots)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t c = 0;
+    for (uint32_t idx = starts[b]; idx < last; ++idx) {
+        const RefLocal L = ref_particle_local(px, py, pz, keys, idx, g, scw);
+        if (L.sx < 2u || L.sy < 2u || L.sz < 2u) continue;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        int w = warp * 4 + q;
-        uint32_t bits = __ballot_sync(0xffffffffu, mark[w * 32 + lane] != 0u);
-        if (lane == 0) masks[(size_t)b * 16 + w] = bits;
-        c += __popc(bits);
+        for (int h = 0; h < 2; ++h) {
+            const int pt = lane + 32 * h;
+            const int x = (int)(L.sx - 2u) + (pt >> 4), y = (int)(L.sy - 2u) + ((pt >> 2) & 3), z = (int)(L.sz - 2u) + (pt & 3);
+            if ((uint32_t)x >= 8u || (uint32_t)y >= 8u || (uint32_t)z >= 8u) continue;
+            const double dx = L.lx - x * scw, dy = L.ly - y * scw, dz = L.lz - z * scw;
+            const double xc = ref_dist(dx, dy + hs, dz + hs);
+            const double yc = ref_dist(dx + hs, dy, dz + hs);
+            const double zc = ref_dist(dx + hs, dy + hs, dz);
+            if (xc < R || yc < R || zc < R) {
+                const int v = x + y * 8 + z * 64;
+                atomicOr(&M[v >> 5], 1u << (v & 31));
+            }
+        }
     }
-    __shared__ uint32_t part[kNodeThreads / 32];
-    if (lane == 0) part[warp] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) counts[b] = part[0] + part[1] + part[2] + part[3];
+    __syncwarp();
+    const uint32_t bits = lane < 16 ? M[lane] : 0u;
+    if (lane < 16) masks[(size_t)b * 16 + lane] = bits;
+    uint32_t c = __popc(bits);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) counts[b] = c;
 }
 
-// generateVoxelIDs (particles.cu:192-321): compaction from the mask
-__global__ void __launch_bounds__(kNodeThreads) ref_voxel_ids_kernel(
+// generateVoxelIDs (particles.cu:192-321): compaction from the mask, a warp
+// per node; lane l writes bit l of each mask word
+__global__ void __launch_bounds__(32 * kVoxWarps) ref_voxel_ids_kernel(
     const uint32_t* __restrict__ keys, uint32_t nodes, const uint32_t* __restrict__ masks,
     const uint32_t* __restrict__ node_voxels, flip_grid g, uint32_t* __restrict__ voxel_ids, int8_t* __restrict__ solids) {
-    __shared__ uint32_t m[16];
-    __shared__ uint32_t pre[17];
-    const uint32_t b = blockIdx.x;
-    if (threadIdx.x < 16) m[threadIdx.x] = masks[(size_t)b * 16 + threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t s = 0;
-        for (int w = 0; w < 16; ++w) { pre[w] = s; s += __popc(m[w]); }
-        pre[16] = s;
+    const int lane = threadIdx.x & 31;
+    const uint32_t b = blockIdx.x * kVoxWarps + (threadIdx.x >> 5);
+    if (b >= nodes) return;
+    const uint32_t m = lane < 16 ? masks[(size_t)b * 16 + lane] : 0u;
+    // exclusive prefix of the words' popcounts over lanes 0..15
+    uint32_t inc = __popc(m);
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
     }
-    __syncthreads();
+    const uint32_t pre = inc - __popc(m);
     uint32_t gx, gy, gz;
     ref_decompose(keys[b], g, gx, gy, gz);
     const uint32_t start = b ? node_voxels[b - 1] : 0u;
-    for (int i = threadIdx.x; i < 512; i += kNodeThreads) {
-        uint32_t w = i >> 5, bit = i & 31;
-        if (m[w] & (1u << bit)) {
-            uint32_t pos = pre[w] + __popc(m[w] & ((1u << bit) - 1u));
-            voxel_ids[start + pos] = (uint32_t)i;
-            solids[start + pos] = ref_tile_solid(i, gx, gy, gz, g) ? 1 : 0;
+    const uint32_t below = (1u << lane) - 1u;
+#pragma unroll 4
+    for (int q = 0; q < 16; ++q) {
+        const uint32_t word = __shfl_sync(0xffffffffu, m, q), base = __shfl_sync(0xffffffffu, pre, q);
+        if ((word >> lane) & 1u) {
+            const uint32_t i = (uint32_t)(q * 32 + lane);
+            const uint32_t pos = start + base + __popc(word & below);
+            voxel_ids[pos] = i;
+            solids[pos] = ref_tile_solid(i, gx, gy, gz, g) ? 1 : 0;
         }
     }
 }
@@ -575,13 +592,17 @@ int ref_launch_ydim(const uint32_t* starts, const uint32_t* keys, uint32_t nodes
 int ref_launch_voxel_counts(const uint32_t* starts, const uint32_t* keys, uint32_t nodes, uint64_t n, const double* px,
                             const double* py, const double* pz, const flip_grid& g, uint32_t* counts, uint32_t* masks,
                             cudaStream_t s) {
-    if (nodes) ref_voxel_counts_kernel<<<nodes, kNodeThreads, 0, s>>>(starts, keys, nodes, n, px, py, pz, g, counts, masks);
+    if (nodes)
+        ref_voxel_counts_kernel<<<(nodes + kVoxWarps - 1) / kVoxWarps, 32 * kVoxWarps, 0, s>>>(starts, keys, nodes, n, px, py,
+                                                                                            pz, g, counts, masks);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 int ref_launch_voxel_ids(const uint32_t* keys, uint32_t nodes, const uint32_t* masks, const uint32_t* node_voxels,
                          const flip_grid& g, uint32_t* voxel_ids, int8_t* solids, cudaStream_t s) {
-    if (nodes) ref_voxel_ids_kernel<<<nodes, kNodeThreads, 0, s>>>(keys, nodes, masks, node_voxels, g, voxel_ids, solids);
+    if (nodes)
+        ref_voxel_ids_kernel<<<(nodes + kVoxWarps - 1) / kVoxWarps, 32 * kVoxWarps, 0, s>>>(keys, nodes, masks, node_voxels, g,
+                                                                                          voxel_ids, solids);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
