@@ -856,8 +856,8 @@ static int nat_pcg_graph(flip_engine* e, int iters, int max_iter) {
     E_TRY(build_loop_graph(e, [&]() {
         int rc = FLIP_OK;
         for (int k = 0; k < iters && rc == FLIP_OK; ++k)
-            rc = nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
-        if (rc == FLIP_OK) rc = nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+            rc = nat_launch_pcgw_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+        if (rc == FLIP_OK) rc = nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
         return rc;
     }, limit, &e->pcg_graph));
     e->pcg_graph_iters = iters;
@@ -1176,8 +1176,8 @@ static bool host_solve_loop() {
 static int run_plain_host(flip_engine* e, int chunk, int max_iter) {
     const int limit = loop_limit(max_iter, chunk);
     for (int c = 0; c < limit; ++c) {
-        for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
-        E_TRY(nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcgw_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+        E_TRY(nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
         E_CUDA(cudaMemcpyAsync(e->h_state, e->pcg.st, sizeof(PcgState), cudaMemcpyDeviceToHost, e->stream));
         E_TRY(dev_err_fetch(e));
         E_CUDA(cudaStreamSynchronize(e->stream));
@@ -1257,8 +1257,8 @@ static int nat_solve(flip_engine* e, const float* const* U, int method, double t
         pcg_state_host(e, tol, max_plain, 0);
         E_CUDA(cudaMemcpyAsync(e->pcg.st, e->h_state, sizeof(PcgState), cudaMemcpyHostToDevice, e->stream));
         const bool w = warm && method == 0;
-        E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
-                                  w ? e->cell_prev : nullptr));
+        E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU,
+                                   e->type, e->pcg, e->stream, w ? e->cell_prev : nullptr));
         e->launches += w ? 2 : 1;
         if (method == 0) E_TRY(e->mark(9));
         if (host_solve_loop()) {
@@ -1432,8 +1432,8 @@ static int cap_loop(flip_engine* e, int limit, Fn body) {
     });
 }
 static int cap_plain_chunk(flip_engine* e, int chunk) {
-    for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcg_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
-    return nat_launch_pcg_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
+    for (int k = 0; k < chunk; ++k) E_TRY(nat_launch_pcgw_iteration(e->node_keys, e->d_counts, e->D, e->pcg, e->stream));
+    return nat_launch_pcgw_check(e->node_keys, e->d_counts, e->D, e->pcg, e->stream);
 }
 static int cap_mg_chunk(flip_engine* e, int chunk, bool network) {
     const int* halt = &e->pcg.st->halt;
@@ -1450,8 +1450,8 @@ static int cap_plain_solve(flip_engine* e, const float* const* U, bool warm, int
     const int chunk = e->P.pcg_check_every;
     const float* const nullU[3] = {nullptr, nullptr, nullptr};
     E_TRY(nat_launch_state_init(e->pcg.st, e->P.pcg_tol, e->P.pcg_max_iter, e->P.true_residual_every, 0, e->stream));
-    E_TRY(nat_launch_pcg_init(e->node_keys, e->d_counts, e->D, U ? U : nullU, e->type, e->pcg, e->stream,
-                              warm ? e->cell_prev : nullptr));
+    E_TRY(nat_launch_pcgw_init(e->node_keys, e->d_counts, e->grid_tiles, e->d_counts + 1, e->D, U ? U : nullU, e->type,
+                               e->pcg, e->stream, warm ? e->cell_prev : nullptr));
     E_TRY(cap_loop(e, loop_limit(e->P.pcg_max_iter, chunk), [&]() { return cap_plain_chunk(e, chunk); }));
     return nat_launch_solve_record(e->d_rec, e->pcg.st, 0, stage, 1, e->stream);
 }

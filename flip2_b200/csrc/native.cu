@@ -546,6 +546,12 @@ __device__ __forceinline__ float jacobi_inv_s(const float* tab, uint8_t c) { ret
 // cell_prev (warm start): the previous solve's cell codes; x starts from the
 // previous solution (x + xg) on cells that are fluid in both solves, 0
 // elsewhere, and pcg_warm_kernel then replaces r = b by b - A x
+// W (the plain solve's scaled form): r holds w = D^-1 r (0 where d = 0: a
+// fluid cell walled in by solids has an empty row of A), and the tiles walked
+// are the dilated list, so that w and both direction buffers are also zero on
+// the non-fluid cells around the fluid: the matvec then reads its halo
+// without the neighbours' cell codes
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ d_ntiles,
                                                         NatDims D, const float* __restrict__ u, const float* __restrict__ v,
                                                         const float* __restrict__ w, const uint8_t* __restrict__ type,
@@ -584,8 +590,9 @@ __global__ void __launch_bounds__(512, 4) pcg_init_kernel(const uint32_t* __rest
     B.x[s] = x0;
     B.xg[s] = 0.0f;
     const float z = b * jacobi_inv(code);
-    B.r[s] = b;
+    B.r[s] = W ? ((code & 7u) ? __fdiv_rn(b, (float)(code & 7u)) : 0.0f) : b;
     B.p0[s] = 0.0f;
+    if (W) B.p1[s] = 0.0f;
     bb += (double)b * (double)b;
     rz += (double)b * (double)z;
     NAT_TILE_LOOP_END
@@ -686,18 +693,29 @@ struct Dm4Loads {
     uint32_t hc;  // the three halo codes, a byte each
 };
 
-template <bool kFlex>
+// what the direction update starts from:
+//   kDmJacobi  r, p' = D^-1 r + beta p on fluid cells (codes of the tile and halo);
+//   kDmFlex    z (flexible CG, the preconditioned residual given), p' = z + beta p on fluid cells;
+//   kDmScaled  w = D^-1 r, zero off the fluid like p on the dilated tiles, p' = w + beta p: the
+//              halo needs no cell codes (the plain solve)
+enum DmMode { kDmJacobi = 0, kDmFlex = 1, kDmScaled = 2 };
+template <int kMode>
+__device__ __forceinline__ float dir1(const float* tab, uint8_t c, float r, float p, float beta) {
+    if (kMode == kDmScaled) return fmaf(beta, p, r);
+    return kMode == kDmFlex ? dir_value_z(c, r, p, beta) : dir_value(tab, c, r, p, beta);
+}
+template <int kMode>
 __device__ __forceinline__ float4 dir4(const float* tab, uint32_t c4, float4 r, float4 p, float beta) {
     float4 o;
-    o.x = kFlex ? dir_value_z((uint8_t)c4, r.x, p.x, beta) : dir_value(tab, (uint8_t)c4, r.x, p.x, beta);
-    o.y = kFlex ? dir_value_z((uint8_t)(c4 >> 8), r.y, p.y, beta) : dir_value(tab, (uint8_t)(c4 >> 8), r.y, p.y, beta);
-    o.z = kFlex ? dir_value_z((uint8_t)(c4 >> 16), r.z, p.z, beta) : dir_value(tab, (uint8_t)(c4 >> 16), r.z, p.z, beta);
-    o.w = kFlex ? dir_value_z((uint8_t)(c4 >> 24), r.w, p.w, beta) : dir_value(tab, (uint8_t)(c4 >> 24), r.w, p.w, beta);
+    o.x = dir1<kMode>(tab, (uint8_t)c4, r.x, p.x, beta);
+    o.y = dir1<kMode>(tab, (uint8_t)(c4 >> 8), r.y, p.y, beta);
+    o.z = dir1<kMode>(tab, (uint8_t)(c4 >> 16), r.z, p.z, beta);
+    o.w = dir1<kMode>(tab, (uint8_t)(c4 >> 24), r.w, p.w, beta);
     return o;
 }
 
 constexpr int kDm4Smem = kDm4Groups * 2 * kBoxFloats * (int)sizeof(float);
-template <bool kFlex>
+template <int kMode>
 __global__ void __launch_bounds__(512, 2) pcg_dirmatvec4_kernel(const uint32_t* __restrict__ tiles,
                                                                  const uint32_t* __restrict__ tcoord,
                                                                  const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -767,7 +785,7 @@ __global__ void __launch_bounds__(512, 2) pcg_dirmatvec4_kernel(const uint32_t* 
                 const uint32_t sn = (((uint32_t)((int)key + fdelta[f])) << 9) | ((hA[k] >> 3) & 511u);
                 L.hr[k] = r[sn];
                 L.hp[k] = p[sn];
-                L.hc |= (uint32_t)cell[sn] << (8 * k);
+                if (kMode != kDmScaled) L.hc |= (uint32_t)cell[sn] << (8 * k);
             }
         }
     };
@@ -778,14 +796,13 @@ __global__ void __launch_bounds__(512, 2) pcg_dirmatvec4_kernel(const uint32_t* 
     for (int it = 0; t < ntiles; t += stride, ++it) {
         float* Bx = dm4_box + (2 * g + (it & 1)) * kBoxFloats;
         const uint32_t s = (cur.key << 9) | lo;
-        const float4 pc = dir4<kFlex>(tab, cur.c, cur.r, cur.p, beta);
+        const float4 pc = dir4<kMode>(tab, cur.c, cur.r, cur.p, beta);
         *reinterpret_cast<float4*>(Bx + bo) = pc;
         *reinterpret_cast<float4*>(pn + s) = pc;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const uint8_t hc = (uint8_t)(cur.hc >> (8 * k));
-            Bx[hA[k] >> 12] = kFlex ? dir_value_z(hc, cur.hr[k], cur.hp[k], beta)
-                                    : dir_value(tab, hc, cur.hr[k], cur.hp[k], beta);
+            Bx[hA[k] >> 12] = dir1<kMode>(tab, hc, cur.hr[k], cur.hp[k], beta);
         }
         if (flush && cur.c) {
             const float* gv = xg + s;
@@ -835,6 +852,8 @@ __global__ void __launch_bounds__(512, 2) pcg_dirmatvec4_kernel(const uint32_t* 
 
 // xg += alpha p, r -= alpha q, partial r.r and r.z; eight cells per thread
 // per round (two 16-byte quads per array, all loads issued before use)
+// W: r4 holds w = D^-1 r: w -= a D^-1 q, r.r = sum (d w)^2, r.z = sum d w^2
+template <bool W>
 __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const float4& p4, const float4& q4, float4& r4,
                                          float4& g4, float a, double& rr, double& rz) {
     float* rv = &r4.x;
@@ -846,11 +865,20 @@ __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const fl
         const uint8_t c = (uint8_t)(c4 >> (8 * m));
         if (!(c & kCellFluid)) continue;
         gv[m] = fmaf(a, pv[m], gv[m]);
-        const float rs = fmaf(-a, qv[m], rv[m]);
-        rv[m] = rs;
-        const float z = rs * jacobi_inv_s(tab, c);
-        rr += (double)rs * (double)rs;
-        rz += (double)rs * (double)z;
+        if (W) {
+            const float d = (float)(c & 7u);
+            const float wn = fmaf(-a, qv[m] * jacobi_inv_s(tab, c), rv[m]);
+            rv[m] = wn;
+            const float rs = d * wn;
+            rr += (double)rs * (double)rs;
+            rz += (double)rs * (double)wn;
+        } else {
+            const float rs = fmaf(-a, qv[m], rv[m]);
+            rv[m] = rs;
+            const float z = rs * jacobi_inv_s(tab, c);
+            rr += (double)rs * (double)rs;
+            rz += (double)rs * (double)z;
+        }
     }
 }
 
@@ -860,6 +888,7 @@ __device__ __forceinline__ void upd_quad(const float* tab, uint32_t c4, const fl
 constexpr int kUpdThreads = 256;
 constexpr int kUpdQuads = 2;                    // quads per lane and unit
 constexpr int kUpdUnits = 128 / (32 * kUpdQuads);  // units per tile
+template <bool W>
 __global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32_t* __restrict__ tiles,
                                                                      const uint32_t* __restrict__ d_ntiles, NatDims D,
                                                                      float* __restrict__ xg, float* __restrict__ r,
@@ -899,7 +928,7 @@ __global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32
         for (int m = 0; m < kUpdQuads; ++m) {
             if (!c[m]) continue;
             const uint32_t s = (key << 9) | ((qbase + 32 * m) << 2);
-            upd_quad(tab, c[m], pv[m], qv[m], rv[m], gv[m], a, rr, rz);
+            upd_quad<W>(tab, c[m], pv[m], qv[m], rv[m], gv[m], a, rr, rz);
             *reinterpret_cast<float4*>(r + s) = rv[m];
             *reinterpret_cast<float4*>(xg + s) = gv[m];
         }
@@ -927,6 +956,7 @@ __global__ void __launch_bounds__(kUpdThreads, 4) pcg_update_kernel(const uint32
 // iterations.  Replaces r, decides convergence on the true value and asks
 // the next direction kernel to fold xg into x.  The FP64 solution of the tile
 // and its halo is staged in shared memory like the matvec.
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __restrict__ tiles,
                                                             const uint32_t* __restrict__ tcoord,
                                                             const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -962,9 +992,15 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
             rr += res * res;
-            const float rs = (float)res;
-            r[s] = rs;
-            rz += (double)rs * (double)(rs * jacobi_inv(c));
+            if (W) {
+                const float ws = (c & 7u) ? (float)(res / (double)(c & 7u)) : 0.0f;
+                r[s] = ws;
+                rz += (double)(c & 7u) * (double)ws * (double)ws;
+            } else {
+                const float rs = (float)res;
+                r[s] = rs;
+                rz += (double)rs * (double)(rs * jacobi_inv(c));
+            }
         }
         __syncthreads();
     }
@@ -997,6 +1033,7 @@ __global__ void __launch_bounds__(512, 4) pcg_check_kernel(const uint32_t* __res
 // warm start: r = b - A x in FP64 for the initial guess, r.r and r.z, and
 // the state for the first iteration (converged already if |r| <= tol |b|;
 // b = 0 gives x = 0)
+template <bool W>
 __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __restrict__ tiles,
                                                            const uint32_t* __restrict__ tcoord,
                                                            const uint32_t* __restrict__ d_ntiles, NatDims D,
@@ -1034,9 +1071,15 @@ __global__ void __launch_bounds__(512, 4) pcg_warm_kernel(const uint32_t* __rest
             const double sum = ((X[bc - 1] + X[bc + 1]) + (X[bc - 10] + X[bc + 10])) + (X[bc - 100] + X[bc + 100]);
             const double res = (double)bv[s] - ((double)(c & 7u) * xs - sum);
             rr += res * res;
-            const float rs = (float)res;
-            r[s] = rs;
-            rz += (double)rs * (double)(rs * jacobi_inv(c));
+            if (W) {
+                const float ws = (c & 7u) ? (float)(res / (double)(c & 7u)) : 0.0f;
+                r[s] = ws;
+                rz += (double)(c & 7u) * (double)ws * (double)ws;
+            } else {
+                const float rs = (float)res;
+                r[s] = rs;
+                rz += (double)rs * (double)(rs * jacobi_inv(c));
+            }
         }
         __syncthreads();
     }
@@ -1429,10 +1472,20 @@ int nat_launch_normalize(const uint32_t* tiles, const uint32_t* d_count, const N
 }
 int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, const float* const* U,
                         const uint8_t* type, PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
-    pcg_init_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
+    pcg_init_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, d_ntiles, D, U[0], U[1], U[2], type, cell_prev, B);
     if (cell_prev)
-        pcg_warm_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
-                                                   B.partials);
+        pcg_warm_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
+                                                          B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
+                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
+                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev) {
+    pcg_init_kernel<true><<<kPcgBlocks, 512, 0, s>>>(dil_tiles, d_ndil, D, U[0], U[1], U[2], type, cell_prev, B);
+    if (cell_prev)
+        pcg_warm_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.b, B.r, B.cell, B.st,
+                                                         B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1440,18 +1493,19 @@ int nat_launch_pcg_init(const uint32_t* tiles, const uint32_t* d_ntiles, const N
 static int dm4_prepare() {
     static bool done = false;
     if (done) return FLIP_OK;
-    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
-    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
+    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<kDmJacobi>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
+    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<kDmFlex>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
+    FLIP_CUDA_TRY(cudaFuncSetAttribute(pcg_dirmatvec4_kernel<kDmScaled>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDm4Smem));
     done = true;
     return FLIP_OK;
 }
 int nat_launch_fpcg_direction_update(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                                      cudaStream_t s) {
     if (int rc = dm4_prepare()) return rc;
-    pcg_dirmatvec4_kernel<true><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell, B.q, B.x,
-                                                          B.xg, B.st, B.partials);
-    pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
-                                                               B.st, B.partials);
+    pcg_dirmatvec4_kernel<kDmFlex><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.z, B.p0, B.p1, B.cell,
+                                                                     B.q, B.x, B.xg, B.st, B.partials);
+    pcg_update_kernel<false><<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q,
+                                                                      B.cell, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
@@ -1464,17 +1518,34 @@ int nat_launch_fpcg_dot(const uint32_t* tiles, const uint32_t* d_ntiles, PcgBuff
 int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                              cudaStream_t s) {
     if (int rc = dm4_prepare()) return rc;
-    pcg_dirmatvec4_kernel<false><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell, B.q, B.x, B.xg,
-                                                    B.st, B.partials);
-    pcg_update_kernel<<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q, B.cell,
-                                                               B.st, B.partials);
+    pcg_dirmatvec4_kernel<kDmJacobi><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell,
+                                                                       B.q, B.x, B.xg, B.st, B.partials);
+    pcg_update_kernel<false><<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q,
+                                                                      B.cell, B.st, B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcgw_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                              cudaStream_t s) {
+    if (int rc = dm4_prepare()) return rc;
+    pcg_dirmatvec4_kernel<kDmScaled><<<kDm4Blocks, 512, kDm4Smem, s>>>(tiles, B.tcoord, d_ntiles, D, B.r, B.p0, B.p1, B.cell,
+                                                                       B.q, B.x, B.xg, B.st, B.partials);
+    pcg_update_kernel<true><<<kPcgUpdateBlocks, kUpdThreads, 0, s>>>(tiles, d_ntiles, D, B.xg, B.r, B.p0, B.p1, B.q,
+                                                                     B.cell, B.st, B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s) {
-    pcg_check_kernel<<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
-                                                B.partials);
+    pcg_check_kernel<false><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
+                                                       B.partials);
+    FLIP_CUDA_TRY(cudaGetLastError());
+    return FLIP_OK;
+}
+int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                          cudaStream_t s) {
+    pcg_check_kernel<true><<<kPcgBlocks, 512, 0, s>>>(tiles, B.tcoord, d_ntiles, D, B.x, B.xg, B.b, B.r, B.cell, B.st,
+                                                      B.partials);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

@@ -178,6 +178,18 @@ int nat_launch_pcg_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, co
 // true_every iterations; decides convergence
 int nat_launch_pcg_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
                          cudaStream_t s);
+// the plain solve's form of the above: the residual kept as w = D^-1 r, zero
+// (like both direction buffers) on the non-fluid cells of the dilated tile
+// list dil_tiles (which nat_launch_pcgw_init walks), so that the matvec
+// reads its halo without cell codes; init, iteration and true-residual check
+// as nat_launch_pcg_init / _iteration / _check otherwise
+int nat_launch_pcgw_init(const uint32_t* tiles, const uint32_t* d_ntiles, const uint32_t* dil_tiles,
+                         const uint32_t* d_ndil, const NatDims& D, const float* const* U, const uint8_t* type,
+                         PcgBuffers& B, cudaStream_t s, const uint8_t* cell_prev = nullptr);
+int nat_launch_pcgw_iteration(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                              cudaStream_t s);
+int nat_launch_pcgw_check(const uint32_t* tiles, const uint32_t* d_ntiles, const NatDims& D, PcgBuffers& B,
+                          cudaStream_t s);
 // end of a loop chunk inside a conditional WHILE graph node: continue while
 // the solve is not done and fewer than limit chunks have run
 int nat_launch_loop_ctl(cudaGraphConditionalHandle h, PcgState* st, int limit, cudaStream_t s);

@@ -286,7 +286,11 @@ int flip_sync(flip_engine* e);
 int flip_step_streamed_f32(flip_engine* e, float* px, float* py, float* pz, float* vx, float* vy, float* vz,
                            uint64_t n, double dt);
 
-/* Buffers for inspection (device pointers lent, not transferred). */
+/* Buffers for inspection (device pointers lent, not transferred).  In
+ * NATIVE mode FLIP_BUF_UX/UY/UZ are the face grids, FLIP_BUF_DIVU the
+ * right-hand side b, FLIP_BUF_P the FP64 solution part and FLIP_BUF_RES the
+ * solver's working residual: D^-1 r (r scaled by the inverse Jacobi diagonal)
+ * after a Jacobi-PCG solve, r after a flexible one. */
 typedef enum {
     FLIP_BUF_PX = 0, FLIP_BUF_PY, FLIP_BUF_PZ, FLIP_BUF_VX, FLIP_BUF_VY, FLIP_BUF_VZ,
     FLIP_BUF_KEYS, FLIP_BUF_PERM, FLIP_BUF_FLAGS, FLIP_BUF_STARTS, FLIP_BUF_YTABLE,
