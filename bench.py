@@ -299,10 +299,31 @@ def ref_cpu_run(cells, steps, warm, budget_s):
     return n * steps / sec, n, sec, sample
 
 
+def testing_h_checks(cells):
+    """The reference's CPU verification path (engine/testing.h:25-53:
+    storeGridCellMap on the cell keys before the sort, validateGridCellOrdering
+    on the sorted keys; std::map on one host thread, as the reference's),
+    restated in the oracle and timed on the whole workload: the reference-mode
+    cell keys of every particle (the reference grid of 4-voxel cells) and the
+    same keys sorted."""
+    from oracle import oracle as O
+    pos, _ = scene(cells)
+    g = O.grid(0.0, 0.0, 0.0, cells // 4, cells // 4, cells // 4, 4.0 / cells)
+    keys, _, _, _ = O.ref_keys(pos[:, 0], pos[:, 1], pos[:, 2], g)
+    del pos
+    sorted_keys, _ = O.sort_pairs(keys)
+    t0 = time.perf_counter()
+    status, ncells = O.ref_grid_cell_checks(keys, sorted_keys)
+    sec = time.perf_counter() - t0
+    return {"what": "storeGridCellMap + validateGridCellOrdering (engine/testing.h:25-53) restated with std::map "
+                    "(oracle/ref_checks.cpp), one host thread", "particles": int(keys.size), "cells": ncells,
+            "seconds": sec, "particles_per_s": keys.size / sec, "passed": status == 0, "cores": 1}
+
+
 def cpu_baseline(cells, budget_s=25.0):
     value, n, sec, sample = ref_cpu_run(cells, 3, 3, budget_s)
     return {"value": value, "unit": METRIC, "cores": os.cpu_count(), "kind": "port", "sample": sample,
-            "seconds": sec}
+            "seconds": sec, "testing_h_checks": testing_h_checks(cells)}
 
 
 # ------------------------------------------------------------ clocks

@@ -53,6 +53,7 @@ def lib():
         I64, U32, D, I = C.c_int64, C.c_uint32, C.c_double, C.c_int
         sig = {
             "orc_ref_keys": (None, [I64, f64p, f64p, f64p, Grid, u32p]),
+            "orc_ref_grid_cell_checks": (I64, [u32p, u32p, C.c_uint64, C.POINTER(C.c_uint64)]),
             "orc_sort_pairs": (None, [I64, u32p, u32p, u32p]),
             "orc_sort_pairs_payload": (None, [I64, u32p, u32p, u32p, u32p]),
             "orc_inclusive_scan": (None, [I64, u32p]),
@@ -107,6 +108,19 @@ def ref_keys(px, py, pz, g):
     keys = np.empty(px.size, np.uint32)
     lib().orc_ref_keys(px.size, px, py, pz, g, keys)
     return keys, px, py, pz
+
+
+def ref_grid_cell_checks(unsorted, sorted_keys):
+    """The reference's CPU verification of its binning (engine/testing.h:25-53):
+    storeGridCellMap on the unsorted cell keys, validateGridCellOrdering on the
+    sorted ones.  Returns (status, cells): status 0 when ordered with equal
+    per-cell counts, 1 + i at the first out-of-order index i, -m for m cells
+    whose counts differ; cells = distinct cells stored."""
+    u = np.ascontiguousarray(unsorted, np.uint32)
+    s = np.ascontiguousarray(sorted_keys, np.uint32)
+    cells = C.c_uint64(0)
+    st = lib().orc_ref_grid_cell_checks(u, s, u.size, C.byref(cells))
+    return int(st), int(cells.value)
 
 
 def sort_pairs(keys, vals=None):

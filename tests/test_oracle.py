@@ -37,6 +37,25 @@ def test_sort_full_32bit_keys():
     assert np.array_equal(perm, np.argsort(keys, kind="stable"))
 
 
+def test_grid_cell_checks_of_testing_h():
+    # the reference's CPU verification of its binning (engine/testing.h):
+    # passes on the oracle's own sort, and catches a key out of order and a
+    # sorted array whose per-cell counts differ (mistakes planted in the
+    # input, on the CPU)
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 5000, 200_000).astype(np.uint32)
+    ko, _ = O.sort_pairs(keys)
+    assert O.ref_grid_cell_checks(keys, ko) == (0, np.unique(keys).size)
+    m = ko.size // 2
+    bad = ko.copy()
+    bad[m] = bad[m - 1] - 1  # keys near the middle are far above 0
+    assert O.ref_grid_cell_checks(keys, bad)[0] == m + 1  # 1 + the index of the first decrease
+    shifted = ko.copy()
+    j = int(np.searchsorted(shifted, shifted[shifted.size // 2], side="right"))
+    shifted[j - 1] = shifted[j]  # one particle moves to the next cell: two counts differ
+    assert O.ref_grid_cell_checks(keys, shifted)[0] == -2
+
+
 def test_getmax_quirk():
     """CudaVec::getMax compares element t with t+256 only (cudaVec.cu:216-222):
     each 512-block yields the pick of its elements 0 and 256."""
