@@ -559,20 +559,41 @@ int lp_forward_dev(const LpNet& net, const LpGrid& G, const float* d_inv_s, cons
 static int lp_backward_path(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz,
                             __nv_bfloat16* const* acts, float sign, int grid, cudaStream_t st) {
     // layer 3 (16 -> 1)
-    lp_wgrad_kernel<2, 16, 1><<<grid, 512, 0, st>>>(G, net.dil[3], gz, acts[2], d_inv_s, sign, G.out_tiles, G.d_nout,
-                                                    net.g + kLpWOff[3]);
+    if (net.tensor_cores) {
+        const int rc = lp_out_wgrad_tc(G, net.dil[3], gz, acts[2], d_inv_s, sign, net.g + kLpWOff[3], net.err, net.sms, st);
+        if (rc != FLIP_OK) return rc;
+    } else {
+        lp_wgrad_kernel<2, 16, 1><<<grid, 512, 0, st>>>(G, net.dil[3], gz, acts[2], d_inv_s, sign, G.out_tiles, G.d_nout,
+                                                        net.g + kLpWOff[3]);
+    }
     lp_out_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[3], net.dil[3], gz, acts[2], d_inv_s, sign, net.gact);
-    // layer 2 (16 -> 16): Gout = gact (wrt act[2]), input act[1]
-    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[2], net.gact, acts[1], d_inv_s, 1.0f, G.act_tiles, G.d_nact,
-                                                     net.g + kLpWOff[2]);
-    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.gact, acts[1], net.gact2);
-    // layer 1: Gout = gact2 (wrt act[1]), input act[0]
-    lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[1], net.gact2, acts[0], d_inv_s, 1.0f, G.act_tiles, G.d_nact,
-                                                     net.g + kLpWOff[1]);
-    lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.gact2, acts[0], net.gact);
+    if (net.tensor_cores) {
+        // layer 2 (16 -> 16): Gout = gact (wrt act[2]), input act[1]; then layer 1
+        int rc = lp_mid_wgrad_tc(G, net.dil[2], net.gact, acts[1], net.g + kLpWOff[2], net.err, net.sms, st);
+        if (rc == FLIP_OK)
+            rc = lp_mid_dgrad_tc(G, net.wb + kLpWOff[2], net.dil[2], net.gact, acts[1], net.gact2, net.err, net.sms, st);
+        if (rc == FLIP_OK) rc = lp_mid_wgrad_tc(G, net.dil[1], net.gact2, acts[0], net.g + kLpWOff[1], net.err, net.sms, st);
+        if (rc == FLIP_OK)
+            rc = lp_mid_dgrad_tc(G, net.wb + kLpWOff[1], net.dil[1], net.gact2, acts[0], net.gact, net.err, net.sms, st);
+        if (rc != FLIP_OK) return rc;
+    } else {
+        // layer 2 (16 -> 16): Gout = gact (wrt act[2]), input act[1]
+        lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[2], net.gact, acts[1], d_inv_s, 1.0f, G.act_tiles,
+                                                         G.d_nact, net.g + kLpWOff[2]);
+        lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[2], net.dil[2], net.gact, acts[1], net.gact2);
+        // layer 1: Gout = gact2 (wrt act[1]), input act[0]
+        lp_wgrad_kernel<1, 16, 16><<<grid, 512, 0, st>>>(G, net.dil[1], net.gact2, acts[0], d_inv_s, 1.0f, G.act_tiles,
+                                                         G.d_nact, net.g + kLpWOff[1]);
+        lp_mid_dgrad_kernel<<<grid, 512, 0, st>>>(G, net.wb + kLpWOff[1], net.dil[1], net.gact2, acts[0], net.gact);
+    }
     // layer 0: Gout = gact (wrt act[0]), input = the three channels
-    lp_wgrad_kernel<0, 3, 16><<<grid, 512, 0, st>>>(G, net.dil[0], net.gact, nullptr, d_inv_s, 1.0f, G.act_tiles, G.d_nact,
-                                                    net.g + kLpWOff[0]);
+    if (net.tensor_cores) {
+        const int rc = lp_in_wgrad_tc(G, net.dil[0], net.gact, d_inv_s, net.g + kLpWOff[0], net.err, net.sms, st);
+        if (rc != FLIP_OK) return rc;
+    } else {
+        lp_wgrad_kernel<0, 3, 16><<<grid, 512, 0, st>>>(G, net.dil[0], net.gact, nullptr, d_inv_s, 1.0f, G.act_tiles,
+                                                        G.d_nact, net.g + kLpWOff[0]);
+    }
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }

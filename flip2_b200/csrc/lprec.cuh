@@ -32,7 +32,7 @@ struct LpNet {
     float* gact;          // gradient of one activation layer: [slot][16]
     float* gact2;         // second gradient buffer: [slot][16]
     int adam_t;
-    int tensor_cores;     // 1: the 16 -> 16 layers of the forward pass run on tcgen05
+    int tensor_cores;     // 1: the 16 -> 16 layers run on tcgen05 (forward and backward)
     int sms;              // SM count (persistent grid of the tensor-core kernels)
     int* err;             // device error word of the tensor-core kernels (bit 0: a wait timed out)
 };
@@ -83,6 +83,20 @@ int lp_small_forward(const LpNet& net, const LpGrid& G, uint32_t ntiles, const f
 // the slots of the active tiles, zero off fluid cells), through both the
 // f(r/s) and the f(0) activations; accumulates into net.g (caller zeroes it)
 int lp_backward_dev(LpNet& net, const LpGrid& G, const float* d_inv_s, const float* gz, int grid, cudaStream_t st);
+// the backward pass of one 16 -> 16 layer on the tensor cores (lprec_tc.cu),
+// over the voxels of the active list: gin = relu'(ain) * (the gradient of the
+// layer's input from gout), and dw += the weight gradient (FP32 atomics)
+int lp_mid_dgrad_tc(const LpGrid& G, const __nv_bfloat16* wb, int dil, const float* gout, const __nv_bfloat16* ain,
+                    float* gin, int* err, int sms, cudaStream_t st);
+int lp_mid_wgrad_tc(const LpGrid& G, int dil, const float* gout, const __nv_bfloat16* ain, float* dw, int* err, int sms,
+                    cudaStream_t st);
+// the weight gradients of the input layer (3 -> 16; its input channels from
+// G.r, G.type and the scale) and of the output layer (16 -> 1; dL/dout =
+// sign * s * gz on the output tiles) on the tensor cores
+int lp_in_wgrad_tc(const LpGrid& G, int dil, const float* gout, const float* d_inv_s, float* dw, int* err, int sms,
+                   cudaStream_t st);
+int lp_out_wgrad_tc(const LpGrid& G, int dil, const float* gz, const __nv_bfloat16* ain, const float* d_inv_s, float sign,
+                    float* dw, int* err, int sms, cudaStream_t st);
 // training loss of the preconditioner M(r) = N(r) + D^-1 r for a sample
 // (r, e) with A e = r: L = |M(r) - e|_A^2 / |e|_A^2 = (m.Am - 2 m.r)/e.r + 1.
 // Accumulates m.Am, m.r, e.r into d_sums[0..2] (caller zeroes them), keeps

@@ -1,14 +1,15 @@
 """Run a few native steps of the dam-break scene and print per-stage times.
 
     python -m flip2_b200.profile_step [--cells 256] [--steps 2] [--dt 1/480]
-        [--method 0|1|2] [--poisson K]
+        [--method 0|1|2] [--poisson K] [--lp-grad K] [--lp-cuda-cores 0|1]
 
 The scene is the benchmark's (block 0.5 x 0.5 x 1 of the unit box, 8
 jittered particles per voxel, seed 0).  Each step runs in full; stage times
 come from CUDA events on the engine stream.  --method picks the pressure
 solve (1 and 2 load the committed weights of the learned preconditioner);
 --poisson K solves K generated pressure problems of the grid (seeds 900000
-and up) with that method instead of stepping.  Short enough to run under a
+and up) with that method instead of stepping; --lp-grad K evaluates the
+network's training loss and weight gradient K times.  Short enough to run under a
 profiler with a kernel filter.
 """
 import argparse
@@ -22,6 +23,33 @@ from . import MODE_NATIVE, Particles, default_params, scenes
 WEIGHTS = {1: "lprec_weights.npy", 2: "mg_weights.npy"}
 
 
+def lp_grad(args, params, R):
+    """--lp-grad K: K evaluations of the network's training loss and weight
+    gradient on a cells^3 problem (fluid below 0.7 of the height, 8% random
+    solid cells, seed 3; random weights and residuals), with the 16 -> 16
+    layers on tcgen05 unless --lp-cuda-cores 1."""
+    import time
+    n = args.cells
+    rng = np.random.default_rng(3)
+    j = np.arange(n)[None, :, None] * np.ones((n, n, n))
+    typ = np.where(j < 0.7 * n, 1, 0).astype(np.uint8)
+    typ[rng.random(typ.shape) < 0.08] = 2
+    typ = typ.ravel()
+    r = (rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    ev = (r + 0.5 * rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    P = Particles(1, mode=MODE_NATIVE, params=params)
+    P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)
+    P.poisson_set(typ, np.zeros(typ.size, np.float32))
+    from . import lib
+    P.lp_set_weights((rng.standard_normal(lib().flip_lp_num_weights()) * 0.15).astype(np.float32))
+    for k in range(args.lp_grad):
+        t0 = time.perf_counter()
+        _, loss = P.lp_eval(r, ev, want_grad=True)
+        print(json.dumps({"lp_grad": k, "cells": n, "loss": loss, "ms_with_transfers": round(1e3 * (time.perf_counter() - t0), 3),
+                          "error_flags": P.info().error_flags}))
+    P.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cells", type=int, default=256)
@@ -31,9 +59,13 @@ def main():
     ap.add_argument("--method", type=int, default=0, choices=(0, 1, 2))
     ap.add_argument("--lp-cuda-cores", type=int, default=0)
     ap.add_argument("--poisson", type=int, default=0)
+    ap.add_argument("--lp-grad", type=int, default=0)
     args = ap.parse_args()
     params = default_params(MODE_NATIVE, pressure_method=args.method, lp_cuda_cores=args.lp_cuda_cores)
     R = args.cells // 4
+    if args.lp_grad:
+        lp_grad(args, params, R)
+        return
     if args.poisson:
         P = Particles(1, mode=MODE_NATIVE, params=params)
         P.setDomain(0.0, 0.0, 0.0, R, R, R, 1.0)

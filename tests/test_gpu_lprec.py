@@ -127,6 +127,34 @@ def test_lp_tensor_cores_match_cuda_cores(torch):
     assert rel_err(zs[0], zs[1]) <= 1e-2
 
 
+@pytest.mark.parametrize("shape,seed", [((64, 48, 40), 7), ((24, 16, 40), 8)])
+def test_lp_backward_tensor_cores_match_cuda_cores(torch, shape, seed):
+    # the weight gradient with the 16 -> 16 layers' backward pass on tcgen05
+    # (input gradients rounded to BF16 as MMA operands; the weight gradient
+    # takes the output gradient as a BF16 pair, FP32 accumulation) against
+    # the CUDA-core kernels (FP32 throughout), forward and backward of each
+    # run on its own path
+    typ = random_types(shape, seed)
+    rng = np.random.default_rng(seed + 1)
+    r = (rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    ev = (r + 0.5 * rng.standard_normal(typ.size) * (typ == 1)).astype(np.float32)
+    w = (rng.standard_normal(F.lib().flip_lp_num_weights()) * 0.15).astype(np.float32)
+    gs = []
+    for cc in (0, 1):
+        P = engine(shape, lp_cuda_cores=cc)
+        P.poisson_set(typ, np.zeros(typ.size, np.float32))
+        P.lp_set_weights(w)
+        P.lp_eval(r, ev, want_grad=True)
+        assert P.info().error_flags == 0
+        gs.append(P.lp_grad())
+        P.close()
+    offs = [0, 27 * 3 * 16, 27 * 3 * 16 + 27 * 256, 27 * 3 * 16 + 2 * 27 * 256, gs[0].size]
+    assert np.linalg.norm(gs[0] - gs[1]) <= 3e-3 * np.linalg.norm(gs[1])
+    for l in range(4):
+        a, b = gs[0][offs[l]:offs[l + 1]], gs[1][offs[l]:offs[l + 1]]
+        assert np.linalg.norm(a - b) <= 5e-3 * np.linalg.norm(b), l
+
+
 # ------------------------------------------------------ pressure problems
 def test_generated_problem_pcg_vs_oracle(torch):
     shape = (64, 64, 64)
