@@ -101,6 +101,33 @@ __device__ __forceinline__ bool ref_tile_solid(uint32_t i, uint32_t gx, uint32_t
     return false;
 }
 
+// true when ref_tile_solid is false for every voxel of the tile: its voxel
+// coordinates run over gx*8 .. gx*8+7 in x and y (the y index is the x index)
+// and gz*8 .. gz*8+7 in z, and the test is monotone in each, so the tile's
+// corners decide (tiles away from the domain faces, nearly all of them)
+__device__ __forceinline__ bool ref_tile_clear(uint32_t gx, uint32_t gy, uint32_t gz, const flip_grid& g) {
+    const double fr = 2.0;
+    if ((double)(gx * 8u) < fr || (double)(gy * 8u) < fr || (double)(gz * 8u) < fr) return false;
+    if ((double)(gx * 8u + 7u) > (double)(g.sizeX * 8u) + fr || (double)(gy * 8u + 7u) > (double)(g.sizeY * 8u) + fr ||
+        (double)(gz * 8u + 7u) > (double)(g.sizeZ * 8u) + fr)
+        return false;
+    return true;
+}
+
+// ref_dist(dx, dy, dz) < R without the square root where the sum of squares
+// s decides it: the square root is correctly rounded and monotone, so it
+// comes out below R exactly when s lies below the square of the midpoint
+// between R and the double below R, which is within a relative 2^-52 of R^2.
+// s below lo = R^2 (1 - 2^-48) is inside, s at or above hi = R^2 (1 + 2^-48)
+// is outside (both bounds hold with the roundings of R^2 and of the
+// products); in the band between, the square root decides, as in ref_dist.
+__device__ __forceinline__ bool ref_within(double dx, double dy, double dz, double R, double lo, double hi) {
+    const double s = fma(dx, dx, fma(dy, dy, dz * dz));
+    if (s < lo) return true;
+    if (s >= hi) return false;
+    return sqrt(s) < R;
+}
+
 struct RefLocal {
     double lx, ly, lz;
     uint32_t sx, sy, sz;
@@ -121,8 +148,10 @@ __device__ __forceinline__ RefLocal ref_particle_local(const double* px, const d
 
 // getNumberVoxelsUsedPerNode (particles.cu:88-190): mask + count per node.
 // A warp per node (kVoxWarps nodes per CTA): the 512 solid tests as 16
-// ballots, then the node's particles one after the other, the 64 points of a
-// particle's 4 x 4 x 4 stencil spread over the lanes (two each).  The tests
+// ballots (none for a tile away from the domain faces, whose tests all
+// fail), then the node's particles in order, the 64 points of a particle's
+// 4 x 4 x 4 stencil spread over the lanes (two each); a lane loads and
+// prepares one particle of each round of 32, so the loads overlap.  The tests
 // and their arithmetic are the reference's; only the work is spread.  Its
 // loops run x from sx - 2 while (unsigned) x < sx + 2, so a stencil
 // coordinate below 2 on any axis leaves a particle without marks, and points
@@ -137,31 +166,54 @@ __global__ void __launch_bounds__(32 * kVoxWarps) ref_voxel_counts_kernel(
     const uint32_t b = blockIdx.x * kVoxWarps + (uint32_t)w;
     if (b >= nodes) return;  // a whole warp; nothing below synchronises the CTA
     uint32_t* M = mark[w];
+    // the node's particle range, loaded with the key below
+    const uint32_t first = starts[b], last = (b == nodes - 1) ? (uint32_t)n : starts[b + 1];
     uint32_t gx, gy, gz;
     ref_decompose(keys[b], g, gx, gy, gz);  // Q3: particle b's key, not the node's
+    if (ref_tile_clear(gx, gy, gz, g)) {
+        if (lane < 16) M[lane] = 0u;
+    } else {
 #pragma unroll 4
-    for (int q = 0; q < 16; ++q) {
-        const uint32_t bits = __ballot_sync(0xffffffffu, ref_tile_solid((uint32_t)(q * 32 + lane), gx, gy, gz, g));
-        if (lane == 0) M[q] = bits;
+        for (int q = 0; q < 16; ++q) {
+            const uint32_t bits = __ballot_sync(0xffffffffu, ref_tile_solid((uint32_t)(q * 32 + lane), gx, gy, gz, g));
+            if (lane == 0) M[q] = bits;
+        }
     }
     __syncwarp();
-    const uint32_t last = (b == nodes - 1) ? (uint32_t)n : starts[b + 1];
     const double scw = ref_scw(g), hs = scw / 2.0, R = 2.0 * scw;
-    for (uint32_t idx = starts[b]; idx < last; ++idx) {
-        const RefLocal L = ref_particle_local(px, py, pz, keys, idx, g, scw);
-        if (L.sx < 2u || L.sy < 2u || L.sz < 2u) continue;
+    const double R2 = R * R, lo = R2 * (1.0 - 0x1p-48), hi = R2 * (1.0 + 0x1p-48);
+    // up to 32 of the node's particles at a time: lane j loads particle j and
+    // works out its local coordinates (the loads and divisions of all of
+    // them in one round), then the warp walks them in order, each lane
+    // taking two of the 64 points of the particle's stencil
+    for (uint32_t i0 = first; i0 < last; i0 += 32u) {
+        RefLocal Lj{};
+        bool ok = false;
+        if (i0 + (uint32_t)lane < last) {
+            Lj = ref_particle_local(px, py, pz, keys, i0 + (uint32_t)lane, g, scw);
+            ok = !(Lj.sx < 2u || Lj.sy < 2u || Lj.sz < 2u);
+        }
+        for (uint32_t live = __ballot_sync(0xffffffffu, ok); live; live &= live - 1u) {
+            const int j = __ffs(live) - 1;
+            RefLocal L;
+            L.lx = __shfl_sync(0xffffffffu, Lj.lx, j);
+            L.ly = __shfl_sync(0xffffffffu, Lj.ly, j);
+            L.lz = __shfl_sync(0xffffffffu, Lj.lz, j);
+            L.sx = __shfl_sync(0xffffffffu, Lj.sx, j);
+            L.sy = __shfl_sync(0xffffffffu, Lj.sy, j);
+            L.sz = __shfl_sync(0xffffffffu, Lj.sz, j);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int pt = lane + 32 * h;
-            const int x = (int)(L.sx - 2u) + (pt >> 4), y = (int)(L.sy - 2u) + ((pt >> 2) & 3), z = (int)(L.sz - 2u) + (pt & 3);
-            if ((uint32_t)x >= 8u || (uint32_t)y >= 8u || (uint32_t)z >= 8u) continue;
-            const double dx = L.lx - x * scw, dy = L.ly - y * scw, dz = L.lz - z * scw;
-            const double xc = ref_dist(dx, dy + hs, dz + hs);
-            const double yc = ref_dist(dx + hs, dy, dz + hs);
-            const double zc = ref_dist(dx + hs, dy + hs, dz);
-            if (xc < R || yc < R || zc < R) {
-                const int v = x + y * 8 + z * 64;
-                atomicOr(&M[v >> 5], 1u << (v & 31));
+            for (int h = 0; h < 2; ++h) {
+                const int pt = lane + 32 * h;
+                const int x = (int)(L.sx - 2u) + (pt >> 4), y = (int)(L.sy - 2u) + ((pt >> 2) & 3),
+                          z = (int)(L.sz - 2u) + (pt & 3);
+                if ((uint32_t)x >= 8u || (uint32_t)y >= 8u || (uint32_t)z >= 8u) continue;
+                const double dx = L.lx - x * scw, dy = L.ly - y * scw, dz = L.lz - z * scw;
+                if (ref_within(dx, dy + hs, dz + hs, R, lo, hi) || ref_within(dx + hs, dy, dz + hs, R, lo, hi) ||
+                    ref_within(dx + hs, dy + hs, dz, R, lo, hi)) {
+                    const int v = x + y * 8 + z * 64;
+                    atomicOr(&M[v >> 5], 1u << (v & 31));
+                }
             }
         }
     }
@@ -195,14 +247,16 @@ __global__ void __launch_bounds__(32 * kVoxWarps) ref_voxel_ids_kernel(
     ref_decompose(keys[b], g, gx, gy, gz);
     const uint32_t start = b ? node_voxels[b - 1] : 0u;
     const uint32_t below = (1u << lane) - 1u;
-#pragma unroll 4
-    for (int q = 0; q < 16; ++q) {
+    const bool clear = ref_tile_clear(gx, gy, gz, g);
+    // the mask words that hold a voxel, in order
+    for (uint32_t rest = __ballot_sync(0xffffffffu, m != 0u); rest; rest &= rest - 1u) {
+        const int q = __ffs(rest) - 1;
         const uint32_t word = __shfl_sync(0xffffffffu, m, q), base = __shfl_sync(0xffffffffu, pre, q);
         if ((word >> lane) & 1u) {
             const uint32_t i = (uint32_t)(q * 32 + lane);
             const uint32_t pos = start + base + __popc(word & below);
             voxel_ids[pos] = i;
-            solids[pos] = ref_tile_solid(i, gx, gy, gz, g) ? 1 : 0;
+            solids[pos] = (!clear && ref_tile_solid(i, gx, gy, gz, g)) ? 1 : 0;
         }
     }
 }

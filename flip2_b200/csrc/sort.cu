@@ -7,9 +7,9 @@
 //
 // Structure (Adinets & Merrill's onesweep):
 //   1. one upfront pass reads every key once and builds all digit histograms
-//      (warp-aggregated shared-memory atomics via __match_any_sync);
+//      (shared-memory atomics into one histogram per warp);
 //   2. one kernel per 8-bit digit: each CTA claims the next tile of 4096 keys
-//      from an atomic counter, ranks its keys per warp with match/ballot,
+//      from an atomic counter, ranks its keys per warp with ballots,
 //      publishes its per-digit counts and resolves its global offsets with a
 //      decoupled look-back over the predecessor tiles, then scatters through
 //      shared memory so that global writes are runs of consecutive addresses.
@@ -24,6 +24,7 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 4;
+constexpr int kLook = 8;  // predecessors a look-back step reads at once
 
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
@@ -49,31 +50,52 @@ static SortLayout sort_layout(uint64_t n) {
     return L;
 }
 
+// The lanes of the warp whose 8-bit digit equals this lane's, from eight
+// ballots (one per digit bit); every lane of the warp takes part.  Same
+// result as __match_any_sync on the digit, which issues far more slowly.
+__device__ __forceinline__ uint32_t warp_match8(uint32_t d) {
+    uint32_t m = 0xFFFFFFFFu;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t v = __ballot_sync(0xFFFFFFFFu, bit);
+        m &= bit ? v : ~v;
+    }
+    return m;
+}
+
 // ----------------------------------------------------------- histogram
+// Each thread counts kHistItems keys per round (loads issued together) with
+// one shared atomic per key and digit into its warp's own histogram: the
+// digits of blob-concentrated keys would otherwise have every warp of the
+// block adding into the same few words.
+constexpr int kHistItems = 8;
 __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint32_t* __restrict__ keys, uint64_t n,
                                                                       int passes, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t sh[kMaxPasses][kRadix];
-    for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+    __shared__ uint32_t sh[kSortWarps][kMaxPasses][kRadix];
+    for (int i = threadIdx.x; i < kSortWarps * kMaxPasses * kRadix; i += blockDim.x) (&sh[0][0][0])[i] = 0;
     __syncthreads();
-    const uint32_t lt = lanemask_lt();
+    const int warp = threadIdx.x >> 5;
+    uint32_t* H = &sh[warp][0][0];
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    // every lane of a warp iterates the same number of times, so the
-    // warp-synchronous match below always sees a full warp
-    const uint64_t nround = (n + stride - 1) / stride;
-    for (uint64_t r = 0; r < nround; ++r) {
-        uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        bool valid = i < n;
-        uint32_t k = valid ? keys[i] : 0u;
-        uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-        for (int p = 0; p < passes; ++p) {
-            uint32_t d = (k >> (8 * p)) & 0xFFu;
-            uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u | d) & vmask;
-            if (valid && (peers & lt) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * kHistItems) {
+        uint32_t k[kHistItems];
+#pragma unroll
+        for (int j = 0; j < kHistItems; ++j) {
+            const uint64_t i = i0 + (uint64_t)j * stride;
+            k[j] = i < n ? keys[i] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kHistItems; ++j) {
+            if (i0 + (uint64_t)j * stride >= n) continue;
+            for (int p = 0; p < passes; ++p) atomicAdd(H + p * kRadix + ((k[j] >> (8 * p)) & 0xFFu), 1u);
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
-        uint32_t v = (&sh[0][0])[i];
+        uint32_t v = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) v += (&sh[w][0][0])[i];
         if (v) atomicAdd(&hist[i], v);
     }
 }
@@ -127,7 +149,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         uint32_t d = (key[i] >> shift) & 0xFFu;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t peers = warp_match8(d);
         uint32_t before = __popc(peers & lt);
         uint32_t prev = s_whist[warp][d];
         __syncwarp();
@@ -152,21 +174,37 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         st_relaxed_u32(st, kFlagPrefix | run);
     } else {
         st_relaxed_u32(st, kFlagAgg | run);
+        // walk back kLook predecessors per poll (independent loads, one round
+        // trip): add their aggregates in order up to the first inclusive
+        // prefix; from a predecessor that has published nothing yet, poll
+        // again (a bounded number of times)
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (t >= 0) {
-            uint32_t s = ld_relaxed_u32(status + (size_t)t * kRadix + d);
-            uint32_t f = s & ~kValueMask;
-            if (f == 0) {
-                if (++spins > spin_limit) {
-                    atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
-                    break;
+            uint32_t sv[kLook];
+#pragma unroll
+            for (int j = 0; j < kLook; ++j)
+                sv[j] = (t - j >= 0) ? ld_relaxed_u32(status + (size_t)(t - j) * kRadix + d) : 0u;
+            int used = 0;
+            bool prefix = false, wait = false;
+#pragma unroll
+            for (int j = 0; j < kLook; ++j) {
+                if (prefix || wait || t - j < 0) continue;
+                const uint32_t f = sv[j] & ~kValueMask;
+                if (f == 0) {
+                    wait = true;
+                    continue;
                 }
-                continue;
+                excl += sv[j] & kValueMask;
+                ++used;
+                prefix = f == kFlagPrefix;
             }
-            excl += s & kValueMask;
-            if (f == kFlagPrefix) break;
-            --t;
+            if (prefix) break;
+            t -= used;
+            if (wait && ++spins > spin_limit) {
+                atomicOr(err, DEVERR_LOOKBACK_TIMEOUT);
+                break;
+            }
         }
         st_relaxed_u32(st, kFlagPrefix | ((excl + run) & kValueMask));
     }

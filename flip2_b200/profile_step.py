@@ -2,6 +2,7 @@
 
     python -m flip2_b200.profile_step [--cells 256] [--steps 2] [--dt 1/480]
         [--method 0|1|2] [--poisson K] [--lp-grad K] [--lp-cuda-cores 0|1]
+        [--binning N]
 
 The scene is the benchmark's (block 0.5 x 0.5 x 1 of the unit box, 8
 jittered particles per voxel, seed 0).  Each step runs in full; stage times
@@ -9,7 +10,8 @@ come from CUDA events on the engine stream.  --method picks the pressure
 solve (1 and 2 load the committed weights of the learned preconditioner);
 --poisson K solves K generated pressure problems of the grid (seeds 900000
 and up) with that method instead of stepping; --lp-grad K evaluates the
-network's training loss and weight gradient K times.  Short enough to run under a
+network's training loss and weight gradient K times; --binning N runs the
+reference-mode binning of N particles of the binning microbenchmark.  Short enough to run under a
 profiler with a kernel filter.
 """
 import argparse
@@ -50,6 +52,37 @@ def lp_grad(args, params, R):
     P.close()
 
 
+def binning(args):
+    """--binning N: the reference-mode binning of N particles in a 512^3
+    domain (50% uniform, 50% in 16 Gaussian blobs of sigma 8, seed 1; FP64
+    positions): alignParticlesToGrid, sortParticles and generateVoxels,
+    --steps times, each from the unsorted input, timed with CUDA events."""
+    import torch
+    from . import MODE_REFERENCE
+    pos = scenes.binning_mix(args.binning, domain=512, seed=1).astype(np.float64)
+    host = tuple(np.ascontiguousarray(pos[:, k]) for k in range(3))
+    del pos
+    stream = torch.cuda.Stream()
+    P = Particles(args.binning, mode=MODE_REFERENCE, params=default_params(MODE_REFERENCE), stream=stream.cuda_stream)
+    P.setDomain(0.0, 0.0, 0.0, 512, 512, 512, 1.0)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for k in range(args.steps):
+        P.upload(host, None)
+        P.sync()
+        ev[0].record(stream)
+        P.alignParticlesToGrid()
+        ev[1].record(stream)
+        P.sortParticles()
+        ev[2].record(stream)
+        P.generateVoxels()
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"binning": k, "particles": args.binning, "align_ms": ev[0].elapsed_time(ev[1]),
+                          "sort_ms": ev[1].elapsed_time(ev[2]), "voxels_ms": ev[2].elapsed_time(ev[3]),
+                          "voxels": P.info().voxels}))
+    P.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cells", type=int, default=256)
@@ -60,11 +93,15 @@ def main():
     ap.add_argument("--lp-cuda-cores", type=int, default=0)
     ap.add_argument("--poisson", type=int, default=0)
     ap.add_argument("--lp-grad", type=int, default=0)
+    ap.add_argument("--binning", type=int, default=0)
     args = ap.parse_args()
     params = default_params(MODE_NATIVE, pressure_method=args.method, lp_cuda_cores=args.lp_cuda_cores)
     R = args.cells // 4
     if args.lp_grad:
         lp_grad(args, params, R)
+        return
+    if args.binning:
+        binning(args)
         return
     if args.poisson:
         P = Particles(1, mode=MODE_NATIVE, params=params)
