@@ -584,6 +584,30 @@ def main():
     part_ms = sum(stages[k] for k in part_keys)
     particle_stages = {"value": n / (part_ms / 1e3), "unit": METRIC, "ms_per_step": part_ms, "stages": part_keys,
                        "note": "stage times from CUDA events of the profiled steps; excludes pressure and projection"}
+    # algorithmic bytes per stage (per particle p, per active voxel v of the
+    # fluid tiles) and the bandwidth they make of the stage's CUDA-event time
+    it_step = pcg_iters / nprof
+    stage_bytes = {
+        "sort": 36.0 * n,                     # histogram 4 B + 2 onesweep passes x 16 B (tile keys)
+        "gather": 52.0 * n,                   # permutation 4 B + 24 B read + 24 B write
+        "segment_heads": 4.0 * n + 8.0 * fluid_tiles,
+        "p2g": 24.0 * n + 24.0 * voxels,      # state read; momentum and weight per face written
+        "g2p_advect": 52.0 * n + 24.0 * voxels,  # state read, state + next key written; new and old faces read
+        "pcg_iterations": per_voxel * voxels * it_step,
+        "projection": 29.0 * voxels,
+    }
+    stages_gbs = {}
+    for k, b in stage_bytes.items():
+        if stages.get(k, 0.0) > 0.0:
+            g = b / (stages[k] / 1e3) / 1e9
+            stages_gbs[k] = {"ms": stages[k], "bytes": b, "gbs": g, "frac": g / peak}
+    # the survey's headline figure for the particle stages: P2G + G2P/advect,
+    # 72 B per particle + 40 B per active voxel
+    pg_ms = stages["p2g"] + stages["g2p_advect"]
+    pg_bytes = 72.0 * n + 40.0 * voxels
+    particle_stages["p2g_g2p"] = {"ms": pg_ms, "algorithmic_bytes": pg_bytes, "gbs": pg_bytes / (pg_ms / 1e3) / 1e9,
+                                  "frac": pg_bytes / (pg_ms / 1e3) / 1e9 / peak,
+                                  "particle_steps_per_s": n / (pg_ms / 1e3)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not c5:
@@ -612,7 +636,7 @@ def main():
                 "particle_stages": particle_stages, "c4_pressure": c4, "c3_binning": c3, "c5_learned": c5_block,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
                 "pcg_iters_per_step": iters, "pressure_solve_ms": stages["pcg_setup"] + stages["pcg_iterations"],
-                "stages_ms": stages, "fluid_tiles": fluid_tiles,
+                "stages_ms": stages, "stages_gbs": stages_gbs, "fluid_tiles": fluid_tiles,
                 "pcg_rel_residual": info.residual, "error_flags": info.error_flags,
                 "graph_steps": info.graph_steps}
         if c5:

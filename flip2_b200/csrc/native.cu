@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
                 }
             __syncthreads();
             const uint32_t b0 = S.off[tid], b1 = b0 + S.cnt[tid];
-#pragma unroll 1
+            // the three components unrolled: every axis choice below is a constant
+#pragma unroll
             for (int comp = 0; comp < 3; ++comp) {
                 // the component's own axis and the two others in order (a1 < a2)
                 const int no = comp == 0 ? D.nx : (comp == 1 ? D.ny : D.nz);

@@ -9,7 +9,7 @@
 //   1. one upfront pass reads every key once and builds all digit histograms
 //      (shared-memory atomics into one histogram per warp);
 //   2. one kernel per 8-bit digit: each CTA claims the next tile of 4096 keys
-//      from an atomic counter, ranks its keys per warp with ballots,
+//      from an atomic counter, ranks its keys per warp with match/ballot,
 //      publishes its per-digit counts and resolves its global offsets with a
 //      decoupled look-back over the predecessor tiles, then scatters through
 //      shared memory so that global writes are runs of consecutive addresses.
@@ -50,25 +50,13 @@ static SortLayout sort_layout(uint64_t n) {
     return L;
 }
 
-// The lanes of the warp whose 8-bit digit equals this lane's, from eight
-// ballots (one per digit bit); every lane of the warp takes part.  Same
-// result as __match_any_sync on the digit, which issues far more slowly.
-__device__ __forceinline__ uint32_t warp_match8(uint32_t d) {
-    uint32_t m = 0xFFFFFFFFu;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const bool bit = (d >> b) & 1u;
-        const uint32_t v = __ballot_sync(0xFFFFFFFFu, bit);
-        m &= bit ? v : ~v;
-    }
-    return m;
-}
-
 // ----------------------------------------------------------- histogram
-// Each thread counts kHistItems keys per round (loads issued together) with
-// one shared atomic per key and digit into its warp's own histogram: the
-// digits of blob-concentrated keys would otherwise have every warp of the
-// block adding into the same few words.
+// Each thread counts kHistItems keys per round (loads issued together) into
+// its warp's own histogram: the digits of blob-concentrated keys would
+// otherwise have every warp of the block adding into the same few words.  A
+// digit the whole warp shares (keys sorted or nearly so, as the tile keys of
+// consecutive steps are) takes one atomic for the warp; otherwise each lane
+// adds its own.
 constexpr int kHistItems = 8;
 __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint32_t* __restrict__ keys, uint64_t n,
                                                                       int passes, uint32_t* __restrict__ hist) {
@@ -78,7 +66,9 @@ __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint
     const int warp = threadIdx.x >> 5;
     uint32_t* H = &sh[warp][0][0];
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * kHistItems) {
+    // the warp's lanes take the same number of rounds (the votes below need all of them)
+    for (uint64_t w0 = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < n; w0 += stride * kHistItems) {
+        const uint64_t i0 = w0 + (threadIdx.x & 31u);
         uint32_t k[kHistItems];
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
@@ -87,8 +77,17 @@ __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint
         }
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
-            if (i0 + (uint64_t)j * stride >= n) continue;
-            for (int p = 0; p < passes; ++p) atomicAdd(H + p * kRadix + ((k[j] >> (8 * p)) & 0xFFu), 1u);
+            const bool valid = i0 + (uint64_t)j * stride < n;
+            const uint32_t nvalid = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
+            for (int p = 0; p < passes; ++p) {
+                const uint32_t d = (k[j] >> (8 * p)) & 0xFFu;
+                const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
+                if (__all_sync(0xffffffffu, !valid || d == d0)) {
+                    if ((threadIdx.x & 31) == 0 && nvalid) atomicAdd(H + p * kRadix + d0, nvalid);
+                } else if (valid) {
+                    atomicAdd(H + p * kRadix + d, 1u);
+                }
+            }
         }
     }
     __syncthreads();
@@ -149,7 +148,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         uint32_t d = (key[i] >> shift) & 0xFFu;
-        uint32_t peers = warp_match8(d);
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = __popc(peers & lt);
         uint32_t prev = s_whist[warp][d];
         __syncwarp();
