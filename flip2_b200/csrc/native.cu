@@ -675,14 +675,16 @@ __device__ __forceinline__ int64_t halo_at(const HaloSlot& h, uint32_t key, uint
 // independent groups of 128; each group walks its own tiles and syncs on its
 // own named barrier.  A thread owns four consecutive x-cells of one (y, z) row
 // (float4 loads and stores) and three of the tile's 384 halo cells.  The
-// tile's p' goes to a 10 x 10 x 16-float shared box (rows padded so that
-// x = 0 and x = 4 start on 16 bytes; x = -1 .. 8 at row offsets 3 .. 12),
+// tile's p' goes to a 10 x 10 x 24-float shared box (rows padded so that
+// x = 0 and x = 4 start on 16 bytes, x = -1 .. 8 at row offsets 3 .. 12, and
+// so that the 16-byte row accesses of a quarter warp, four consecutive rows,
+// fall on distinct banks),
 // two boxes per group alternating per tile, and the stencil reads its y and
 // z neighbours as 16-byte rows.  Loads of the group's next tile are issued
 // before the current tile's barrier.
 constexpr int kDm4Groups = 4;
 constexpr int kDm4Blocks = 296;  // 148 SMs x 2 CTAs
-constexpr int kBoxRow = 16;
+constexpr int kBoxRow = 24;  // 96 B rows: four consecutive rows start 8 banks apart
 constexpr int kBoxFloats = 10 * 10 * kBoxRow;
 __device__ __forceinline__ int box_at(int x, int y, int z) { return ((z + 1) * 10 + (y + 1)) * kBoxRow + x + 4; }
 
