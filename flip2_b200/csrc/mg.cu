@@ -192,19 +192,37 @@ __device__ __forceinline__ float4 mg_quad_sweep(uint32_t c4, const float4& u, co
     return o;
 }
 // neighbour sums of the quad at float index b of a box of row stride SY and
-// plane stride SZ (rows of 16 floats); qd = the quad's place in its row
+// plane stride SZ (rows of 16 floats), c its own values, l and r the cells
+// left of its first and right of its last.  The x neighbours come from the
+// neighbouring lanes rather than from scalar shared loads, which hit their
+// banks four times over:
+//   mg_quad_nb_row: the four quads of a row sit in four consecutive active
+//     lanes (qd = the quad's place in its row; the first sweep's layout);
+//   mg_quad_nb_pair: quads 1 and 2 of a row sit in lanes 2k, 2k + 1 of a full
+//     warp (the second sweep's layout); the outer neighbour still comes from
+//     shared memory.
 template <int SY, int SZ>
-__device__ __forceinline__ float4 mg_quad_nb(const float* v, int b, int qd) {
-    const float4 c = *reinterpret_cast<const float4*>(v + b);
+__device__ __forceinline__ float4 mg_quad_nb_yz(const float* v, int b, const float4& c, float l, float r) {
     const float4 ym = *reinterpret_cast<const float4*>(v + b - SY), yp = *reinterpret_cast<const float4*>(v + b + SY);
     const float4 zm = *reinterpret_cast<const float4*>(v + b - SZ), zp = *reinterpret_cast<const float4*>(v + b + SZ);
-    const float l = qd > 0 ? v[b - 1] : 0.0f, r = qd < 3 ? v[b + 4] : 0.0f;
     float4 s;
     s.x = ((l + c.y) + (ym.x + yp.x)) + (zm.x + zp.x);
     s.y = ((c.x + c.z) + (ym.y + yp.y)) + (zm.y + zp.y);
     s.z = ((c.y + c.w) + (ym.z + yp.z)) + (zm.z + zp.z);
     s.w = ((c.z + r) + (ym.w + yp.w)) + (zm.w + zp.w);
     return s;
+}
+template <int SY, int SZ>
+__device__ __forceinline__ float4 mg_quad_nb_row(const float* v, int b, int qd, const float4& c) {
+    const unsigned m = __activemask();
+    const float l = __shfl_up_sync(m, c.w, 1), r = __shfl_down_sync(m, c.x, 1);
+    return mg_quad_nb_yz<SY, SZ>(v, b, c, qd > 0 ? l : 0.0f, qd < 3 ? r : 0.0f);
+}
+template <int SY, int SZ>
+__device__ __forceinline__ float4 mg_quad_nb_pair(const float* v, int b, int half, const float4& c) {
+    const float got = __shfl_xor_sync(0xffffffffu, half ? c.x : c.w, 1);
+    const float outer = v[b + (half ? 4 : -1)];
+    return mg_quad_nb_yz<SY, SZ>(v, b, c, half ? got : outer, half ? outer : got);
 }
 
 // pre-smoothing and restriction of level F into C:
@@ -275,8 +293,9 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
             const int qd = w & 3, row = w >> 2;
             const int by = row % 10 + 1, bz = row / 10 + 1;
             const int b = 4 * qd + kBX * (by + kBY * bz);
-            const float4 o = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(ub + b),
-                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * kBY>(ub, b, qd), inv);
+            const float4 uc = *reinterpret_cast<const float4*>(ub + b);
+            const float4 o = mg_quad_sweep(cb[b >> 2], uc, *reinterpret_cast<const float4*>(rb + b),
+                                           mg_quad_nb_row<kBX, kBX * kBY>(ub, b, qd, uc), inv);
             *reinterpret_cast<float4*>(tb + 4 * qd + kBX * (row % 10 + 10 * (row / 10))) = o;
         }
         __syncthreads();
@@ -287,7 +306,7 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_down_kernel(MgLevel F, MgLev
             const int t = 4 * qd + kBX * ((ly + 1) + 10 * (lz + 1));
             const uint32_t c4 = cb[b >> 2];
             const float4 tv = *reinterpret_cast<const float4*>(tb + t), r = *reinterpret_cast<const float4*>(rb + b);
-            const float4 nb = mg_quad_nb<kBX, kBX * 10>(tb, t, qd);
+            const float4 nb = mg_quad_nb_pair<kBX, kBX * 10>(tb, t, half, tv);
             float res[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -422,8 +441,9 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
             const int qd = w & 3, row = w >> 2;
             const int by = row % 10 + 1, bz = row / 10 + 1;
             const int b = 4 * qd + kBX * (by + kBY * bz);
-            const float4 o = mg_quad_sweep(cb[b >> 2], *reinterpret_cast<const float4*>(ub + b),
-                                           *reinterpret_cast<const float4*>(rb + b), mg_quad_nb<kBX, kBX * kBY>(ub, b, qd), inv);
+            const float4 uc = *reinterpret_cast<const float4*>(ub + b);
+            const float4 o = mg_quad_sweep(cb[b >> 2], uc, *reinterpret_cast<const float4*>(rb + b),
+                                           mg_quad_nb_row<kBX, kBX * kBY>(ub, b, qd, uc), inv);
             *reinterpret_cast<float4*>(tb + 4 * qd + kBX * (row % 10 + 10 * (row / 10))) = o;
         }
         __syncthreads();
@@ -437,8 +457,8 @@ __global__ void __launch_bounds__(kMgThreads, 5) mg_sweeps_kernel(MgLevel L, MgL
             if (DOT) q4 = *reinterpret_cast<const float4*>(dot.q + zs);
             const uint32_t c4 = cb[b >> 2];
             const float4 r4 = *reinterpret_cast<const float4*>(rb + b);
-            const float4 z = mg_quad_sweep(c4, *reinterpret_cast<const float4*>(tb + t), r4,
-                                           mg_quad_nb<kBX, kBX * 10>(tb, t, qd), inv);
+            const float4 tv = *reinterpret_cast<const float4*>(tb + t);
+            const float4 z = mg_quad_sweep(c4, tv, r4, mg_quad_nb_pair<kBX, kBX * 10>(tb, t, half, tv), inv);
             *reinterpret_cast<float4*>(L.z + zs) = z;
             if (DOT) {
                 double rz = 0.0, zq = 0.0;
