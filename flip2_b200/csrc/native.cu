@@ -109,11 +109,17 @@ constexpr int kBoxN = kBox * kBox * kBox;
 constexpr int kPcThreads = 512;         // one thread per cell of the tile
 constexpr int kPcChunk = 4096;          // particles sorted per round (a denser tile takes several)
 constexpr int kPcPer = kPcChunk / kPcThreads;
+// Sorted slot j lives at j + j / 8: with about eight particles a cell, the
+// threads of a warp (consecutive cells) read slots about eight apart, which
+// would otherwise fall on four banks; one word of padding per eight slots
+// spreads them over all 32.
+constexpr int kPcSlots = kPcChunk + kPcChunk / 8;
+__device__ __forceinline__ uint32_t pc_slot(uint32_t j) { return j + (j >> 3); }
 struct P2GCellSmem {
     float m[3][kBoxN], w[3][kBoxN];     // the box: momentum and weight sums per component
-    float g[3][kPcChunk];               // grid coordinates of each sorted slot's particle
+    float g[3][kPcSlots];               // grid coordinates of each sorted slot's particle
     uint32_t cnt[kPcThreads], off[kPcThreads];
-    uint16_t order[kPcChunk];           // particle (within the round) of each sorted slot
+    uint16_t order[kPcSlots];           // particle (within the round) of each sorted slot
     uint32_t scan[kPcThreads / 32 + 1];
 };
 
@@ -178,9 +184,9 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
             for (int i = 0; i < kPcPer; ++i)
                 if (slot[i] != 0xFFFFFFFFu) {
                     const uint32_t q = (uint32_t)(tid + kPcThreads * i), at = S.off[slot[i] & 511u] + (slot[i] >> 9);
-                    S.order[at] = (uint16_t)q;
+                    S.order[pc_slot(at)] = (uint16_t)q;
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) S.g[a][at] = nat_grid_coord(P[a][r0 + q], o[a], D.inv_h);
+                    for (int a = 0; a < 3; ++a) S.g[a][pc_slot(at)] = nat_grid_coord(P[a][r0 + q], o[a], D.inv_h);
                 }
             __syncthreads();
             const uint32_t b0 = S.off[tid], b1 = b0 + S.cnt[tid];
@@ -196,8 +202,9 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
 #pragma unroll
                 for (int k = 0; k < 18; ++k) am[k] = aw[k] = 0.0f;
                 for (uint32_t j = b0; j < b1; ++j) {
-                    const uint64_t p = r0 + S.order[j];
-                    const float gx = S.g[0][j], gy = S.g[1][j], gz = S.g[2][j];
+                    const uint32_t js = pc_slot(j);
+                    const uint64_t p = r0 + S.order[js];
+                    const float gx = S.g[0][js], gy = S.g[1][js], gz = S.g[2][js];
                     const float go = comp == 0 ? gx : (comp == 1 ? gy : gz);
                     const float g1 = comp == 0 ? gy : gx, g2 = comp == 2 ? gy : gz;
                     int b;
