@@ -601,7 +601,7 @@ def main():
         if stages.get(k, 0.0) > 0.0:
             g = b / (stages[k] / 1e3) / 1e9
             stages_gbs[k] = {"ms": stages[k], "bytes": b, "gbs": g, "frac": g / peak}
-    # the survey's headline figure for the particle stages: P2G + G2P/advect,
+    # the particle stages' headline figure: P2G + G2P/advect at their minimum,
     # 72 B per particle + 40 B per active voxel
     pg_ms = stages["p2g"] + stages["g2p_advect"]
     pg_bytes = 72.0 * n + 40.0 * voxels
