@@ -197,8 +197,9 @@ typedef struct {
                                     less) the network solves                          */
     double max_substep_dt;       /* NATIVE: largest sub-step of solveFrame (1/240)  */
     int32_t learned_max_iter;    /* NATIVE: FPCG cap before the Jacobi-PCG restart   */
-    int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers on CUDA
-                                    cores instead of tcgen05 (for comparison)         */
+    int32_t lp_cuda_cores;       /* NATIVE: 1 runs the network's 16->16 layers and its
+                                    backward pass (training) on CUDA cores instead of
+                                    tcgen05 (for comparison)                          */
     int32_t pcg_warm_start;      /* NATIVE: 1 (default) starts each step's Jacobi-PCG
                                     or multilevel FCG (pressure_method 0 or 2) from
                                     the previous step's pressure on the cells fluid in
