@@ -30,13 +30,17 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 int set_cuda_error(cudaError_t e, const char* what);
 
-// flip_sort_pairs with two extra controls (sort.cu): err_accum, when not
-// null, is a device word that receives the look-back timeout bit instead of
-// the scratch's own error word; tile_base > 0 leaves the first tile_base
-// tiles of every pass unclaimed (the timeout test only).
+// flip_sort_pairs with extra controls (sort.cu): err_accum, when not null,
+// is a device word that receives the look-back timeout bit instead of the
+// scratch's own error word; tile_base > 0 leaves the first tile_base tiles
+// of every pass unclaimed (the timeout test only); head_dense, when not
+// null, receives the segment heads of the sorted keys: head_dense[k] = the
+// output index of the first key equal to k for every k < head_limit that
+// occurs, 0xFFFFFFFF for the others (the last pass finds them as it
+// scatters).
 int sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out, uint64_t n,
                   int key_bits, void* scratch, size_t scratch_bytes, cudaStream_t s, uint32_t* err_accum,
-                  uint32_t spin_limit, uint32_t tile_base);
+                  uint32_t spin_limit, uint32_t tile_base, uint32_t* head_dense = nullptr, uint32_t head_limit = 0);
 void set_error_text(const char* text);
 const char* error_text();
 

@@ -760,16 +760,17 @@ static int nat_bin(flip_engine* e) {
         e->keys_valid = true;
     }
     E_TRY(e->mark(1));
+    // the sort's last pass also marks the segment heads in head_dense
     E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
-                        e->stream, e->d_err, kSpinLimit, 0));
+                        e->stream, e->d_err, kSpinLimit, 0, e->head_dense, (uint32_t)e->ntiles_total));
     E_TRY(e->mark(2));
     E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
     for (int a = 0; a < 6; ++a) std::swap(e->fp[a], e->fq[a]);
     E_TRY(e->mark(3));
-    E_TRY(nat_launch_segment_heads(e->keys, e->n, (uint32_t)e->ntiles_total, e->head_dense, e->node_keys, e->starts,
-                                   e->d_counts, nat_grid(e, 8), e->stream));
+    E_TRY(nat_launch_segment_heads(e->head_dense, (uint32_t)e->ntiles_total, e->node_keys, e->starts, e->d_counts,
+                                   e->stream));
     E_TRY(e->mark(4));
-    e->launches += 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 2;
+    e->launches += 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 1;
     e->binned = true;
     return FLIP_OK;
 }
@@ -1484,10 +1485,10 @@ static int cap_step(flip_engine* e) {
     const float* gdtp = &e->d_frame->gdt;
     // binning (the keys come from the previous G2P or from the launch)
     E_TRY(sort_pairs_ex(e->keys, nullptr, e->keys, e->perm, e->n, e->key_bits, e->sort_scratch, e->sort_scratch_bytes,
-                        e->stream, e->d_err, kSpinLimit, 0));
+                        e->stream, e->d_err, kSpinLimit, 0, e->head_dense, (uint32_t)e->ntiles_total));
     E_TRY(nat_launch_gather(e->perm, e->n, (const float* const*)e->fp, e->fq, e->stream));
-    E_TRY(nat_launch_segment_heads(e->keys, e->n, (uint32_t)e->ntiles_total, e->head_dense, e->node_keys, e->starts,
-                                   e->d_counts, nat_grid(e, 8), e->stream));
+    E_TRY(nat_launch_segment_heads(e->head_dense, (uint32_t)e->ntiles_total, e->node_keys, e->starts, e->d_counts,
+                                   e->stream));
     // P2G and the face grids
     const size_t fb = 4 * e->nslots;
     for (int c = 0; c < 3; ++c) {
@@ -1514,7 +1515,7 @@ static int cap_step(flip_engine* e) {
 }
 // kernels of one captured step outside its loops and its restart branch
 static uint32_t cap_step_launches(flip_engine* e) {
-    uint32_t k = 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 2;  // sort, gather, heads
+    uint32_t k = 2 + (uint32_t)((e->key_bits + 7) / 8) + 1 + 1;  // sort, gather, heads
     k += 1 + (e->has_solid ? 1 : 0) + 3 + 1;                       // P2G .. normalise
     k += 2 + (e->P.pcg_warm_start ? 1 : 0) + 1 + 1;                // state, init (+ warm), loop condition, record
     if (e->P.pressure_method == 2) {

@@ -198,6 +198,22 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
                 const int n1 = comp == 0 ? D.ny : D.nx, n2 = comp == 2 ? D.ny : D.nz;
                 const int c1 = comp == 0 ? cell[1] : cell[0], c2 = comp == 2 ? cell[1] : cell[2];
                 const float* __restrict__ vc = comp == 0 ? vx : (comp == 1 ? vy : vz);
+                // Every particle of the walk lies in this thread's cell, so the
+                // stencil's bases are constants of the thread: along the own
+                // axis the cell co (weights 1 - f, f with f = sat(g - co));
+                // along a staggered axis the cell or the one below, chosen by
+                // the sign of f' = g - (c + 1/2), with the weights
+                // max(-f', 0), 1 - |f'|, max(f', 0) on the nodes c - 1, c,
+                // c + 1.  At the first and last cell f' is clamped at 0, where
+                // the stencil's clamp puts all the weight on the cell's own
+                // node.  The values equal those of nat_stencil bit for bit
+                // (every subtraction here is exact; 1 - |f'| rounds as 1 - f
+                // does there).  The own axis's wall faces take no weight: the
+                // flush below skips them.
+                const int co = comp == 0 ? cell[0] : (comp == 1 ? cell[1] : cell[2]);
+                const float cof = (float)co, c1h = (float)c1 + 0.5f, c2h = (float)c2 + 0.5f;
+                const float lo1 = c1 == 0 ? 0.0f : -1.0f, hi1 = c1 == n1 - 1 ? 0.0f : 1.0f;
+                const float lo2 = c2 == 0 ? 0.0f : -1.0f, hi2 = c2 == n2 - 1 ? 0.0f : 1.0f;
                 float am[18], aw[18];
 #pragma unroll
                 for (int k = 0; k < 18; ++k) am[k] = aw[k] = 0.0f;
@@ -207,41 +223,34 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
                     const float gx = S.g[0][js], gy = S.g[1][js], gz = S.g[2][js];
                     const float go = comp == 0 ? gx : (comp == 1 ? gy : gz);
                     const float g1 = comp == 0 ? gy : gx, g2 = comp == 2 ? gy : gz;
-                    int b;
-                    float f;
-                    // own axis: the stencil's base is the cell itself; the wall
-                    // faces of this component take no weight
-                    nat_axis(go, no, b, f);
-                    const float wo0 = (b == 0) ? 0.0f : 1.0f - f, wo1 = (b + 1 == no) ? 0.0f : f;
-                    // staggered axes: the base is the cell or the one below
-                    float w1[3], w2[3];
-                    nat_axis(g1 - 0.5f, n1 - 1, b, f);
-                    {
-                        const bool below = b < c1;
-                        w1[0] = below ? 1.0f - f : 0.0f;
-                        w1[1] = below ? f : 1.0f - f;
-                        w1[2] = below ? 0.0f : f;
-                    }
-                    nat_axis(g2 - 0.5f, n2 - 1, b, f);
-                    {
-                        const bool below = b < c2;
-                        w2[0] = below ? 1.0f - f : 0.0f;
-                        w2[1] = below ? f : 1.0f - f;
-                        w2[2] = below ? 0.0f : f;
-                    }
                     const float v = vc[p];
+                    const float fo = __saturatef(go - cof);
+                    const float wo0 = 1.0f - fo, wo1 = fo;
+                    const float f1 = fminf(fmaxf(g1 - c1h, lo1), hi1), f2 = fminf(fmaxf(g2 - c2h, lo2), hi2);
+                    const float w1[3] = {fmaxf(-f1, 0.0f), 1.0f - fabsf(f1), fmaxf(f1, 0.0f)};
+                    const float w2[3] = {fmaxf(-f2, 0.0f), 1.0f - fabsf(f2), fmaxf(f2, 0.0f)};
+                    const float wv0 = wo0 * v, wv1 = wo1 * v;
 #pragma unroll
                     for (int d2 = 0; d2 < 3; ++d2)
 #pragma unroll
                         for (int d1 = 0; d1 < 3; ++d1) {
                             const float w12 = w1[d1] * w2[d2];
                             const int k = 2 * (d1 + 3 * d2);
-                            const float wa = wo0 * w12, wb = wo1 * w12;
-                            aw[k] += wa;
-                            am[k] = fmaf(wa, v, am[k]);
-                            aw[k + 1] += wb;
-                            am[k + 1] = fmaf(wb, v, am[k + 1]);
+                            aw[k] = fmaf(wo0, w12, aw[k]);
+                            am[k] = fmaf(wv0, w12, am[k]);
+                            aw[k + 1] = fmaf(wo1, w12, aw[k + 1]);
+                            am[k + 1] = fmaf(wv1, w12, am[k + 1]);
                         }
+                }
+                // the wall faces of the own axis (face 0 below the first cell,
+                // face n above the last) keep no weight
+                if (co == 0) {
+#pragma unroll
+                    for (int k = 0; k < 18; k += 2) aw[k] = 0.0f;
+                }
+                if (co == no - 1) {
+#pragma unroll
+                    for (int k = 1; k < 18; k += 2) aw[k] = 0.0f;
                 }
                 // 18 phases: in phase k every thread adds its node k; at one
                 // offset no two cells share a node.  Box origin: tile origin - 1.
@@ -422,39 +431,57 @@ __global__ void __launch_bounds__(kCompactThreads) nat_compact_kernel(const uint
     if (threadIdx.x == 0) *d_count = total;
 }
 
-// Segment heads of the sorted tile keys through a dense per-tile table
-// (replaces a scan of head flags: no look-back chain).  dense[key] = index of
-// the first particle with that tile key (kNoHead if the tile is empty); the
-// compaction then lists the occupied tiles in key order -- the order of the
-// sorted segments -- with their starts.
+// Segment heads of the sorted tile keys: the sort's last pass leaves
+// dense[key] = the index of the first particle with that tile key (kNoHead
+// for an empty tile; no scan of head flags, no look-back chain), and one CTA
+// lists the occupied tiles in key order -- the order of the sorted segments
+// -- with their starts.  It takes the table in chunks staged in shared
+// memory by coalesced loads; a thread then counts and writes 8 consecutive
+// entries (stored one word of padding per 8, so that a warp's reads fall on
+// distinct banks).
 constexpr uint32_t kNoHead = 0xFFFFFFFFu;
-__global__ void nat_heads_kernel(const uint32_t* __restrict__ keys, uint64_t n, uint32_t ntotal,
-                                 uint32_t* __restrict__ dense) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        if ((i == 0 || keys[i - 1] != k) && k < ntotal) dense[k] = (uint32_t)i;
-    }
-}
+constexpr int kHcPer = 8;
+constexpr uint32_t kHcChunk = (uint32_t)kCompactThreads * kHcPer;
+__device__ __forceinline__ uint32_t hc_slot(uint32_t i) { return i + (i >> 3); }
 __global__ void __launch_bounds__(kCompactThreads) nat_heads_compact_kernel(const uint32_t* __restrict__ dense,
                                                                             uint32_t ntotal, uint32_t* __restrict__ list,
                                                                             uint32_t* __restrict__ starts,
                                                                             uint32_t* __restrict__ d_count) {
+    __shared__ uint32_t sd[kHcChunk + kHcChunk / 8];
     __shared__ uint32_t sh[kCompactThreads / 32 + 1];
-    const uint32_t per = (ntotal + kCompactThreads - 1) / kCompactThreads;
-    const uint32_t b0 = min(ntotal, threadIdx.x * per), b1 = min(ntotal, b0 + per);
-    uint32_t c = 0;
-    for (uint32_t i = b0; i < b1; ++i) c += dense[i] != kNoHead ? 1u : 0u;
-    uint32_t total;
-    uint32_t o = block_exclusive_scan<kCompactThreads>(c, sh, &total);
-    for (uint32_t i = b0; i < b1; ++i) {
-        const uint32_t st = dense[i];
-        if (st != kNoHead) {
-            list[o] = i;
-            starts[o] = st;
-            ++o;
+    const uint32_t tid = threadIdx.x;
+    uint32_t out = 0;
+    for (uint32_t c0 = 0; c0 < ntotal; c0 += kHcChunk) {
+        const uint32_t m = min(kHcChunk, ntotal - c0);
+        uint32_t v[kHcPer];
+#pragma unroll
+        for (int r = 0; r < kHcPer; ++r) {
+            const uint32_t i = tid + r * kCompactThreads;
+            v[r] = i < m ? dense[c0 + i] : kNoHead;
         }
+#pragma unroll
+        for (int r = 0; r < kHcPer; ++r) sd[hc_slot(tid + r * kCompactThreads)] = v[r];
+        __syncthreads();
+        const uint32_t b0 = tid * kHcPer;
+        uint32_t c = 0;
+#pragma unroll
+        for (int r = 0; r < kHcPer; ++r) {
+            v[r] = sd[hc_slot(b0 + r)];
+            c += v[r] != kNoHead ? 1u : 0u;
+        }
+        uint32_t total;
+        uint32_t o = out + block_exclusive_scan<kCompactThreads>(c, sh, &total);
+#pragma unroll
+        for (int r = 0; r < kHcPer; ++r)
+            if (v[r] != kNoHead) {
+                list[o] = c0 + b0 + r;
+                starts[o] = v[r];
+                ++o;
+            }
+        out += total;
+        __syncthreads();  // the next chunk overwrites sd and sh
     }
-    if (threadIdx.x == 0) *d_count = total;
+    if (tid == 0) *d_count = out;
 }
 
 // solid mask (tile-blocked) onto the cell types
@@ -1425,10 +1452,8 @@ int nat_launch_fluid_tiles(const uint8_t* type, uint8_t* flags, uint32_t ntiles_
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;
 }
-int nat_launch_segment_heads(const uint32_t* keys, uint64_t n, uint32_t ntiles_total, uint32_t* dense, uint32_t* list,
-                             uint32_t* starts, uint32_t* d_count, int grid, cudaStream_t s) {
-    FLIP_CUDA_TRY(cudaMemsetAsync(dense, 0xFF, sizeof(uint32_t) * ntiles_total, s));
-    if (n) nat_heads_kernel<<<grid, 256, 0, s>>>(keys, n, ntiles_total, dense);
+int nat_launch_segment_heads(const uint32_t* dense, uint32_t ntiles_total, uint32_t* list, uint32_t* starts,
+                             uint32_t* d_count, cudaStream_t s) {
     nat_heads_compact_kernel<<<1, kCompactThreads, 0, s>>>(dense, ntiles_total, list, starts, d_count);
     FLIP_CUDA_TRY(cudaGetLastError());
     return FLIP_OK;

@@ -127,10 +127,11 @@ int nat_launch_keys(const float* px, const float* py, const float* pz, uint64_t 
                     cudaStream_t s);
 int nat_launch_gather(const uint32_t* perm, uint64_t n, const float* const* src, float* const* dst, cudaStream_t s);
 // occupied tiles of sorted tile keys, in key order: list[c] the tile key,
-// starts[c] its first particle, *d_count their number (dense: a scratch
-// table of ntiles_total words)
-int nat_launch_segment_heads(const uint32_t* keys, uint64_t n, uint32_t ntiles_total, uint32_t* dense, uint32_t* list,
-                             uint32_t* starts, uint32_t* d_count, int grid, cudaStream_t s);
+// starts[c] its first particle, *d_count their number, from the sort's head
+// table (dense[key] = the first particle of the tile, 0xFFFFFFFF for an
+// empty tile; ntiles_total words)
+int nat_launch_segment_heads(const uint32_t* dense, uint32_t ntiles_total, uint32_t* list, uint32_t* starts,
+                             uint32_t* d_count, cudaStream_t s);
 int nat_launch_p2g(const uint32_t* tile_keys, const uint32_t* starts, const uint32_t* d_ntiles, uint64_t n,
                    const float* const* ps, const float* const* vs, const NatDims& D, float* const* m, float* const* w,
                    uint8_t* type, int grid, cudaStream_t s);

@@ -51,33 +51,39 @@ static SortLayout sort_layout(uint64_t n) {
 }
 
 // ----------------------------------------------------------- histogram
-// Each thread counts kHistItems keys per round (loads issued together) into
-// its warp's own histogram: the digits of blob-concentrated keys would
-// otherwise have every warp of the block adding into the same few words.  A
-// digit the whole warp shares (keys sorted or nearly so, as the tile keys of
-// consecutive steps are) takes one atomic for the warp; otherwise each lane
-// adds its own.
+// A block counts one contiguous chunk of the keys, kHistItems keys per
+// thread and round (loads issued together, each warp reading 128 contiguous
+// bytes), into its warps' own histograms: the digits of blob-concentrated
+// keys would otherwise have every warp of the block adding into the same few
+// words.  A digit the whole warp shares (keys sorted or nearly so, as the
+// tile keys of consecutive steps are) takes one atomic for the warp;
+// otherwise each lane adds its own.  With nearly sorted keys a chunk holds
+// few digits, so few of the block's bins reach the global histogram.
 constexpr int kHistItems = 8;
-__global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint32_t* __restrict__ keys, uint64_t n,
-                                                                      int passes, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t sh[kSortWarps][kMaxPasses][kRadix];
-    for (int i = threadIdx.x; i < kSortWarps * kMaxPasses * kRadix; i += blockDim.x) (&sh[0][0][0])[i] = 0;
+constexpr uint64_t kHistRound = (uint64_t)kSortThreads * kHistItems;
+__global__ void __launch_bounds__(kSortThreads, 6) sort_histogram_kernel(const uint32_t* __restrict__ keys, uint64_t n,
+                                                                      int passes, uint64_t chunk,
+                                                                      uint32_t* __restrict__ hist) {
+    extern __shared__ uint32_t sh[];  // [kSortWarps][passes][kRadix]
+    for (int i = threadIdx.x; i < kSortWarps * passes * kRadix; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     const int warp = threadIdx.x >> 5;
-    uint32_t* H = &sh[warp][0][0];
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    // the warp's lanes take the same number of rounds (the votes below need all of them)
-    for (uint64_t w0 = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < n; w0 += stride * kHistItems) {
-        const uint64_t i0 = w0 + (threadIdx.x & 31u);
+    uint32_t* H = sh + warp * passes * kRadix;
+    const uint64_t c0 = (uint64_t)blockIdx.x * chunk;
+    const uint64_t c1 = c0 + chunk < n ? c0 + chunk : n;
+    // every thread of the block takes the same number of rounds (the votes
+    // below need all lanes of a warp)
+    for (uint64_t r0 = c0; r0 < c1; r0 += kHistRound) {
+        const uint64_t i0 = r0 + threadIdx.x;
         uint32_t k[kHistItems];
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
-            const uint64_t i = i0 + (uint64_t)j * stride;
-            k[j] = i < n ? keys[i] : 0u;
+            const uint64_t i = i0 + (uint64_t)j * kSortThreads;
+            k[j] = i < c1 ? keys[i] : 0u;
         }
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
-            const bool valid = i0 + (uint64_t)j * stride < n;
+            const bool valid = i0 + (uint64_t)j * kSortThreads < c1;
             const uint32_t nvalid = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
             for (int p = 0; p < passes; ++p) {
                 const uint32_t d = (k[j] >> (8 * p)) & 0xFFu;
@@ -94,7 +100,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_histogram_kernel(const uint
     for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
         uint32_t v = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) v += (&sh[w][0][0])[i];
+        for (int w = 0; w < kSortWarps; ++w) v += sh[w * passes * kRadix + i];
         if (v) atomicAdd(&hist[i], v);
     }
 }
@@ -111,11 +117,11 @@ __global__ void sort_offsets_kernel(const uint32_t* __restrict__ hist, uint32_t*
 
 // ------------------------------------------------------------ onesweep
 template <bool kIota>
-__global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 4) onesweep_kernel(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, uint64_t n, int shift, const uint32_t* __restrict__ offsets,
     uint32_t* __restrict__ status, uint32_t* __restrict__ tile_ctr, uint32_t* __restrict__ err, uint32_t spin_limit,
-    uint32_t tile_base) {
+    uint32_t tile_base, uint32_t* __restrict__ head_dense, uint32_t head_limit) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_whist[kSortWarps][kRadix];  // warp counts, then warp offsets within the digit
     __shared__ uint32_t s_blk[kRadix];                // tile-local exclusive offset of each digit
@@ -228,6 +234,10 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         if (o < n) {  // always true unless a look-back wait timed out
             kout[o] = k;
             vout[o] = s_vals[j];
+            // last pass: the tile's keys are sorted in full, so the first of a
+            // run of equal keys here is a candidate head; the smallest
+            // candidate over the tiles is the head
+            if (head_dense && (j == 0 || s_keys[j - 1] != k) && k < head_limit) atomicMin(head_dense + k, o);
         }
     }
 }
@@ -240,7 +250,9 @@ extern "C" size_t flip_sort_pairs_scratch_bytes(uint64_t n) { return sort_layout
 
 int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                         uint64_t n, int key_bits, void* scratch, size_t scratch_bytes, cudaStream_t s,
-                        uint32_t* err_accum, uint32_t spin_limit, uint32_t tile_base) {
+                        uint32_t* err_accum, uint32_t spin_limit, uint32_t tile_base, uint32_t* head_dense,
+                        uint32_t head_limit) {
+    if (head_dense && head_limit) FLIP_CUDA_TRY(cudaMemsetAsync(head_dense, 0xFF, sizeof(uint32_t) * head_limit, s));
     if (n == 0) return FLIP_OK;
     if (!keys_in || !keys_out || !vals_out || !scratch || key_bits < 1 || key_bits > 32 || n >= (1ull << 30)) {
         set_error_text("flip_sort_pairs: bad argument (null pointer, key_bits outside 1..32 or n >= 2^30)");
@@ -272,9 +284,16 @@ int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    uint64_t hblocks = (n + kSortThreads * 16 - 1) / (kSortThreads * 16);
-    if (hblocks > (uint64_t)sms * 8) hblocks = (uint64_t)sms * 8;
-    sort_histogram_kernel<<<(unsigned)hblocks, kSortThreads, 0, s>>>(keys_in, n, passes, hist);
+    // one wave: as many blocks as are resident at once
+    const size_t hsmem = sizeof(uint32_t) * kSortWarps * passes * kRadix;
+    int per_sm = 1;
+    FLIP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sort_histogram_kernel, kSortThreads, hsmem));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t hblocks = (n + kHistRound - 1) / kHistRound;
+    if (hblocks > (uint64_t)sms * per_sm) hblocks = (uint64_t)sms * per_sm;
+    const uint64_t hchunk = (n + hblocks * kHistRound - 1) / (hblocks * kHistRound) * kHistRound;
+    hblocks = (n + hchunk - 1) / hchunk;
+    sort_histogram_kernel<<<(unsigned)hblocks, kSortThreads, hsmem, s>>>(keys_in, n, passes, hchunk, hist);
     sort_offsets_kernel<<<passes, kRadix, 0, s>>>(hist, offs);
     // pass p writes `out` when (passes-1-p) is even, so the last pass lands in out
     const bool inplace_odd = (keys_in == keys_out || (vals_in && vals_in == vals_out)) && (passes % 2 == 1);
@@ -286,12 +305,13 @@ int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32
         uint32_t* ok = to_out ? keys_out : ak;
         uint32_t* ov = to_out ? vals_out : av;
         uint32_t* pstat = status + (size_t)p * tiles * kRadix;
+        uint32_t* hd = p == passes - 1 ? head_dense : nullptr;
         if (p == 0 && cv == nullptr)
             onesweep_kernel<true><<<grid, kSortThreads, 0, s>>>(ck, nullptr, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
-                                                                ctr + p, err, spin_limit, tile_base);
+                                                                ctr + p, err, spin_limit, tile_base, hd, head_limit);
         else
             onesweep_kernel<false><<<grid, kSortThreads, 0, s>>>(ck, cv, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
-                                                                 ctr + p, err, spin_limit, tile_base);
+                                                                 ctr + p, err, spin_limit, tile_base, hd, head_limit);
         ck = ok;
         cv = ov;
     }
