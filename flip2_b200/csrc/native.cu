@@ -109,17 +109,18 @@ constexpr int kBoxN = kBox * kBox * kBox;
 constexpr int kPcThreads = 512;         // one thread per cell of the tile
 constexpr int kPcChunk = 4096;          // particles sorted per round (a denser tile takes several)
 constexpr int kPcPer = kPcChunk / kPcThreads;
-// Sorted slot j lives at j + j / 8: with about eight particles a cell, the
-// threads of a warp (consecutive cells) read slots about eight apart, which
-// would otherwise fall on four banks; one word of padding per eight slots
-// spreads them over all 32.
+// Sorted slot j (16 bytes) lives at j + j / 8: with about eight particles a
+// cell, the threads of a warp (consecutive cells) read slots about eight
+// apart, and the eight threads of a quarter warp, whose 16-byte reads share
+// one pass over the banks, would otherwise hit the same four banks; one slot
+// of padding per eight spreads them over all 32.
 constexpr int kPcSlots = kPcChunk + kPcChunk / 8;
 __device__ __forceinline__ uint32_t pc_slot(uint32_t j) { return j + (j >> 3); }
 struct P2GCellSmem {
     float m[3][kBoxN], w[3][kBoxN];     // the box: momentum and weight sums per component
-    float g[3][kPcSlots];               // grid coordinates of each sorted slot's particle
+    float4 gq[kPcSlots];                // per sorted slot: the particle's grid coordinates and
+                                        // (w, as bits) its index within the round
     uint32_t cnt[kPcThreads], off[kPcThreads];
-    uint16_t order[kPcSlots];           // particle (within the round) of each sorted slot
     uint32_t scan[kPcThreads / 32 + 1];
 };
 
@@ -184,9 +185,9 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
             for (int i = 0; i < kPcPer; ++i)
                 if (slot[i] != 0xFFFFFFFFu) {
                     const uint32_t q = (uint32_t)(tid + kPcThreads * i), at = S.off[slot[i] & 511u] + (slot[i] >> 9);
-                    S.order[pc_slot(at)] = (uint16_t)q;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) S.g[a][pc_slot(at)] = nat_grid_coord(P[a][r0 + q], o[a], D.inv_h);
+                    S.gq[pc_slot(at)] = make_float4(nat_grid_coord(P[0][r0 + q], o[0], D.inv_h),
+                                                    nat_grid_coord(P[1][r0 + q], o[1], D.inv_h),
+                                                    nat_grid_coord(P[2][r0 + q], o[2], D.inv_h), __uint_as_float(q));
                 }
             __syncthreads();
             const uint32_t b0 = S.off[tid], b1 = b0 + S.cnt[tid];
@@ -218,9 +219,9 @@ __global__ void __launch_bounds__(kPcThreads, 2) nat_p2g_cells_kernel(
 #pragma unroll
                 for (int k = 0; k < 18; ++k) am[k] = aw[k] = 0.0f;
                 for (uint32_t j = b0; j < b1; ++j) {
-                    const uint32_t js = pc_slot(j);
-                    const uint64_t p = r0 + S.order[js];
-                    const float gx = S.g[0][js], gy = S.g[1][js], gz = S.g[2][js];
+                    const float4 gq = S.gq[pc_slot(j)];
+                    const uint64_t p = r0 + __float_as_uint(gq.w);
+                    const float gx = gq.x, gy = gq.y, gz = gq.z;
                     const float go = comp == 0 ? gx : (comp == 1 ? gy : gz);
                     const float g1 = comp == 0 ? gy : gx, g2 = comp == 2 ? gy : gz;
                     const float v = vc[p];
