@@ -39,13 +39,14 @@ __device__ __forceinline__ uint8_t nat_type(const uint8_t* type, int i, int j, i
     if (i < 0 || j < 0 || k < 0 || i >= D.nx || j >= D.ny || k >= D.nz) return kSolid;
     return type[nslot(i, j, k, D)];
 }
+// stencil base and weight on one axis of M + 1 nodes: s clamped into
+// [0, M], base floor(s) capped at M - 1 (computed as a float, which is exact
+// for these small integers), weight s - base
 __device__ __forceinline__ void nat_axis(float s, int M, int& i0, float& f) {
     s = fminf(fmaxf(s, 0.0f), (float)M);
-    int b = (int)floorf(s);
-    b = min(b, M - 1);
-    b = max(b, 0);
-    i0 = b;
-    f = s - (float)b;
+    const float b = fminf(floorf(s), (float)(M - 1));
+    i0 = (int)b;
+    f = s - b;
 }
 // trilinear stencil of component c at grid coordinates (gx, gy, gz)
 __device__ __forceinline__ void nat_stencil(int c, float gx, float gy, float gz, const NatDims& D, int& i0, int& j0, int& k0,
