@@ -55,10 +55,11 @@ static SortLayout sort_layout(uint64_t n) {
 // thread and round (loads issued together, each warp reading 128 contiguous
 // bytes), into its warps' own histograms: the digits of blob-concentrated
 // keys would otherwise have every warp of the block adding into the same few
-// words.  A digit the whole warp shares (keys sorted or nearly so, as the
-// tile keys of consecutive steps are) takes one atomic for the warp;
-// otherwise each lane adds its own.  With nearly sorted keys a chunk holds
-// few digits, so few of the block's bins reach the global histogram.
+// words.  A key the whole warp shares (keys sorted or nearly so, as the
+// tile keys of consecutive steps are) is counted for the warp, in registers
+// while consecutive items keep it; otherwise each lane adds its own.  With
+// nearly sorted keys a chunk holds few digits, so few of the block's bins
+// reach the global histogram.
 constexpr int kHistItems = 8;
 constexpr uint64_t kHistRound = (uint64_t)kSortThreads * kHistItems;
 __global__ void __launch_bounds__(kSortThreads, 6) sort_histogram_kernel(const uint32_t* __restrict__ keys, uint64_t n,
@@ -71,6 +72,11 @@ __global__ void __launch_bounds__(kSortThreads, 6) sort_histogram_kernel(const u
     uint32_t* H = sh + warp * passes * kRadix;
     const uint64_t c0 = (uint64_t)blockIdx.x * chunk;
     const uint64_t c1 = c0 + chunk < n ? c0 + chunk : n;
+    // a key the whole warp shares, over consecutive items, is counted in
+    // registers (warp-uniform values) and reaches the histograms when the key
+    // changes
+    uint32_t run_key = 0u, run_cnt = 0u;
+    const bool lane0 = (threadIdx.x & 31u) == 0u;
     // every thread of the block takes the same number of rounds (the votes
     // below need all lanes of a warp)
     for (uint64_t r0 = c0; r0 < c1; r0 += kHistRound) {
@@ -85,17 +91,22 @@ __global__ void __launch_bounds__(kSortThreads, 6) sort_histogram_kernel(const u
         for (int j = 0; j < kHistItems; ++j) {
             const bool valid = i0 + (uint64_t)j * kSortThreads < c1;
             const uint32_t nvalid = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
-            for (int p = 0; p < passes; ++p) {
-                const uint32_t d = (k[j] >> (8 * p)) & 0xFFu;
-                const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
-                if (__all_sync(0xffffffffu, !valid || d == d0)) {
-                    if ((threadIdx.x & 31) == 0 && nvalid) atomicAdd(H + p * kRadix + d0, nvalid);
-                } else if (valid) {
-                    atomicAdd(H + p * kRadix + d, 1u);
+            const uint32_t k0 = __shfl_sync(0xffffffffu, k[j], 0);
+            if (__all_sync(0xffffffffu, !valid || k[j] == k0)) {
+                if (k0 != run_key || run_cnt == 0u) {
+                    if (lane0 && run_cnt)
+                        for (int p = 0; p < passes; ++p) atomicAdd(H + p * kRadix + ((run_key >> (8 * p)) & 0xFFu), run_cnt);
+                    run_key = k0;
+                    run_cnt = 0u;
                 }
+                run_cnt += nvalid;
+            } else if (valid) {
+                for (int p = 0; p < passes; ++p) atomicAdd(H + p * kRadix + ((k[j] >> (8 * p)) & 0xFFu), 1u);
             }
         }
     }
+    if (lane0 && run_cnt)
+        for (int p = 0; p < passes; ++p) atomicAdd(H + p * kRadix + ((run_key >> (8 * p)) & 0xFFu), run_cnt);
     __syncthreads();
     for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
         uint32_t v = 0;
