@@ -8,7 +8,7 @@
 // Structure (Adinets & Merrill's onesweep):
 //   1. one upfront pass reads every key once and builds all digit histograms
 //      (shared-memory atomics into one histogram per warp);
-//   2. one kernel per 8-bit digit: each CTA claims the next tile of 4096 keys
+//   2. one kernel per 8-bit digit: each CTA claims the next tile of 6144 keys
 //      from an atomic counter, ranks its keys per warp with match/ballot,
 //      publishes its per-digit counts and resolves its global offsets with a
 //      decoupled look-back over the predecessor tiles, then scatters through
@@ -20,8 +20,8 @@ namespace flip {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
+constexpr int kSortItems = 24;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 6144 keys
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 4;
 constexpr int kLook = 8;  // predecessors a look-back step reads at once
@@ -128,7 +128,7 @@ __global__ void sort_offsets_kernel(const uint32_t* __restrict__ hist, uint32_t*
 
 // ------------------------------------------------------------ onesweep
 template <bool kIota>
-__global__ void __launch_bounds__(kSortThreads, 4) onesweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, uint64_t n, int shift, const uint32_t* __restrict__ offsets,
     uint32_t* __restrict__ status, uint32_t* __restrict__ tile_ctr, uint32_t* __restrict__ err, uint32_t spin_limit,
@@ -138,8 +138,9 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_kernel(
     __shared__ uint32_t s_blk[kRadix];                // tile-local exclusive offset of each digit
     __shared__ uint32_t s_gbase[kRadix];              // global output base of each digit for this tile
     __shared__ uint32_t s_scan[kSortWarps + 1];
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
+    extern __shared__ uint32_t s_stage[];  // the tile reordered: keys, then values
+    uint32_t* s_keys = s_stage;
+    uint32_t* s_vals = s_stage + kSortTile;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u) + tile_base;
@@ -283,6 +284,7 @@ int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32
     uint32_t* ak = (uint32_t*)(S + L.alt_k);
     uint32_t* av = (uint32_t*)(S + L.alt_v);
     const int passes = (key_bits + 7) / 8;
+
     const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
     if (tile_base >= tiles) {
         set_error_text("flip_sort_pairs: tile_base beyond the tile count");
@@ -294,6 +296,15 @@ int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32
     FLIP_CUDA_TRY(cudaMemsetAsync(S, 0, L.status + sizeof(uint32_t) * passes * tiles * kRadix, s));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
+    // the staging buffer may exceed the default 48 KB (once per device)
+    static bool stage_attr[64] = {};
+    if (dev >= 0 && dev < 64 && !stage_attr[dev]) {
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(onesweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           2 * kSortTile * (int)sizeof(uint32_t)));
+        FLIP_CUDA_TRY(cudaFuncSetAttribute(onesweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           2 * kSortTile * (int)sizeof(uint32_t)));
+        stage_attr[dev] = true;
+    }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // one wave: as many blocks as are resident at once
     const size_t hsmem = sizeof(uint32_t) * kSortWarps * passes * kRadix;
@@ -317,11 +328,12 @@ int flip::sort_pairs_ex(const uint32_t* keys_in, const uint32_t* vals_in, uint32
         uint32_t* ov = to_out ? vals_out : av;
         uint32_t* pstat = status + (size_t)p * tiles * kRadix;
         uint32_t* hd = p == passes - 1 ? head_dense : nullptr;
+        constexpr int kStage = 2 * kSortTile * (int)sizeof(uint32_t);
         if (p == 0 && cv == nullptr)
-            onesweep_kernel<true><<<grid, kSortThreads, 0, s>>>(ck, nullptr, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
+            onesweep_kernel<true><<<grid, kSortThreads, kStage, s>>>(ck, nullptr, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
                                                                 ctr + p, err, spin_limit, tile_base, hd, head_limit);
         else
-            onesweep_kernel<false><<<grid, kSortThreads, 0, s>>>(ck, cv, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
+            onesweep_kernel<false><<<grid, kSortThreads, kStage, s>>>(ck, cv, ok, ov, n, 8 * p, offs + p * kRadix, pstat,
                                                                  ctr + p, err, spin_limit, tile_base, hd, head_limit);
         ck = ok;
         cv = ov;
