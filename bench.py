@@ -585,12 +585,13 @@ def main():
     particle_stages = {"value": n / (part_ms / 1e3), "unit": METRIC, "ms_per_step": part_ms, "stages": part_keys,
                        "note": "stage times from CUDA events of the profiled steps; excludes pressure and projection"}
     # algorithmic bytes per stage (per particle p, per active voxel v of the
-    # fluid tiles) and the bandwidth they make of the stage's CUDA-event time
+    # fluid tiles) and the bandwidth they make of the stage's CUDA-event time.
+    # The segment heads have none: the sort's last pass finds them, and their
+    # stage only compacts the per-tile table (one CTA, latency bound).
     it_step = pcg_iters / nprof
     stage_bytes = {
         "sort": 36.0 * n,                     # histogram 4 B + 2 onesweep passes x 16 B (tile keys)
         "gather": 52.0 * n,                   # permutation 4 B + 24 B read + 24 B write
-        "segment_heads": 4.0 * n + 8.0 * fluid_tiles,
         "p2g": 24.0 * n + 24.0 * voxels,      # state read; momentum and weight per face written
         "g2p_advect": 52.0 * n + 24.0 * voxels,  # state read, state + next key written; new and old faces read
         "pcg_iterations": per_voxel * voxels * it_step,
