@@ -109,7 +109,8 @@ int flip_inclusive_scan_u32_noalloc_status(void* stream, uint32_t* flags);
 int flip_scratch_status(const void* scratch, void* stream, uint32_t* flags);
 /* Test hook for those bounded waits (no reference counterpart): the scan
  * (which = 0, out_keys receives the scan) or the sort with the index payload
- * (which = 1, 32-bit keys) of n > 4096 keys from `in`, run with tile 0 never
+ * (which = 1, 32-bit keys) of more keys than one tile holds (4096 for the
+ * scan, 6144 for the sort) from `in`, run with tile 0 never
  * claimed, so that tile 1's look-back polls a word nothing publishes and
  * gives up after spin_limit polls.  Returns flip_scratch_status's result:
  * FLIP_ERR_TIMEOUT with bit 0 in *flags.  The outputs are invalid; the
