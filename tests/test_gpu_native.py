@@ -261,3 +261,36 @@ def test_native_particles_stay_out_of_solids(torch):
     info = P.info()
     assert info.converged == 1 and info.error_flags == 0
     P.close()
+
+
+def _tile_keys(px, py, pz, nc):
+    """Tile key of each position as the binning computes it: grid coordinate
+    p / h in FP32 (exact here: h is a power of two), cell floor(g) clamped
+    into [0, nc), key = tx + (nc / 8) (ty + (nc / 8) tz) of the 8^3 tile."""
+    t = nc // 8
+    c = [np.clip(np.floor(np.asarray(a, np.float32) * np.float32(nc)), 0, nc - 1).astype(np.int64) >> 3
+         for a in (px, py, pz)]
+    return c[0] + t * (c[1] + t * c[2])
+
+
+def test_native_binning_segments(torch):
+    """The native binning's sort and segment heads (the tile list and each
+    tile's first particle, found by the sort's last radix pass) against numpy:
+    a stable argsort of the tile keys and the first index of every run, on two
+    consecutive steps (the second step's keys come from G2P)."""
+    nc, dt = 64, 1.0 / 120
+    pos, _ = scenes.dam_break(nc, seed=1)
+    vel = scenes.random_velocities(pos.shape[0], seed=5, scale=2.0)
+    P = native(pos.shape[0], nc)
+    P.upload(pos, vel)
+    for _ in range(2):
+        x0, _ = P.download()  # positions at the start of the step, in the engine's order
+        P.step(dt)
+        keys = _tile_keys(x0[:, 0], x0[:, 1], x0[:, 2], nc)
+        perm = P.read(F.BUF_PERM).astype(np.int64)
+        assert np.array_equal(perm, np.argsort(keys, kind="stable"))
+        sk = keys[perm]
+        heads = np.flatnonzero(np.r_[True, sk[1:] != sk[:-1]])
+        assert np.array_equal(P.read(F.BUF_TILE_LIST).astype(np.int64), sk[heads])
+        assert np.array_equal(P.read(F.BUF_STARTS).astype(np.int64), heads)
+    P.close()
