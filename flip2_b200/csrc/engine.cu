@@ -229,7 +229,7 @@ extern "C" void flip_default_params(int mode, flip_params* out) {
     out->pcg_tol = 1e-6;
     out->pcg_max_iter = 5000;
     out->pcg_check_every = 16;
-    out->true_residual_every = 32;
+    out->true_residual_every = 64;
     out->permute_velocities = 0;
     out->device = 0;
     out->max_substep_dt = 1.0 / 240.0;
